@@ -1,0 +1,182 @@
+/* ofeli_gpu.h -- C ABI of libofeli_gpu.so, the B200 (sm_100a) implementation
+ * of OFELI's P1 assembly + preconditioned Krylov path.
+ *
+ * Every entry point takes plain pointers and sizes.  A vector argument may be
+ * a host pointer (pageable or pinned) or a device pointer on the current
+ * device; the library detects which and stages host data through its own
+ * device buffers.  All calls are synchronous with respect to the host when
+ * they return a value that depends on device work; the library runs its work
+ * on one stream per device (ofg_get_stream) unless ofg_set_stream selects
+ * another.
+ *
+ * Conventions follow OFELI (OFELI 5.3.3, paths within that project):
+ *   - CSR patterns are exchanged in SpMatrix's layout: row_ptr 0-based with
+ *     n+1 entries, col_ind 1-based (include/linear_algebra/SpMatrix_impl.h
+ *     :108-119, 392-413).  Device storage is int32 0-based.
+ *   - Preconditioner codes are OFELI's enum Preconditioner values
+ *     (include/linear_algebra/Matrix.h:87-93): IDENT 0, DIAG 1, DILU 2,
+ *     ILU 3, SSOR 4.  ILU is OFELI's ILUFactorize, i.e. diagonal ILU.
+ *   - Krylov results are returned as OFELI does: the number of iterations
+ *     when converged, minus the number of iterations when not
+ *     (include/solvers/CG.h:99-157, include/solvers/GMRes.h:148-241).
+ *
+ * Status codes: 0 = success, negative = error (ofg_last_error() gives the
+ * message of the calling thread's last failure).  Errors never leave the
+ * device in a faulted state: waits inside kernels are bounded and report
+ * through a status word.
+ */
+#ifndef OFELI_GPU_H
+#define OFELI_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OFG_OK 0
+#define OFG_ERR_ARG (-1)        /* bad argument (null handle, size mismatch) */
+#define OFG_ERR_CUDA (-2)       /* a CUDA runtime call failed */
+#define OFG_ERR_PIVOT (-3)      /* zero pivot / missing diagonal (OFELIException in OFELI) */
+#define OFG_ERR_JACOBIAN (-4)   /* non-positive element Jacobian (Triang3/Tetra4 throw) */
+#define OFG_ERR_PATTERN (-5)    /* pattern not supported (nnz >= 2^31, row wider than limit) */
+#define OFG_ERR_TIMEOUT (-6)    /* a bounded in-kernel wait ran out */
+#define OFG_ERR_NOMEM (-7)
+#define OFG_ERR_SIZE (-8)       /* size beyond a stated maximum */
+
+enum { OFG_IDENT = 0, OFG_DIAG = 1, OFG_DILU = 2, OFG_ILU = 3, OFG_SSOR = 4 };
+
+typedef struct ofg_matrix ofg_matrix;
+typedef struct ofg_mesh ofg_mesh;
+typedef struct ofg_prec ofg_prec;
+
+/* ---------------------------------------------------------------- runtime */
+const char* ofg_last_error(void);
+const char* ofg_version(void);
+/* Selects the stream used by later calls (NULL = the library's own). */
+int ofg_set_stream(void* cuda_stream);
+void* ofg_get_stream(void);
+/* Number of kernels this library has launched in this process. */
+int64_t ofg_launch_count(void);
+
+/* ------------------------------------------------------ sparse CSR matrix */
+/* SpMatrix<real_t>(row_ptr, col_ind) -- include/linear_algebra/SpMatrix.h:94-210.
+ * Values start at zero. */
+int ofg_matrix_create(int64_t n, int64_t nnz, const int64_t* row_ptr, const int64_t* col_ind,
+                      ofg_matrix** out);
+int ofg_matrix_destroy(ofg_matrix* A);
+int ofg_matrix_info(const ofg_matrix* A, int64_t* n, int64_t* nnz);
+/* Pattern back in OFELI layout (getRowPtr/getColInd, SpMatrix_impl.h:816-826). */
+int ofg_matrix_get_pattern(const ofg_matrix* A, int64_t* row_ptr, int64_t* col_ind);
+/* SpMatrix::set values / SpMatrix::get() (SpMatrix_impl.h:983-995). */
+int ofg_matrix_set_values(ofg_matrix* A, const double* a);
+int ofg_matrix_get_values(const ofg_matrix* A, double* a);
+/* Device pointers of the CSR arrays (int32 0-based columns, FP64 values). */
+int ofg_matrix_device_arrays(const ofg_matrix* A, const int32_t** row_ptr, const int32_t** col,
+                             double** values);
+/* SpMatrix::clear (SpMatrix_impl.h:974-979). */
+int ofg_matrix_clear(ofg_matrix* A);
+/* SpMatrix::Mult / MultAdd: y = A x, y += A x (SpMatrix_impl.h:729-745). */
+int ofg_spmv(const ofg_matrix* A, const double* x, double* y);
+int ofg_spmv_add(const ofg_matrix* A, const double* x, double* y);
+/* Device-only SpMV with an explicit layout choice, for measurement:
+ * kind 0 = CSR warp-segment kernel, 1 = SELL-32 kernel. */
+int ofg_spmv_device(const ofg_matrix* A, int kind, const double* d_x, double* d_y);
+
+/* -------------------------------------------------------------- P1 meshes */
+/* Mesh(xmin,xmax,ymin,ymax,nx,ny,cx0,cxN,cy0,cyN,TRIANGLE) --
+ * src/mesh/Mesh.cpp:547-676: x-major nodes, 2 triangles per cell, node code
+ * from the boundary line codes; equations numbered over code-0 nodes
+ * (Mesh::removeImposedDOF, include/mesh/Mesh.h:420). */
+int ofg_mesh_create_rect(double xmin, double xmax, double ymin, double ymax, int64_t nx, int64_t ny,
+                         int cx0, int cxN, int cy0, int cyN, ofg_mesh** out);
+/* Unit cube split into M^3 cells, 6 positively oriented tetrahedra per cell
+ * (Kuhn subdivision), nodes x fastest, code 1 on every face.  Replaces
+ * OFELI's 3-D structured tetrahedral generator (src/mesh/Mesh.cpp:678-836),
+ * which produces inverted elements. */
+int ofg_mesh_create_kuhn(int64_t M, ofg_mesh** out);
+/* General P1 mesh (Mesh::Add of nodes and elements, include/mesh/Mesh.h:321-325):
+ * dim 2 (triangles, nen 3) or 3 (tetrahedra, nen 4); elem holds 0-based node
+ * indices; a node with code > 0 carries an imposed value and no equation. */
+int ofg_mesh_create(int dim, int64_t nn, const double* coords, int64_t ne, const int32_t* elem,
+                    const int32_t* code, ofg_mesh** out);
+int ofg_mesh_destroy(ofg_mesh* m);
+int ofg_mesh_info(const ofg_mesh* m, int* dim, int64_t* nn, int64_t* ne, int64_t* neq,
+                  int* ncolors);
+int ofg_mesh_get(const ofg_mesh* m, double* coords, int32_t* elem, int32_t* code, int64_t* dof);
+/* Node::setCoord for every node (coordinates only; topology unchanged). */
+int ofg_mesh_set_coords(ofg_mesh* m, const double* coords);
+
+/* NodeGraph (src/linear_algebra/GraphOfMatrix.cpp:347-375): the CSR pattern
+ * of SpMatrix(mesh) built on the device, bit-identical to OFELI's sort+unique
+ * result, plus the element-to-CSR scatter map used by assembly. */
+int ofg_matrix_create_from_mesh(ofg_mesh* m, ofg_matrix** out);
+
+/* Equation::build() for the stationary P1 problems (A cleared first):
+ *   dim 2: Laplace2DT3::LHS (times kel when given) and BodyRHS
+ *          (src/equations/laplace/Laplace2DT3.cpp:131-143);
+ *   dim 3: DC3DT4::Diffusion(kel) and BodyRHS (src/equations/therm/DC3DT4.cpp
+ *          :128-135, 207-211);
+ * with Equation::updateBC lifting the nodal bc values of coded nodes
+ * (include/equations/Equation_impl.h:160-176).  kel (ne), f (nn) and bc (nn)
+ * may be NULL (k = 1, f = 0, bc = 0).  b receives the n-vector RHS. */
+int ofg_assemble_p1(ofg_mesh* m, ofg_matrix* A, const double* kel, const double* f,
+                    const double* bc, double* b);
+/* Equa_Therm::build for DC2DT3 under backward Euler
+ * (include/equations/therm/Equa_Therm.h:162-218): consistent + lumped
+ * capacity (OFELI's CAPACITY and LUMPED_CAPACITY share one bit), diffusion
+ * eps, convection by the nodal velocity v (2*nn, interleaved), RHS
+ * (dti*eA1)*u_old plus the updateBC lift. */
+int ofg_assemble_cd2d(ofg_mesh* m, ofg_matrix* A, double eps, const double* v, double dt,
+                      const double* u_old, const double* bc, double* b);
+/* Vect::insertBC (include/linear_algebra/Vect_impl.h:1098-1130): nodal
+ * vector from the equation-space solution x and bc (may be NULL). */
+int ofg_insert_bc(const ofg_mesh* m, const double* x, const double* bc, double* u);
+
+/* ------------------------------------------------------- preconditioners */
+/* Prec<real_t>(A, type) -- include/solvers/Prec_impl.h:164-195: DIAG
+ * inverts the diagonal, DILU/ILU run DILUFactorize (SpMatrix_impl.h:837-878),
+ * SSOR keeps the diagonal.  The factorisation uses the current values of A. */
+int ofg_prec_create(ofg_matrix* A, int type, ofg_prec** out);
+int ofg_prec_destroy(ofg_prec* P);
+/* Recompute the factorisation after the values of A changed. */
+int ofg_prec_update(ofg_prec* P);
+/* Prec::solve(b, x) (Prec_impl.h:227-255). */
+int ofg_prec_apply(ofg_prec* P, const double* b, double* x);
+/* Prec::getPivot for all rows (inverse pivots for DIAG/DILU/ILU). */
+int ofg_prec_get_pivot(const ofg_prec* P, double* pivot);
+
+/* ----------------------------------------------------------------- Krylov */
+/* CG(A, P, b, x, max_it, toler) -- include/solvers/CG.h:99-157.  x holds the
+ * initial guess and receives the solution.  *result = iterations (>= 0) or
+ * -iterations when max_it was reached; *res (may be NULL) = last relative
+ * residual ||r||/||b||. */
+int ofg_cg(ofg_prec* P, const double* b, double* x, int max_it, double toler, int* result,
+           double* res);
+/* ofg_cg that also records the relative residual after every iteration in
+ * hist[1 .. iterations] (hist holds max_it + 1 values), the sequence OFELI
+ * prints at Verbosity > 3 (CG.h:140-143). */
+int ofg_cg_history(ofg_prec* P, const double* b, double* x, int max_it, double toler, int* result,
+                   double* res, double* hist);
+/* GMRes(A, P, b, x, m, max_it, toler) -- include/solvers/GMRes.h:148-241
+ * (left preconditioned, modified Gram-Schmidt, Givens rotations). */
+int ofg_gmres(ofg_prec* P, const double* b, double* x, int m, int max_it, double toler,
+              int* result, double* res);
+/* Mixed-precision solve: FP64 iterative refinement whose correction equation
+ * is solved by preconditioned CG in FP32 (inner_bits 32) or with BF16 matrix
+ * values and FP32 vectors (inner_bits 16).  Converged when the FP64 true
+ * relative residual ||b - A x|| / ||b|| <= toler.  prec_type: DIAG, DILU,
+ * ILU or SSOR, built in the inner precision.  *outer = refinement steps,
+ * *inner = total inner CG iterations, *true_res = final FP64 relative
+ * residual. */
+int ofg_solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, const double* b, double* x,
+                    int max_outer, int max_inner, double inner_tol, double toler, int* outer,
+                    int* inner, double* true_res);
+/* FP64 true relative residual ||b - A x|| / ||b|| on the device. */
+int ofg_residual(const ofg_matrix* A, const double* b, const double* x, double* rel);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OFELI_GPU_H */

@@ -1,0 +1,105 @@
+// internal.cuh -- the handle types behind the C ABI and the helpers the
+// translation units share.
+#pragma once
+
+#include "common.cuh"
+
+// Device CSR matrix.  The CSR arrays are the master copy (OFELI's SpMatrix
+// layout, 0-based int32 columns on the device); a SELL-32 copy of the values
+// (slices of 32 consecutive rows stored column-major, rows kept in natural
+// order) is rebuilt lazily when the values change and feeds the SpMV inside
+// the Krylov loops.
+struct ofg_matrix {
+   int64_t n = 0, nnz = 0;
+   ofg::DBuf<int32_t> row_ptr, col;
+   ofg::DBuf<double> val;
+   uint64_t version = 1;  // bumped whenever values change
+
+   // diagonal position of every row (OFELI's id[i]-1); -1 if absent
+   ofg::DBuf<int32_t> dpos;
+   bool dpos_ready = false;
+   bool dpos_complete = false;
+
+   // SELL-32 layout
+   int64_t nslices = 0;
+   ofg::DBuf<int32_t> sell_ptr;  // nslices+1, offsets in entries
+   ofg::DBuf<int32_t> sell_col;  // padded entries point at a valid row, value 0
+   ofg::DBuf<int32_t> sell_src;  // CSR index of every SELL entry, -1 for padding
+   ofg::DBuf<double> sell_val;
+   ofg::DBuf<float> sell_val32;
+   bool sell_ready = false;
+   uint64_t sell_version = 0, sell32_version = 0;
+   int max_row = 0;
+   double avg_row = 0;
+
+   // element-to-CSR map of the mesh this pattern came from
+   ofg_mesh* mesh = nullptr;
+   ofg::DBuf<int32_t> emap;  // ne * nen * nen, -1 where a DOF is imposed
+};
+
+struct ofg_mesh {
+   int dim = 2, nen = 3;
+   int64_t nn = 0, ne = 0, neq = 0;
+   ofg::DBuf<double> coords;  // nn * dim
+   ofg::DBuf<int32_t> elem;   // ne * nen, 0-based
+   ofg::DBuf<int32_t> code;   // nn
+   ofg::DBuf<int32_t> dof;    // nn, 1-based equation number or 0
+   // node -> element adjacency (elements in ascending order)
+   ofg::DBuf<int32_t> n2e_ptr, n2e;
+   // element colouring: elements of colour c are color_elems[color_ptr[c] ..
+   // color_ptr[c+1]); no two elements of one colour share a node
+   std::vector<int64_t> color_ptr;
+   ofg::DBuf<int32_t> color_elems;
+};
+
+namespace ofg {
+// Strand plan of one sweep direction (see prec.cu).
+struct SweepPlan {
+   int64_t nstrands = 0;
+   DBuf<int32_t> start;       // logical row where each strand starts, nstrands+1
+   DBuf<double> strand_dot;   // per-strand partial dot products
+   DBuf<int> ticket;          // [0] next strand, [1] finished strands
+};
+}  // namespace ofg
+
+struct ofg_prec {
+   ofg_matrix* A = nullptr;
+   int type = OFG_DIAG;
+   ofg::DBuf<double> pivot;  // DIAG/DILU/ILU: inverse pivots; SSOR: diagonal
+   uint64_t version = 0;     // matrix version the factorisation belongs to
+   // forward-sweep result, kept at the "not ready" sentinel between sweeps
+   ofg::DBuf<double> t;
+   ofg::DBuf<int> status;    // bounded-wait failures (bit 0: timeout, bit 1: wave)
+   ofg::SweepPlan fwd, bwd;
+   ofg::DBuf<int32_t> tpos;  // D-ILU: transposed position of each lower entry
+   ofg::DBuf<double> dot;    // (r, z) of the last backward sweep that was asked for it
+   int grid = 0;             // blocks of the persistent sweep launch
+};
+
+namespace ofg {
+
+// matrix.cu
+void ensure_dpos(ofg_matrix* A);
+void ensure_sell(ofg_matrix* A);
+void ensure_sell32(ofg_matrix* A);
+void spmv_csr(const ofg_matrix* A, const double* x, double* y, bool add);
+void spmv_sell(const ofg_matrix* A, const double* x, double* y, const int* skip = nullptr);
+void matrix_touch(ofg_matrix* A);
+void matrix_finish_pattern(ofg_matrix* A);
+void scan_exclusive_i64(const int64_t* d_in, int64_t* d_out, int64_t n);
+
+// prec.cu
+void prec_setup(ofg_prec* P);
+// z = M^{-1} r on device buffers (r and z may alias).  With rz != nullptr
+// the sweep preconditioners also leave (r, z) in *rz (device scalar).  With
+// skip != nullptr every launch is a no-op while *skip != 0.
+void prec_apply_device(ofg_prec* P, const double* r, double* z, double* rz = nullptr,
+                       const int* skip = nullptr);
+void check_status(ofg_prec* P);
+
+// The "value not ready yet" marker of the triangular sweeps: a NaN payload
+// that IEEE arithmetic never produces (results are the canonical NaN).
+constexpr unsigned long long kSentinelBits = 0x7FF4DEADBEEF0001ULL;
+void fill_sentinel(double* p, int64_t n);
+
+}  // namespace ofg

@@ -1,0 +1,587 @@
+// prec.cu -- OFELI's Prec<real_t> on the device: DIAG, D-ILU (= OFELI's ILU)
+// and SSOR (symmetric Gauss-Seidel), with the triangular sweeps of
+// SpMatrix::DILUSolve / SSORSolve (include/linear_algebra/SpMatrix_impl.h
+// :882-942) and the pivot recurrence of DILUFactorize (:837-870).
+//
+// Sweep scheduling.  Rows keep OFELI's natural order, so the preconditioner
+// is the reference's own.  Rows are cut into strands: maximal runs of
+// consecutive rows where each row depends on the row just before it (on a
+// structured mesh one strand is one grid line of unknowns).  A warp takes
+// the next strand from a ticket counter and walks it in 32-row segments.
+// Readiness travels with the data: every result buffer is pre-filled with a
+// NaN payload that arithmetic never produces, a producer publishes a row by
+// storing its value (one relaxed 8-byte store, no fence), and a consumer of
+// a row in an earlier strand spins on that value with a bounded wait.
+// Tickets are taken in row order by running warps, so every row a warp waits
+// for belongs to a warp that is already running: the sweep always drains.
+// Within a segment the dependence on the previous row is a first-order
+// affine recurrence z_r = C_r + M_r z_{r-1}, resolved with a 5-step warp
+// scan; segments with other intra-segment couplings fall back to an exact
+// wave over the warp.  The D-ILU factorisation uses the same machinery in
+// its exact form, with the reference's operation order (no FMA
+// contraction), so its pivots are bit-identical to the reference's.
+//
+// Per application: 12*nnz + 4*n (matrix, once per sweep over its half) +
+// ~40*n bytes of vectors.  Time is set by the dependency chain (about 2 grid
+// lines' worth of segments on a structured 2-D mesh), not by bandwidth.
+#include <algorithm>
+
+#include "internal.cuh"
+
+namespace ofg {
+namespace {
+
+constexpr int kWarpsPerBlock = 4;
+constexpr int kMinStrand = 32;
+constexpr int kMaxStrand = 1 << 16;
+constexpr long long kSpinFast = 2048;
+constexpr long long kSpinSlow = 1 << 22;  // x ~0.5 us sleep: a few seconds at most
+
+enum { FWD_DILU = 0, FWD_SSOR = 1, BWD_DILU = 2, BWD_SSOR = 3, FACTOR = 4 };
+
+struct SweepArgs {
+   int64_t n;
+   const int32_t* rp;
+   const int32_t* col;
+   const double* val;
+   const int32_t* dpos;
+   const int32_t* tpos;    // FACTOR: CSR index of the transposed entry, -1 if absent
+   const double* piv;      // DILU: inverse pivots; SSOR: diagonal
+   const double* in;       // FWD: b; BWD: t
+   double* out;            // results, sentinel-filled on entry
+   double* reset;          // entries of this buffer get the sentinel (row by row), may be null
+   const double* dot_with; // optional: accumulates (dot_with, out)
+   double* strand_dot;     // per-strand partial sums
+   double* dot_out;        // the sum, written by the last warp
+   const int32_t* sstart;  // strand starts in logical row order, nstrands+1
+   int64_t nstrands;
+   int* ticket;            // [0] next strand, [1] finished strands
+   int* status;
+   const int* skip;        // optional: the whole launch is a no-op while *skip != 0
+};
+
+__device__ __forceinline__ bool is_sentinel(double v)
+{
+   return (unsigned long long)__double_as_longlong(v) == kSentinelBits;
+}
+
+__device__ __forceinline__ double sentinel_value()
+{
+   return __longlong_as_double((long long)kSentinelBits);
+}
+
+__device__ __noinline__ double wait_value_slow(const double* p, int* status)
+{
+   double v;
+   for (long long it = 0; it < kSpinFast; ++it) {
+      v = ld_relaxed(p);
+      if (!is_sentinel(v)) return v;
+   }
+   for (long long it = 0; it < kSpinSlow; ++it) {
+      __nanosleep(500);
+      v = ld_relaxed(p);
+      if (!is_sentinel(v)) return v;
+   }
+   atomicOr(status, 1);
+   return 0.0;
+}
+
+// Value of an earlier row, waiting (bounded) until its producer stored it.
+__device__ __forceinline__ double wait_value(const double* p, int* status)
+{
+   const double v = ld_relaxed(p);
+   return is_sentinel(v) ? wait_value_slow(p, status) : v;
+}
+
+template <int MODE>
+__device__ __forceinline__ double finish_row(double s, double bi, double pv)
+{
+   if (MODE == FWD_DILU) return pv * (bi - s);
+   if (MODE == FWD_SSOR) return (bi - s) / pv;
+   if (MODE == BWD_DILU) return bi - pv * s;
+   return bi - s / pv;  // BWD_SSOR
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) sweep_kernel(SweepArgs g)
+{
+   constexpr bool FWD = (MODE == FWD_DILU || MODE == FWD_SSOR || MODE == FACTOR);
+   __shared__ double seg[kWarpsPerBlock][32];
+   const int lane = threadIdx.x & 31;
+   const int w = threadIdx.x >> 5;
+   const unsigned FULL = 0xffffffffu;
+   const int64_t n = g.n;
+   if (g.skip && *g.skip) return;
+
+   for (;;) {
+      int s = 0;
+      if (lane == 0) s = atomicAdd(&g.ticket[0], 1);
+      s = __shfl_sync(FULL, s, 0);
+      if (s >= g.nstrands) break;
+      const int64_t beg = g.sstart[s], end = g.sstart[s + 1];
+      double carry = 0.0;
+      bool have_carry = false;
+      double dotp = 0.0;
+
+      for (int64_t s0 = beg; s0 < end; s0 += 32) {
+         const int64_t rho = s0 + lane;
+         const bool valid = rho < end;
+         const int64_t row = FWD ? rho : n - 1 - rho;
+         int32_t kb = 0, ke = 0, dk = 0;
+         if (valid) {
+            dk = g.dpos[row];
+            if (FWD) { kb = g.rp[row]; ke = dk; }
+            else { kb = dk + 1; ke = g.rp[row + 1]; }
+         }
+         // external part of the row sum (rows of earlier segments), in
+         // column order; intra-segment couplings are recorded
+         double sext = 0.0, m1 = 0.0;
+         bool other_intra = false;
+         if (MODE == FACTOR) sext = valid ? g.val[dk] : 0.0;
+         for (int32_t k = kb; k < ke; ++k) {
+            const int64_t j = g.col[k];
+            const int64_t lj = FWD ? j : n - 1 - j;
+            const double a = g.val[k];
+            if (MODE == FACTOR) {
+               const int32_t tp = g.tpos[k];
+               if (tp < 0) continue;
+               if (lj >= s0) { other_intra = true; continue; }
+               const double v = (lj == s0 - 1 && have_carry) ? carry : wait_value(g.out + j, g.status);
+               sext = __dsub_rn(sext, __dmul_rn(__dmul_rn(a, v), g.val[tp]));
+            }
+            else {
+               if (lj >= s0) {
+                  if (lj == rho - 1) m1 = a;
+                  else other_intra = true;
+                  continue;
+               }
+               const double v = (lj == s0 - 1 && have_carry) ? carry : wait_value(g.out + j, g.status);
+               sext += a * v;
+            }
+         }
+         double bi = 0.0, pv = 0.0;
+         if (valid && MODE != FACTOR) {
+            bi = g.in[row];
+            pv = g.piv[row];
+         }
+         double z;
+         const bool exact = (MODE == FACTOR) || __any_sync(FULL, other_intra);
+         if (!exact) {
+            // z = C + M * z_prev with z_prev the previous lane's result
+            double C, M;
+            if (MODE == FWD_DILU) { C = pv * (bi - sext); M = -pv * m1; }
+            else if (MODE == FWD_SSOR) { C = (bi - sext) / pv; M = -m1 / pv; }
+            else if (MODE == BWD_DILU) { C = bi - pv * sext; M = -pv * m1; }
+            else { C = bi - sext / pv; M = -m1 / pv; }
+            if (!valid) { C = 0.0; M = 0.0; }
+            if (lane == 0) M = 0.0;  // lane 0 has no intra-segment predecessor
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+               const double Cp = __shfl_up_sync(FULL, C, o);
+               const double Mp = __shfl_up_sync(FULL, M, o);
+               if (lane >= o) {
+                  C = C + M * Cp;
+                  M = M * Mp;
+               }
+            }
+            z = C;
+         }
+         else {
+            // exact wave: a lane computes once all its intra-segment
+            // predecessors are in shared memory
+            seg[w][lane] = sentinel_value();
+            __syncwarp();
+            bool done = !valid;
+            z = 0.0;
+            for (int round = 0; round < 32; ++round) {
+               if (!done) {
+                  bool ready = true;
+                  double acc = sext;
+                  for (int32_t k = kb; k < ke && ready; ++k) {
+                     const int64_t j = g.col[k];
+                     const int64_t lj = FWD ? j : n - 1 - j;
+                     if (lj < s0) continue;
+                     if (MODE == FACTOR && g.tpos[k] < 0) continue;
+                     const double v = seg[w][lj - s0];
+                     if (is_sentinel(v)) { ready = false; break; }
+                     if (MODE == FACTOR)
+                        acc = __dsub_rn(acc, __dmul_rn(__dmul_rn(g.val[k], v), g.val[g.tpos[k]]));
+                     else
+                        acc += g.val[k] * v;
+                  }
+                  if (ready) {
+                     if (MODE == FACTOR) z = __ddiv_rn(1.0, acc);
+                     else z = finish_row<MODE>(acc, bi, pv);
+                     done = true;
+                  }
+               }
+               __syncwarp();
+               if (done && valid) seg[w][lane] = z;
+               __syncwarp();
+               if (__all_sync(FULL, done)) break;
+            }
+            if (!__all_sync(FULL, done)) {
+               if (lane == 0) atomicOr(g.status, 2);
+            }
+         }
+         if (valid) {
+            st_relaxed(g.out + row, z);
+            if (g.reset) g.reset[row] = sentinel_value();
+            if (g.dot_with) dotp += g.dot_with[row] * z;
+         }
+         const int64_t last = min((int64_t)31, end - 1 - s0);
+         carry = __shfl_sync(FULL, z, (int)last);
+         have_carry = true;
+      }
+      if (g.dot_with) {
+         // last-finisher reduction over strands, in strand order
+         dotp = warp_sum(dotp);
+         int last = 0;
+         if (lane == 0) {
+            g.strand_dot[s] = dotp;
+            __threadfence();
+            last = atomicAdd(&g.ticket[1], 1) == (int)g.nstrands - 1;
+         }
+         last = __shfl_sync(FULL, last, 0);
+         if (last) {
+            __threadfence();
+            double acc = 0.0;
+            for (int64_t t = lane; t < g.nstrands; t += 32) acc += ld_relaxed(g.strand_dot + t);
+            acc = warp_sum(acc);
+            if (lane == 0) *g.dot_out = acc;
+         }
+      }
+   }
+}
+
+__global__ void fill_sentinel_kernel(double* p, int64_t n)
+{
+   int64_t stride = (int64_t)gridDim.x * blockDim.x;
+   const double s = __longlong_as_double((long long)kSentinelBits);
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) p[i] = s;
+}
+
+__global__ void diag_setup(int64_t n, const int32_t* dpos, const double* val, double* piv,
+                           int invert, int* bad)
+{
+   int64_t stride = (int64_t)gridDim.x * blockDim.x;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+      const int32_t d = dpos[i];
+      const double a = d >= 0 ? val[d] : 0.0;
+      if (a == 0.0) atomicMin(bad, (int)i);
+      piv[i] = invert ? 1.0 / a : a;
+   }
+}
+
+__global__ void diag_apply(int64_t n, const double* piv, const double* r, double* z,
+                           const int* skip)
+{
+   if (skip && *skip) return;
+   int64_t stride = (int64_t)gridDim.x * blockDim.x;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+      z[i] = r[i] * piv[i];
+}
+
+// Transposed positions for the strictly lower entries: tpos[k] = index of
+// (col[k], row) in the upper part of row col[k], -1 when absent.
+__global__ void transpose_positions(int64_t n, const int32_t* rp, const int32_t* col,
+                                    const int32_t* dpos, int32_t* tpos)
+{
+   int64_t stride = (int64_t)gridDim.x * blockDim.x;
+   for (int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; l < n; l += stride) {
+      for (int32_t k = rp[l]; k < rp[l + 1]; ++k) {
+         const int32_t i = col[k];
+         int32_t pos = -1;
+         if (i < l) {
+            int32_t lo = dpos[i] + 1, hi = rp[i + 1] - 1;
+            while (lo <= hi) {
+               const int32_t mid = (lo + hi) >> 1;
+               const int32_t c = col[mid];
+               if (c == (int32_t)l) { pos = mid; break; }
+               if (c < (int32_t)l) lo = mid + 1;
+               else hi = mid - 1;
+            }
+         }
+         tpos[k] = pos;
+      }
+   }
+}
+
+// chain[rho] = 1 when logical row rho depends on logical row rho-1
+__global__ void chain_flags(int64_t n, const int32_t* rp, const int32_t* col, const int32_t* dpos,
+                            int fwd, int8_t* chain)
+{
+   int64_t stride = (int64_t)gridDim.x * blockDim.x;
+   for (int64_t rho = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; rho < n; rho += stride) {
+      int8_t c = 0;
+      if (rho > 0) {
+         if (fwd) {
+            const int64_t r = rho;
+            for (int32_t k = rp[r]; k < dpos[r]; ++k)
+               if (col[k] == r - 1) c = 1;
+         }
+         else {
+            const int64_t r = n - 1 - rho;
+            for (int32_t k = dpos[r] + 1; k < rp[r + 1]; ++k)
+               if (col[k] == r + 1) c = 1;
+         }
+      }
+      chain[rho] = c;
+   }
+}
+
+
+}  // namespace
+
+void fill_sentinel(double* p, int64_t n)
+{
+   if (n <= 0) return;
+   fill_sentinel_kernel<<<grid_for(n, 256), 256, 0, stream()>>>(p, n);
+   count_launch();
+   OFG_LAUNCH_CHECK();
+}
+
+namespace {
+
+// Strands start where a row does not depend on its predecessor; runs shorter
+// than kMinStrand are merged forward, runs longer than kMaxStrand are split.
+void build_plan(ofg_matrix* A, bool fwd, SweepPlan& plan)
+{
+   const int64_t n = A->n;
+   DBuf<int8_t> chain(n > 0 ? n : 1);
+   if (n) {
+      chain_flags<<<grid_for(n, 256), 256, 0, stream()>>>(n, A->row_ptr.p, A->col.p, A->dpos.p,
+                                                          fwd ? 1 : 0, chain.p);
+      count_launch();
+      OFG_LAUNCH_CHECK();
+   }
+   std::vector<int8_t> c = chain.to_host(n);
+   std::vector<int32_t> starts;
+   int64_t cur = 0;
+   for (int64_t r = 1; r <= n; ++r) {
+      const bool brk = (r == n) || !c[r];
+      if ((brk && r - cur >= kMinStrand) || r - cur >= kMaxStrand || r == n) {
+         if (r > cur) starts.push_back((int32_t)cur);
+         cur = r;
+      }
+   }
+   starts.push_back((int32_t)n);
+   plan.nstrands = (int64_t)starts.size() - 1;
+   plan.start.alloc(starts.size());
+   plan.start.upload(starts.data(), starts.size());
+   plan.strand_dot.alloc(plan.nstrands > 0 ? plan.nstrands : 1);
+   plan.ticket.alloc(4);
+}
+
+SweepArgs base_args(ofg_prec* P, const SweepPlan& plan)
+{
+   ofg_matrix* A = P->A;
+   SweepArgs g{};
+   g.n = A->n;
+   g.rp = A->row_ptr.p;
+   g.col = A->col.p;
+   g.val = A->val.p;
+   g.dpos = A->dpos.p;
+   g.tpos = P->tpos.p;
+   g.piv = P->pivot.p;
+   g.sstart = plan.start.p;
+   g.nstrands = plan.nstrands;
+   g.ticket = plan.ticket.p;
+   g.strand_dot = plan.strand_dot.p;
+   g.status = P->status.p;
+   return g;
+}
+
+template <int MODE>
+void launch_sweep(ofg_prec* P, SweepPlan& plan, SweepArgs g)
+{
+   if (!plan.nstrands) return;
+   OFG_CUDA(cudaMemsetAsync(plan.ticket.p, 0, 4 * sizeof(int), stream()));
+   int blocks = (int)std::min<int64_t>((plan.nstrands + kWarpsPerBlock - 1) / kWarpsPerBlock,
+                                       (int64_t)P->grid);
+   if (blocks < 1) blocks = 1;
+   sweep_kernel<MODE><<<blocks, kWarpsPerBlock * 32, 0, stream()>>>(g);
+   count_launch();
+   OFG_LAUNCH_CHECK();
+}
+
+}  // namespace
+
+void check_status(ofg_prec* P)
+{
+   if (P->type != OFG_DILU && P->type != OFG_ILU && P->type != OFG_SSOR) return;
+   int h = 0;
+   P->status.download(&h, 1);
+   if (h) {
+      P->status.zero();
+      throw Error(OFG_ERR_TIMEOUT, "triangular sweep wait ran out (status " + std::to_string(h) + ")");
+   }
+}
+
+void prec_setup(ofg_prec* P)
+{
+   ofg_matrix* A = P->A;
+   const int64_t n = A->n;
+   ensure_dpos(A);
+   OFG_REQUIRE(A->dpos_complete || P->type == OFG_IDENT, OFG_ERR_PIVOT,
+               "a row has no diagonal entry");
+   P->version = A->version;
+   if (P->type == OFG_IDENT) return;
+   P->pivot.reserve(n > 0 ? n : 1);
+   DBuf<int> bad(1);
+   int big = INT32_MAX;
+   bad.upload(&big, 1);
+   const int invert = (P->type == OFG_SSOR) ? 0 : 1;
+   if (n) {
+      diag_setup<<<grid_for(n, 256), 256, 0, stream()>>>(n, A->dpos.p, A->val.p, P->pivot.p, invert,
+                                                         bad.p);
+      count_launch();
+      OFG_LAUNCH_CHECK();
+   }
+   int h = 0;
+   bad.download(&h, 1);
+   if (h != INT32_MAX)
+      throw Error(OFG_ERR_PIVOT, "zero pivot detected in row " + std::to_string(h + 1));
+   if (P->type == OFG_DIAG) return;
+
+   if (!P->fwd.start.p) {
+      int per_sm = 0;
+      OFG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_kernel<FWD_DILU>,
+                                                             kWarpsPerBlock * 32, 0));
+      P->grid = std::max(1, per_sm) * num_sms();
+      build_plan(A, true, P->fwd);
+      build_plan(A, false, P->bwd);
+      P->status.alloc(1);
+      P->t.alloc(n > 0 ? n : 1);
+      P->dot.alloc(1);
+   }
+   P->status.zero();
+   fill_sentinel(P->t.p, n);
+   if (P->type == OFG_DILU || P->type == OFG_ILU) {
+      if (!P->tpos.p) {
+         P->tpos.alloc(A->nnz > 0 ? A->nnz : 1);
+         if (n) {
+            transpose_positions<<<grid_for(n, 256), 256, 0, stream()>>>(n, A->row_ptr.p, A->col.p,
+                                                                        A->dpos.p, P->tpos.p);
+            count_launch();
+            OFG_LAUNCH_CHECK();
+         }
+      }
+      // pivots = 1/(a_ll - sum a_li pinv_i a_il), rows in natural order
+      fill_sentinel(P->pivot.p, n);
+      SweepArgs g = base_args(P, P->fwd);
+      g.out = P->pivot.p;
+      launch_sweep<FACTOR>(P, P->fwd, g);
+      check_status(P);
+   }
+}
+
+void prec_apply_device(ofg_prec* P, const double* r, double* z, double* rz, const int* skip)
+{
+   const int64_t n = P->A->n;
+   if (!n) return;
+   switch (P->type) {
+      case OFG_IDENT:
+         if (z != r) {
+            OFG_REQUIRE(!skip, OFG_ERR_ARG, "IDENT copy cannot be skipped on the device");
+            OFG_CUDA(cudaMemcpyAsync(z, r, n * sizeof(double), cudaMemcpyDeviceToDevice, stream()));
+         }
+         return;
+      case OFG_DIAG:
+         diag_apply<<<grid_for(n, 256), 256, 0, stream()>>>(n, P->pivot.p, r, z, skip);
+         count_launch();
+         OFG_LAUNCH_CHECK();
+         return;
+      default: break;
+   }
+   const bool dilu = (P->type != OFG_SSOR);
+   // forward: t = L-solve(r); clears z for the backward sweep
+   SweepArgs f = base_args(P, P->fwd);
+   f.in = r;
+   f.out = P->t.p;
+   f.reset = z;
+   f.skip = skip;
+   if (dilu) launch_sweep<FWD_DILU>(P, P->fwd, f);
+   else launch_sweep<FWD_SSOR>(P, P->fwd, f);
+   // backward: z = U-solve(t); clears t for the next application
+   SweepArgs b = base_args(P, P->bwd);
+   b.in = P->t.p;
+   b.out = z;
+   b.reset = P->t.p;
+   b.skip = skip;
+   if (rz && r != z) {
+      b.dot_with = r;
+      b.dot_out = rz;
+   }
+   if (dilu) launch_sweep<BWD_DILU>(P, P->bwd, b);
+   else launch_sweep<BWD_SSOR>(P, P->bwd, b);
+}
+
+}  // namespace ofg
+
+using namespace ofg;
+
+extern "C" {
+
+int ofg_prec_create(ofg_matrix* A, int type, ofg_prec** out)
+{
+   return guarded("ofg_prec_create", [&] {
+      OFG_REQUIRE(A && out, OFG_ERR_ARG, "null argument");
+      OFG_REQUIRE(type >= OFG_IDENT && type <= OFG_SSOR, OFG_ERR_ARG, "unknown preconditioner");
+      auto P = new ofg_prec();
+      P->A = A;
+      P->type = type;
+      try {
+         prec_setup(P);
+      }
+      catch (...) {
+         delete P;
+         throw;
+      }
+      *out = P;
+   });
+}
+
+int ofg_prec_destroy(ofg_prec* P)
+{
+   return guarded("ofg_prec_destroy", [&] {
+      delete P;
+      OFG_CUDA(cudaStreamSynchronize(stream()));
+   });
+}
+
+int ofg_prec_update(ofg_prec* P)
+{
+   return guarded("ofg_prec_update", [&] {
+      OFG_REQUIRE(P, OFG_ERR_ARG, "null preconditioner");
+      prec_setup(P);
+      OFG_CUDA(cudaStreamSynchronize(stream()));
+   });
+}
+
+int ofg_prec_apply(ofg_prec* P, const double* b, double* x)
+{
+   return guarded("ofg_prec_apply", [&] {
+      OFG_REQUIRE(P && b && x, OFG_ERR_ARG, "null argument");
+      if (P->version != P->A->version) prec_setup(P);
+      const int64_t n = P->A->n;
+      In<double> db(b, n);
+      InOut<double> dx(x, n, false);
+      prec_apply_device(P, db.d, dx.d);
+      dx.finish();
+      check_status(P);
+   });
+}
+
+int ofg_prec_get_pivot(const ofg_prec* P, double* pivot)
+{
+   return guarded("ofg_prec_get_pivot", [&] {
+      OFG_REQUIRE(P && pivot, OFG_ERR_ARG, "null argument");
+      OFG_REQUIRE(P->type != OFG_IDENT, OFG_ERR_ARG, "IDENT has no pivots");
+      OFG_CUDA(cudaMemcpyAsync(pivot, P->pivot.p, P->A->n * sizeof(double), cudaMemcpyDefault,
+                               stream()));
+      OFG_CUDA(cudaStreamSynchronize(stream()));
+   });
+}
+
+}  // extern "C"

@@ -1,0 +1,67 @@
+// reduce.cuh -- deterministic grid-wide reductions for the Krylov kernels.
+//
+// Every block adds its share, stores one partial per value and bumps an
+// arrival counter; the last block to arrive sums the partials in block order
+// with a fixed tree and runs the finisher on thread 0.  The grid size of a
+// kernel depends only on the problem size, so results are bitwise
+// reproducible from run to run.
+#pragma once
+
+#include "common.cuh"
+
+namespace ofg {
+
+constexpr int kRedBlock = 256;
+
+// Returns true on thread 0 of the last block, with tot[] holding the sums.
+template <int NV>
+__device__ __forceinline__ bool grid_reduce(double (&v)[NV], double* partials, unsigned* counter,
+                                            double (&tot)[NV])
+{
+   __shared__ double sh[NV][kRedBlock / 32];
+   __shared__ bool last;
+   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+   for (int i = 0; i < NV; ++i) {
+      double s = warp_sum(v[i]);
+      if (lane == 0) sh[i][wid] = s;
+   }
+   __syncthreads();
+   if (threadIdx.x == 0) {
+#pragma unroll
+      for (int i = 0; i < NV; ++i) {
+         double s = 0.0;
+         for (int w = 0; w < nw; ++w) s += sh[i][w];
+         partials[(size_t)blockIdx.x * NV + i] = s;
+      }
+      __threadfence();
+      last = atomicAdd(counter, 1u) == gridDim.x - 1;
+   }
+   __syncthreads();
+   if (!last) return false;
+   __threadfence();
+   double t[NV];
+#pragma unroll
+   for (int i = 0; i < NV; ++i) t[i] = 0.0;
+   for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+#pragma unroll
+      for (int i = 0; i < NV; ++i) t[i] += ld_relaxed(partials + (size_t)b * NV + i);
+   __syncthreads();
+#pragma unroll
+   for (int i = 0; i < NV; ++i) {
+      double s = warp_sum(t[i]);
+      if (lane == 0) sh[i][wid] = s;
+   }
+   __syncthreads();
+   if (threadIdx.x != 0) return false;
+#pragma unroll
+   for (int i = 0; i < NV; ++i) {
+      double s = 0.0;
+      for (int w = 0; w < nw; ++w) s += sh[i][w];
+      tot[i] = s;
+   }
+   *counter = 0;
+   return true;
+}
+
+}  // namespace ofg

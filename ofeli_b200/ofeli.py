@@ -1,0 +1,430 @@
+"""OFELI's API for the P1 assembly + Krylov path, backed by libofeli_gpu.so.
+
+Names, argument meanings, 1-based/0-based conventions and return values
+follow OFELI 5.3.3 (paths within that project):
+
+* ``Mesh(xmin, xmax, ymin, ymax, nx, ny, cx0, cxN, cy0, cyN)``: the structured
+  triangulation of src/mesh/Mesh.cpp:547-676; ``Mesh.kuhn(M)`` the unit cube;
+  ``Mesh.from_arrays`` a general P1 mesh (Mesh::Add).
+* ``SpMatrix(mesh)`` / ``SpMatrix(row_ptr, col_ind[, a])``: CSR with OFELI's
+  layout (0-based row_ptr, 1-based col_ind), include/linear_algebra/SpMatrix.h.
+* ``Prec(A, type)``, ``CG(A, P, b, x, max_it, toler)``,
+  ``GMRes(A, P, b, x, m, max_it, toler)``, ``LinearSolver``: include/solvers.
+* ``Laplace2DT3``, ``Laplace3DT4`` / ``DC3DT4``, ``DC2DT3``: ``build()``,
+  ``updateBC`` (folded into build), ``run()``.
+
+Vectors are numpy float64 arrays (host) or CUDA tensors (device pointers).
+Errors raise ``OFELIException`` as OFELI throws on zero pivots, negative
+Jacobians, missing matrices.
+"""
+import ctypes
+import math
+
+import numpy as np
+
+from . import capi
+
+IDENT_PREC, DIAG_PREC, DILU_PREC, ILU_PREC, SSOR_PREC = 0, 1, 2, 3, 4
+DIRECT_SOLVER, CG_SOLVER, CGS_SOLVER, BICG_SOLVER, BICG_STAB_SOLVER, GMRES_SOLVER = 1, 2, 3, 4, 5, 6
+OFELI_EPSMCH = 2.220446049250313e-16
+
+
+class OFELIException(RuntimeError):
+    pass
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return ctypes.c_void_p(a.ctypes.data)
+    if hasattr(a, "data_ptr"):
+        return ctypes.c_void_p(a.data_ptr())
+    raise TypeError("expected a numpy array or a CUDA tensor")
+
+
+def _call(name, *args):
+    try:
+        capi.call(name, *args)
+    except capi.OFGError as e:
+        raise OFELIException(str(e)) from e
+
+
+def _f64(a, n=None):
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return a
+    out = np.ascontiguousarray(a, dtype=np.float64)
+    if n is not None and out.size != n:
+        raise OFELIException("vector size %d, expected %d" % (out.size, n))
+    return out
+
+
+class Mesh:
+    """Mesh(xmin, xmax, ymin, ymax, nx, ny, cx0, cxN, cy0, cyN) -- structured
+    triangulation, 2 triangles per cell, equations on code-0 nodes."""
+
+    def __init__(self, xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0, nx=None, ny=None, cx0=1, cxN=1,
+                 cy0=1, cyN=1, _handle=None):
+        if _handle is not None:
+            self._h = _handle
+        else:
+            h = ctypes.c_void_p()
+            _call("ofg_mesh_create_rect", xmin, xmax, ymin, ymax, nx, ny, cx0, cxN, cy0, cyN,
+                  ctypes.byref(h))
+            self._h = h
+        self._info()
+
+    @classmethod
+    def kuhn(cls, M):
+        h = ctypes.c_void_p()
+        _call("ofg_mesh_create_kuhn", M, ctypes.byref(h))
+        return cls(_handle=h)
+
+    @classmethod
+    def from_arrays(cls, dim, coords, elem, code):
+        coords = np.ascontiguousarray(coords, dtype=np.float64)
+        elem = np.ascontiguousarray(elem, dtype=np.int32)
+        code = np.ascontiguousarray(code, dtype=np.int32)
+        h = ctypes.c_void_p()
+        _call("ofg_mesh_create", dim, code.size, _ptr(coords), elem.size // (dim + 1), _ptr(elem),
+              _ptr(code), ctypes.byref(h))
+        return cls(_handle=h)
+
+    def _info(self):
+        d, nc = ctypes.c_int(), ctypes.c_int()
+        nn, ne, neq = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        _call("ofg_mesh_info", self._h, ctypes.byref(d), ctypes.byref(nn), ctypes.byref(ne),
+              ctypes.byref(neq), ctypes.byref(nc))
+        self.dim, self.nn, self.ne, self.neq, self.ncolors = d.value, nn.value, ne.value, neq.value, nc.value
+
+    def getNbNodes(self):
+        return self.nn
+
+    def getNbElements(self):
+        return self.ne
+
+    def getNbEq(self):
+        return self.neq
+
+    def arrays(self):
+        coords = np.zeros(self.nn * self.dim)
+        elem = np.zeros(self.ne * (self.dim + 1), dtype=np.int32)
+        code = np.zeros(self.nn, dtype=np.int32)
+        dof = np.zeros(self.nn, dtype=np.int64)
+        _call("ofg_mesh_get", self._h, _ptr(coords), _ptr(elem), _ptr(code), _ptr(dof))
+        return coords, elem, code, dof
+
+    def setCoords(self, coords):
+        coords = _f64(coords, self.nn * self.dim)
+        _call("ofg_mesh_set_coords", self._h, _ptr(coords))
+
+    def __del__(self):
+        if getattr(self, "_h", None) and capi._lib is not None:
+            capi.lib().ofg_mesh_destroy(self._h)
+            self._h = None
+
+
+class SpMatrix:
+    """SpMatrix<real_t>: SpMatrix(mesh) builds the node graph on the device;
+    SpMatrix(row_ptr, col_ind[, a]) takes OFELI's CSR layout."""
+
+    def __init__(self, *args):
+        h = ctypes.c_void_p()
+        self.mesh = None
+        if len(args) == 1 and isinstance(args[0], Mesh):
+            self.mesh = args[0]
+            _call("ofg_matrix_create_from_mesh", self.mesh._h, ctypes.byref(h))
+        else:
+            rp = np.ascontiguousarray(args[0], dtype=np.int64)
+            ci = np.ascontiguousarray(args[1], dtype=np.int64)
+            _call("ofg_matrix_create", rp.size - 1, ci.size, _ptr(rp), _ptr(ci), ctypes.byref(h))
+        self._h = h
+        n, nnz = ctypes.c_int64(), ctypes.c_int64()
+        _call("ofg_matrix_info", self._h, ctypes.byref(n), ctypes.byref(nnz))
+        self.n, self.nnz = n.value, nnz.value
+        if len(args) >= 3 and args[2] is not None:
+            self.set_values(args[2])
+
+    def size(self):
+        return self.n
+
+    def getNbRows(self):
+        return self.n
+
+    def getLength(self):
+        return self.nnz
+
+    def pattern(self):
+        rp = np.zeros(self.n + 1, dtype=np.int64)
+        ci = np.zeros(self.nnz, dtype=np.int64)
+        _call("ofg_matrix_get_pattern", self._h, _ptr(rp), _ptr(ci))
+        return rp, ci
+
+    def set_values(self, a):
+        a = _f64(a, self.nnz)
+        _call("ofg_matrix_set_values", self._h, _ptr(a))
+
+    def values(self):
+        a = np.zeros(self.nnz)
+        _call("ofg_matrix_get_values", self._h, _ptr(a))
+        return a
+
+    def clear(self):
+        _call("ofg_matrix_clear", self._h)
+
+    def Mult(self, x, y=None):
+        x = _f64(x, self.n)
+        if y is None:
+            y = np.zeros(self.n)
+        _call("ofg_spmv", self._h, _ptr(x), _ptr(y))
+        return y
+
+    def MultAdd(self, x, y):
+        x = _f64(x, self.n)
+        _call("ofg_spmv_add", self._h, _ptr(x), _ptr(y))
+        return y
+
+    def __mul__(self, x):
+        return self.Mult(x)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and capi._lib is not None:
+            capi.lib().ofg_matrix_destroy(self._h)
+            self._h = None
+
+
+class Prec:
+    """Prec<real_t>(A, type): DIAG, DILU/ILU (diagonal ILU), SSOR (SGS)."""
+
+    def __init__(self, A, type=DIAG_PREC):
+        self.A = A
+        self.type = type
+        h = ctypes.c_void_p()
+        _call("ofg_prec_create", A._h, type, ctypes.byref(h))
+        self._h = h
+
+    def setMatrix(self, A=None):
+        if A is not None and A is not self.A:
+            self.__init__(A, self.type)
+        else:
+            _call("ofg_prec_update", self._h)
+
+    def solve(self, b, x=None):
+        b = _f64(b, self.A.n)
+        if x is None:
+            x = np.zeros(self.A.n)
+        _call("ofg_prec_apply", self._h, _ptr(b), _ptr(x))
+        return x
+
+    def getPivot(self):
+        p = np.zeros(self.A.n)
+        _call("ofg_prec_get_pivot", self._h, _ptr(p))
+        return p
+
+    def __del__(self):
+        if getattr(self, "_h", None) and capi._lib is not None:
+            capi.lib().ofg_prec_destroy(self._h)
+            self._h = None
+
+
+def _as_prec(A, P):
+    return P if isinstance(P, Prec) else Prec(A, int(P))
+
+
+def CG(A, P, b, x, max_it, toler, history=False):
+    """CG(A, P|prec, b, x, max_it, toler) -> iterations (negative when max_it
+    was reached); x holds the initial guess and receives the solution."""
+    P = _as_prec(A, P)
+    b = _f64(b, A.n)
+    res = ctypes.c_int()
+    rr = ctypes.c_double()
+    if history:
+        hist = np.zeros(max_it + 1)
+        _call("ofg_cg_history", P._h, _ptr(b), _ptr(x), max_it, toler, ctypes.byref(res),
+              ctypes.byref(rr), _ptr(hist))
+        return res.value, hist
+    _call("ofg_cg", P._h, _ptr(b), _ptr(x), max_it, toler, ctypes.byref(res), ctypes.byref(rr))
+    return res.value
+
+
+def GMRes(A, P, b, x, m, max_it, toler):
+    """GMRes(A, P|prec, b, x, m, max_it, toler) -> iterations or -iterations."""
+    P = _as_prec(A, P)
+    b = _f64(b, A.n)
+    res = ctypes.c_int()
+    rr = ctypes.c_double()
+    _call("ofg_gmres", P._h, _ptr(b), _ptr(x), m, max_it, toler, ctypes.byref(res),
+          ctypes.byref(rr))
+    return res.value
+
+
+def solve_mixed(A, b, x, prec=DIAG_PREC, inner_bits=32, toler=1e-10, max_outer=50,
+                max_inner=100000, inner_tol=1e-4):
+    """FP64 iterative refinement around an FP32 (or BF16-matrix) PCG.
+    Returns (outer steps, inner iterations, FP64 true relative residual)."""
+    b = _f64(b, A.n)
+    o, i, r = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+    _call("ofg_solve_mixed", A._h, prec, inner_bits, _ptr(b), _ptr(x), max_outer, max_inner,
+          inner_tol, toler, ctypes.byref(o), ctypes.byref(i), ctypes.byref(r))
+    return o.value, i.value, r.value
+
+
+def residual(A, b, x):
+    r = ctypes.c_double()
+    _call("ofg_residual", A._h, _ptr(_f64(b, A.n)), _ptr(_f64(x, A.n)), ctypes.byref(r))
+    return r.value
+
+
+class LinearSolver:
+    """LinearSolver (src/solvers/LinearSolver.cpp): defaults max_it 1000,
+    toler sqrt(eps); GMRES uses OFELI's restart length n/5."""
+
+    def __init__(self, A=None, b=None, x=None):
+        self._A, self._b, self._x = A, b, x
+        self._max_it = 1000
+        self._toler = math.sqrt(OFELI_EPSMCH)
+        self._s, self._p = CG_SOLVER, DIAG_PREC
+        self._nb_it = 0
+
+    def setMaxIter(self, m):
+        self._max_it = m
+
+    def setTolerance(self, t):
+        self._toler = t
+
+    def setMatrix(self, A):
+        self._A = A
+
+    def setRHS(self, b):
+        self._b = b
+
+    def setSolution(self, x):
+        self._x = x
+
+    def setSolver(self, s, p):
+        self._s, self._p = s, p
+
+    def getNbIter(self):
+        return self._nb_it
+
+    def solve(self, s=None, p=None):
+        if s is not None:
+            self.setSolver(s, p)
+        if self._A is None:
+            raise OFELIException("In LinearSolver::solve(): No matrix has been defined.")
+        if self._s == CG_SOLVER:
+            self._nb_it = CG(self._A, self._p, self._b, self._x, self._max_it, self._toler)
+        elif self._s == GMRES_SOLVER:
+            self._nb_it = GMRes(self._A, self._p, self._b, self._x, max(1, self._A.n // 5),
+                                self._max_it, self._toler)
+        else:
+            raise OFELIException("solver %d is outside the GPU path" % self._s)
+        return -self._nb_it if self._nb_it < 0 else 0
+
+
+class _P1Equation:
+    """Equation<...>::build() / run() for one P1 element family."""
+
+    def __init__(self, mesh, u=None):
+        self.mesh = mesh
+        self.u = u
+        self._A = None
+        self._b = None
+        self._bf = None
+        self._bc = None
+        self._k = None
+        self._ls = LinearSolver()
+        self._ls.setSolver(CG_SOLVER, DILU_PREC)
+
+    def setSolver(self, s, p=DIAG_PREC):
+        self._ls.setSolver(s, p)
+        if self._A is None:
+            self._A = SpMatrix(self.mesh)
+
+    def getLinearSolver(self):
+        return self._ls
+
+    def setSource(self, f):
+        self._bf = _f64(f, self.mesh.nn)
+
+    setBodyForce = setSource
+
+    def setDirichlet(self, bc):
+        self._bc = _f64(bc, self.mesh.nn)
+
+    setBoundaryCondition = setDirichlet
+
+    def setElementCoefficient(self, k):
+        """Per-element scale of the stiffness (conductivity), ne values."""
+        self._k = _f64(k, self.mesh.ne)
+
+    def getMatrix(self):
+        return self._A
+
+    def getRHS(self):
+        return self._b
+
+    def build(self):
+        if self._A is None:
+            self._A = SpMatrix(self.mesh)
+        self._b = np.zeros(self._A.n)
+        _call("ofg_assemble_p1", self.mesh._h, self._A._h, _ptr(self._k), _ptr(self._bf),
+              _ptr(self._bc), _ptr(self._b))
+
+    def run(self):
+        self.build()
+        x = np.zeros(self._A.n)
+        self._ls.setMatrix(self._A)
+        self._ls.setRHS(self._b)
+        self._ls.setSolution(x)
+        ret = self._ls.solve()
+        u = np.zeros(self.mesh.nn) if self.u is None else self.u
+        _call("ofg_insert_bc", self.mesh._h, _ptr(x), _ptr(self._bc), _ptr(u))
+        self.u = u
+        self.x = x
+        return ret
+
+
+class Laplace2DT3(_P1Equation):
+    """Laplace2DT3: area*(grad phi_i . grad phi_j) (times the element
+    coefficient), lumped source f*area/3 (src/equations/laplace/Laplace2DT3.cpp)."""
+
+
+class DC3DT4(_P1Equation):
+    """DC3DT4 stationary diffusion: k*vol*(grad phi_i . grad phi_j), lumped
+    source f*vol/4 (src/equations/therm/DC3DT4.cpp)."""
+
+
+Laplace3DT4 = DC3DT4
+
+
+class DC2DT3:
+    """DC2DT3 under backward Euler: capacity (consistent + lumped, as OFELI's
+    shared CAPACITY bit gives), diffusion eps, convection by the nodal
+    velocity; one build() per time step (include/equations/therm/Equa_Therm.h)."""
+
+    def __init__(self, mesh, u0, v, eps, dt):
+        self.mesh = mesh
+        self.u = _f64(u0, mesh.nn).copy()
+        self.v = _f64(v, 2 * mesh.nn)
+        self.eps, self.dt = eps, dt
+        self._A = SpMatrix(mesh)
+        self._bc = None
+        self.x = np.zeros(self._A.n)
+
+    def setDirichlet(self, bc):
+        self._bc = _f64(bc, self.mesh.nn)
+
+    def build(self):
+        self._b = np.zeros(self._A.n)
+        _call("ofg_assemble_cd2d", self.mesh._h, self._A._h, self.eps, _ptr(self.v), self.dt,
+              _ptr(self.u), _ptr(self._bc), _ptr(self._b))
+        return self._A, self._b
+
+    def step(self, prec=ILU_PREC, m=30, max_it=1000, toler=1e-10):
+        self.build()
+        it = GMRes(self._A, Prec(self._A, prec), self._b, self.x, m, max_it, toler)
+        _call("ofg_insert_bc", self.mesh._h, _ptr(self.x), _ptr(self._bc), _ptr(self.u))
+        return it
