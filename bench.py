@@ -1,0 +1,412 @@
+"""Benchmark: FP64-accurate solves/s of the 2-D P1 Poisson problem on a
+2049x2049-node triangulated unit square (n = 4,190,209 unknowns, nnz =
+29,315,089), f uniform in [-1, 1] per node from seed 1234, u = 0 on the
+boundary.
+
+One step = Equation::build() (element assembly into the CSR matrix and RHS
+from the source term resident in HBM) + the solve to an FP64 true relative
+residual ||b - A x|| / ||b|| <= 1e-10 + insertBC.  The chosen solver is the
+mixed-precision one (FP64 refinement around FP32 Jacobi-PCG); the plain FP64
+CG + D-ILU solve (OFELI's own method) is timed once beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 runs N independent replicas (the problem does not shard; no
+collective in the data path), launched one rank per GPU by torchrun.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "FP64-accurate solves/sec (2-D P1 Poisson 2049x2049, true rel. residual <= 1e-10)"
+UNIT = "solves/s"
+SEED = 1234
+TOL = 1e-10
+# OFELI's own CG + ILU (= diagonal ILU) on this problem converges in this
+# many iterations (run to convergence with the reference built from its
+# sources, tol 1e-10); used to extrapolate the bounded CPU samples.
+REF_ITERS_2049_ILU = None
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nx", type=int, default=2048, help="cells per side (nodes = nx+1)")
+    ap.add_argument("--inner-bits", type=int, default=32, choices=[32, 16])
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 CG+D-ILU solve")
+    ap.add_argument("--cpu-iters", type=int, default=10, help="CG iterations per CPU sample")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ clocks --
+class ClockSampler:
+    """nvidia-smi sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(HERE, "MEASURED_PEAKS.json")) as fh:
+            j = json.load(fh)
+        return float(j["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel):
+    """DRAM bytes per launch from the committed ncu summary, or None."""
+    try:
+        with open(os.path.join(HERE, "profiles", "traffic.json")) as fh:
+            return json.load(fh).get(kernel)
+    except (OSError, ValueError):
+        return None
+
+
+# ------------------------------------------------------ CPU baseline (port) --
+def cpu_baseline_port(nx, iters):
+    """The oracle port (C restatement, 1 thread) on a bounded sample of the
+    same workload: mesh, graph, assembly, D-ILU setup and `iters` CG
+    iterations; the solve is extrapolated to the iteration count OFELI
+    needs at this size."""
+    from oracle import oracle as O
+    from ofeli_b200 import fields
+    xy, elem, code = O.mesh2d(nx, nx)
+    f = fields.uniform_pm1(SEED, code.size)
+    dof, n = O.number_equations(code)
+    rp, ci = O.node_graph(elem, 3, dof, n)
+    t0 = time.perf_counter()
+    a, b = O.assemble(2, xy, elem, dof, code, n, rp, ci, f=f, bc=np.zeros(code.size))
+    t1 = time.perf_counter()
+    x, it = O.cg(rp, ci, a, b, O.ILU, iters, 1e-300)
+    t2 = time.perf_counter()
+    full_iters = REF_ITERS_2049_ILU if (nx == 2048 and REF_ITERS_2049_ILU) else None
+    per_it = (t2 - t1) / iters
+    if full_iters is None:
+        full_iters = int(round(1097 * (nx / 1024.0)))  # CG+ILU iterations grow ~ linearly in nx
+    t_solve = (t1 - t0) + per_it * full_iters
+    return {"value": 1.0 / t_solve, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": "oracle port, 1 thread: assembly + D-ILU setup + %d CG iterations at %dx%d "
+                      "nodes, solve extrapolated to %d iterations (%.3f s assembly, %.4f s/iter)"
+                      % (iters, nx + 1, nx + 1, full_iters, t1 - t0, per_it),
+            "host_cores": os.cpu_count()}
+
+
+# --------------------------------------------------------- reference arm ----
+def run_reference(args):
+    from oracle import oracle as O
+    from ofeli_b200 import fields
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    nx = args.nx
+    flavour = "ofast" if O.have_reference("ofast") else "o2"
+    if not O.have_reference(flavour):
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref was not built (needs the reference sources)"}))
+        return 0
+    f = fields.uniform_pm1(SEED, (nx + 1) ** 2)
+    nsteps = args.warmup + args.steps
+    t0 = time.perf_counter()
+    info, _ = O.run_reference(["bench2d", nx, "ILU", args.cpu_iters, nsteps], {"f": f},
+                              flavour=flavour)
+    wall = time.perf_counter() - t0
+    ta = [float(v) for v in str(info["t_assembly_steps"]).split(",")][args.warmup:]
+    tp = [float(v) for v in str(info["t_prec_steps"]).split(",")][args.warmup:]
+    ti = [float(v) for v in str(info["t_iters_steps"]).split(",")][args.warmup:]
+    full_iters = REF_ITERS_2049_ILU if (nx == 2048 and REF_ITERS_2049_ILU) else \
+        int(round(1097 * (nx / 1024.0)))
+    per_step = [a + p + i / args.cpu_iters * full_iters for a, p, i in zip(ta, tp, ti)]
+    t_step = statistics.mean(per_step)
+    value = 1.0 / t_step
+    sample = ("OFELI (reference sources, -%s), 1 thread: per step Equation::build() + "
+              "Prec(A, ILU_PREC) + %d CG iterations at %dx%d nodes, solve extrapolated to %d "
+              "iterations; graph (SpMatrix(mesh)) %.1f s once, outside the steps"
+              % ("Ofast" if flavour == "ofast" else "O2", args.cpu_iters, nx + 1, nx + 1,
+                 full_iters, float(info["t_graph"])))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "2-D P1 Poisson %dx%d nodes, CG + ILU (OFELI's diagonal ILU), "
+                                   "tol 1e-10" % (nx + 1, nx + 1), "nodes": (nx + 1) ** 2,
+                       "unknowns": int(info["n"]), "seed": SEED},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                             "sample": sample, "host_cores": os.cpu_count()},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "wall_s": wall}
+    print(json.dumps(line))
+    return 0
+
+
+# --------------------------------------------------------------- our arm ----
+def run_ours(args):
+    import torch
+    from ofeli_b200 import capi, fields
+    from ofeli_b200 import ofeli as F
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    L = capi.lib()
+    # one stream for torch and the library: ordering without extra syncs
+    work_stream = torch.cuda.Stream(device=torch.device("cuda", local))
+    torch.cuda.set_stream(work_stream)
+    capi.call("ofg_set_stream", ctypes.c_void_p(work_stream.cuda_stream))
+    nx = args.nx
+    mesh = F.Mesh(0.0, 1.0, 0.0, 1.0, nx, nx, 1, 1, 1, 1)
+    A = F.SpMatrix(mesh)
+    n, nn = A.n, mesh.nn
+    f_host = fields.uniform_pm1(SEED, nn)
+    dev = torch.device("cuda", local)
+    f_dev = torch.from_numpy(f_host).to(dev)
+    b_dev = torch.zeros(n, dtype=torch.float64, device=dev)
+    x_dev = torch.zeros(n, dtype=torch.float64, device=dev)
+    u_dev = torch.zeros(nn, dtype=torch.float64, device=dev)
+    P = F._ptr
+    stream = work_stream
+
+    def step_device():
+        capi.call("ofg_assemble_p1", mesh._h, A._h, None, P(f_dev), None, P(b_dev))
+        x_dev.zero_()
+        o, i, r = F.solve_mixed(A, b_dev, x_dev, prec=F.DIAG_PREC, inner_bits=args.inner_bits,
+                                toler=TOL)
+        capi.call("ofg_insert_bc", mesh._h, P(x_dev), None, P(u_dev))
+        return o, i, r
+
+    f_pin = torch.from_numpy(f_host).pin_memory()
+    u_pin = torch.zeros(nn, dtype=torch.float64).pin_memory()
+
+    def step_e2e():
+        # public API with host buffers: f goes up, u comes back, every step
+        capi.call("ofg_assemble_p1", mesh._h, A._h, None, P(f_pin), None, P(b_dev))
+        x_dev.zero_()
+        o, i, r = F.solve_mixed(A, b_dev, x_dev, prec=F.DIAG_PREC, inner_bits=args.inner_bits,
+                                toler=TOL)
+        capi.call("ofg_insert_bc", mesh._h, P(x_dev), None, P(u_pin))
+        return o, i, r
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if not dist:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        step_device()
+    torch.cuda.synchronize()
+
+    # ------------------------------------------------ timed: device-resident
+    launches0 = capi.launch_count()
+    capi.profile_enable(4)  # every 4th launch of a kernel family timed with events
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.4)
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    stats = []
+    for _ in range(args.steps):
+        stats.append(step_device())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    launches = capi.launch_count() - launches0
+    prof = {k: capi.profile_read(k) for k in ("spmv32", "spmv16", "spmv64", "assembly")}
+    capi.profile_enable(0)
+    ms = max_over_ranks(ms)
+    worst_res = max(s[2] for s in stats)
+    if worst_res > TOL:
+        raise SystemExit("solve missed the FP64 target: %.3e" % worst_res)
+
+    # ------------------------------------------------ timed: end to end
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    g0 = torch.cuda.Event(enable_timing=True)
+    g1 = torch.cuda.Event(enable_timing=True)
+    g0.record(stream)
+    e2e_stats = [step_e2e() for _ in range(args.steps)]
+    g1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max(g0.elapsed_time(g1), (time.perf_counter() - t0) * 1e3)
+    e2e_ms = max_over_ranks(e2e_ms)
+    if max(s[2] for s in e2e_stats) > TOL:
+        raise SystemExit("end-to-end solve missed the FP64 target")
+    u_ref = u_dev.cpu().numpy()
+    if not np.allclose(u_pin.numpy(), u_ref, rtol=0, atol=1e-12 * np.abs(u_ref).max()):
+        raise SystemExit("end-to-end result differs from the device-resident one")
+
+    # ------------------------------------------------ plain FP64 CG + D-ILU
+    plain = None
+    if not args.no_plain and rank == 0:
+        capi.call("ofg_assemble_p1", mesh._h, A._h, None, P(f_dev), None, P(b_dev))
+        Pc = F.Prec(A, F.ILU_PREC)
+        x_dev.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        it = F.CG(A, Pc, b_dev, x_dev, 100000, TOL)
+        torch.cuda.synchronize()
+        t_plain = time.perf_counter() - t0
+        plain = {"solver": "CG + ILU (OFELI's diagonal ILU), FP64, natural order",
+                 "iterations": it, "solve_s": t_plain,
+                 "true_rel_residual": F.residual(A, b_dev, x_dev)}
+        del Pc
+    # SpMV FP64 bandwidth (the plain path's kernel), live CUDA events
+    xs = torch.rand(n, dtype=torch.float64, device=dev)
+    ys = torch.empty_like(xs)
+    for _ in range(3):
+        capi.call("ofg_spmv_device", A._h, 1, P(xs), P(ys))
+    torch.cuda.synchronize()
+    h0 = torch.cuda.Event(enable_timing=True)
+    h1 = torch.cuda.Event(enable_timing=True)
+    reps = 50
+    h0.record(stream)
+    for _ in range(reps):
+        capi.call("ofg_spmv_device", A._h, 1, P(xs), P(ys))
+    h1.record(stream)
+    torch.cuda.synchronize()
+    spmv64_us = h0.elapsed_time(h1) / reps * 1e3
+    spmv64_bytes = 12.0 * A.nnz + 20.0 * n + 4.0
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return 0
+
+    peak, peak_kind = measured_peaks()
+    fam = "spmv32" if args.inner_bits == 32 else "spmv16"
+    cnt, tot_ms, tot_bytes = prof[fam]
+    avg_us = tot_ms / max(cnt, 1) * 1e3
+    achieved = (tot_bytes / max(cnt, 1)) / (avg_us * 1e-6) / 1e9 if cnt else None
+    traffic = ncu_traffic("mx_spmv_f32" if args.inner_bits == 32 else "mx_spmv_bf16")
+    cpu = cpu_baseline_port(nx, args.cpu_iters) if world == 1 else None
+    outer = sum(s[0] for s in stats) / len(stats)
+    inner = sum(s[1] for s in stats) / len(stats)
+    value = world * args.steps / (ms / 1e3)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 (refinement, residual, dots) / f32 (inner CG: SpMV, Jacobi, vectors)"
+        if args.inner_bits == 32 else "f64 refinement / bf16 matrix values, f32 vectors",
+        "data": "synthetic",
+        "config": {"workload": "2-D P1 Poisson, %dx%d nodes (%d unknowns, %d nonzeros), "
+                               "assembly + solve to FP64 true rel. residual <= 1e-10"
+                               % (nx + 1, nx + 1, n, A.nnz),
+                   "solver": "FP64 refinement around FP32 Jacobi-PCG (direction kept)",
+                   "seed": SEED, "inputs_larger_than_l2": True,
+                   "refinements_per_solve": outer, "inner_iterations_per_solve": inner},
+        "gpu_launches": launches,
+        "e2e": {"value": world * args.steps / (e2e_ms / 1e3), "unit": UNIT,
+                "h2d_bytes_per_step": 8 * nn, "d2h_bytes_per_step": 8 * nn},
+        "roofline": {"kernel": "mx_spmv<float> (SELL-32 SpMV inside the FP32 CG)"
+                     if args.inner_bits == 32 else "mx_spmv<bf16>",
+                     "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                     "peak_source": peak_kind, "launches_timed": cnt,
+                     "avg_launch_us": avg_us,
+                     "bytes_per_launch": tot_bytes / max(cnt, 1)},
+        "spmv_fp64": {"us": spmv64_us, "GB/s": spmv64_bytes / (spmv64_us * 1e-6) / 1e9,
+                      "frac_of_peak": spmv64_bytes / (spmv64_us * 1e-6) / 1e9 / peak},
+        "plain": plain,
+        "cpu_baseline": cpu,
+        "clocks": clk,
+    }
+    if plain:
+        line["plain"]["solves_per_s"] = 1.0 / plain["solve_s"]
+    print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

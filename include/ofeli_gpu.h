@@ -59,6 +59,16 @@ int ofg_set_stream(void* cuda_stream);
 void* ofg_get_stream(void);
 /* Number of kernels this library has launched in this process. */
 int64_t ofg_launch_count(void);
+/* CUDA-event timing of kernel families, for measurement: enabling (or
+ * disabling) resets the totals; while enabled (on >= 1), every on-th launch
+ * of an instrumented kernel is bracketed by events on the library stream.  Families: "spmv64", "spmv32",
+ * "spmv16" (SELL SpMV in FP64 / FP32 / BF16 values, inside the solvers too),
+ * "sweep" (triangular sweeps), "assembly" (element colour launches).
+ * *bytes = algorithmic bytes summed over the counted launches (0 when the
+ * family has no bandwidth model).  Launches that found their stop flag set
+ * are not counted.  No counterpart in OFELI (its Timer is wall clock). */
+int ofg_profile_enable(int on);
+int ofg_profile_read(const char* family, int64_t* launches, double* total_ms, double* bytes);
 
 /* ------------------------------------------------------ sparse CSR matrix */
 /* SpMatrix<real_t>(row_ptr, col_ind) -- include/linear_algebra/SpMatrix.h:94-210.
@@ -163,16 +173,23 @@ int ofg_cg_history(ofg_prec* P, const double* b, double* x, int max_it, double t
  * (left preconditioned, modified Gram-Schmidt, Givens rotations). */
 int ofg_gmres(ofg_prec* P, const double* b, double* x, int m, int max_it, double toler,
               int* result, double* res);
-/* Mixed-precision solve: FP64 iterative refinement whose correction equation
- * is solved by preconditioned CG in FP32 (inner_bits 32) or with BF16 matrix
- * values and FP32 vectors (inner_bits 16).  Converged when the FP64 true
- * relative residual ||b - A x|| / ||b|| <= toler.  prec_type: DIAG, DILU,
- * ILU or SSOR, built in the inner precision.  *outer = refinement steps,
- * *inner = total inner CG iterations, *true_res = final FP64 relative
- * residual. */
-int ofg_solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, const double* b, double* x,
-                    int max_outer, int max_inner, double inner_tol, double toler, int* outer,
-                    int* inner, double* true_res);
+/* Mixed-precision solve: FP64 iterative refinement whose correction is
+ * computed by Jacobi-preconditioned CG in FP32 (inner_bits 32) or with BF16
+ * matrix values and FP32 vectors (inner_bits 16); FP64 only for b - A x,
+ * x += correction and the accumulation of dot products.  No counterpart in
+ * OFELI (its solvers are FP64 only).
+ *   mode 0: one FP32 CG sequence; a refinement (FP64 true residual
+ *           replacing the recursive one, search direction kept) happens
+ *           whenever the FP32 residual fell by inner_tol since the last one
+ *           or predicts convergence;
+ *   mode 1: restarted refinement, each correction solved from zero to a
+ *           relative inner_tol.
+ * prec_type: DIAG or IDENT.  Converged when the FP64 true relative residual
+ * ||b - A x|| / ||b|| <= toler.  *outer = refinement steps, *inner = total
+ * inner CG iterations, *true_res = final FP64 relative residual. */
+int ofg_solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const double* b,
+                    double* x, int max_outer, int max_inner, double inner_tol, double toler,
+                    int* outer, int* inner, double* true_res);
 /* FP64 true relative residual ||b - A x|| / ||b|| on the device. */
 int ofg_residual(const ofg_matrix* A, const double* b, const double* x, double* rel);
 

@@ -32,6 +32,8 @@ SIGNATURES = {
     "ofg_set_stream": (_i32, [_p]),
     "ofg_get_stream": (_p, []),
     "ofg_launch_count": (_i64, []),
+    "ofg_profile_enable": (_i32, [_i32]),
+    "ofg_profile_read": (_i32, [ctypes.c_char_p, _pi64, _pd, _pd]),
     "ofg_matrix_create": (_i32, [_i64, _i64, _p, _p, _pp]),
     "ofg_matrix_destroy": (_i32, [_p]),
     "ofg_matrix_info": (_i32, [_p, _pi64, _pi64]),
@@ -62,7 +64,8 @@ SIGNATURES = {
     "ofg_cg": (_i32, [_p, _p, _p, _i32, _d, _pi32, _pd]),
     "ofg_cg_history": (_i32, [_p, _p, _p, _i32, _d, _pi32, _pd, _p]),
     "ofg_gmres": (_i32, [_p, _p, _p, _i32, _i32, _d, _pi32, _pd]),
-    "ofg_solve_mixed": (_i32, [_p, _i32, _i32, _p, _p, _i32, _i32, _d, _d, _pi32, _pi32, _pd]),
+    "ofg_solve_mixed": (_i32, [_p, _i32, _i32, _i32, _p, _p, _i32, _i32, _d, _d, _pi32, _pi32,
+                               _pd]),
     "ofg_residual": (_i32, [_p, _p, _p, _pd]),
 }
 
@@ -108,3 +111,14 @@ def call(name, *args):
 
 def launch_count():
     return int(lib().ofg_launch_count())
+
+
+def profile_enable(on=True):
+    call("ofg_profile_enable", 1 if on else 0)
+
+
+def profile_read(family):
+    """(launches, total ms, algorithmic bytes) of a kernel family."""
+    n, ms, b = ctypes.c_int64(), ctypes.c_double(), ctypes.c_double()
+    call("ofg_profile_read", family.encode(), ctypes.byref(n), ctypes.byref(ms), ctypes.byref(b))
+    return n.value, ms.value, b.value

@@ -262,7 +262,10 @@ static void for_each_color(ofg_mesh* m, Launch&& launch)
    for (size_t c = 0; c + 1 < m->color_ptr.size(); ++c) {
       int64_t beg = m->color_ptr[c], cnt = m->color_ptr[c + 1] - beg;
       if (!cnt) continue;
+      int* worked = prof_begin();
+      if (worked) OFG_CUDA(cudaMemsetAsync(worked, 1, sizeof(int), stream()));
       launch(m->color_elems.p + beg, cnt, grid_for(cnt, 256, 16));
+      prof_end(PROF_ASSEMBLY, 0.0);
       count_launch();
       OFG_LAUNCH_CHECK();
    }

@@ -64,6 +64,23 @@ void count_launch(int n = 1);
 
 #define OFG_LAUNCH_CHECK() OFG_CUDA(cudaGetLastError())
 
+// Optional CUDA-event timing of kernel families (ofg_profile_enable):
+// prof_begin() before a launch returns a device flag the kernel sets when it
+// does work (kernels that can be skipped by a device-side stop flag), or
+// nullptr when profiling is off; prof_end(kind, algorithmic bytes) after the
+// launch.  Launches that found their stop flag set are not counted.
+enum { PROF_SPMV64 = 0, PROF_SPMV32 = 1, PROF_SPMV16 = 2, PROF_SWEEP = 3, PROF_ASSEMBLY = 4,
+       kProfKinds = 5 };
+bool prof_on();
+int* prof_begin();
+void prof_end(int kind, double bytes);
+void prof_collect();
+
+__device__ __forceinline__ void prof_mark(int* worked)
+{
+   if (worked && blockIdx.x == 0 && threadIdx.x == 0) *worked = 1;
+}
+
 // ---------------------------------------------------------------- buffers --
 // Owning device allocation (stream-ordered on the library stream).
 template <class T>

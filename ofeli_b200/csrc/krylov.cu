@@ -91,9 +91,11 @@ __global__ void __launch_bounds__(kRedBlock) cg_spmv(int64_t n, int64_t nslices,
                                                      const double* __restrict__ sval,
                                                      const double* __restrict__ p,
                                                      double* __restrict__ q, CGState* S,
-                                                     double* partials, unsigned* counter)
+                                                     double* partials, unsigned* counter,
+                                                     int* worked)
 {
    if (S->done) return;
+   prof_mark(worked);
    double v[1] = {0.0};
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
    for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < nslices * 32;
@@ -395,9 +397,11 @@ void cg_iteration(ofg_prec* P, int64_t n, double* x, double* r, double* p, doubl
    const unsigned g = red_grid(n);
    if (PT == PT_SWEEP) prec_apply_device(P, r, z, &S->rho, &S->done);
    cg_direction<PT><<<g, kRedBlock, 0, stream()>>>(n, r, P->pivot.p, z, p, S);
+   int* worked = prof_begin();
    cg_spmv<<<grid_for(A->nslices * 32, kRedBlock, 4), kRedBlock, 0, stream()>>>(
       n, A->nslices, A->sell_ptr.p, A->sell_col.p, A->sell_val.p, p, q, S, rs.partials.p,
-      rs.counter.p);
+      rs.counter.p, worked);
+   prof_end(PROF_SPMV64, 12.0 * A->nnz + 20.0 * A->n + 4.0);
    cg_update<PT><<<g, kRedBlock, 0, stream()>>>(n, x, p, r, q, P->pivot.p, S, rs.partials.p,
                                                 rs.counter.p, tol, max_it, hist);
    count_launch(3);

@@ -156,9 +156,11 @@ __global__ void __launch_bounds__(256) spmv_sell_kernel(int64_t n, int64_t nslic
                                                         const int32_t* __restrict__ scol,
                                                         const double* __restrict__ sval,
                                                         const double* __restrict__ x,
-                                                        double* __restrict__ y, const int* skip)
+                                                        double* __restrict__ y, const int* skip,
+                                                        int* worked)
 {
    if (skip && *skip) return;
+   prof_mark(worked);
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nslices * 32; r += stride) {
       int64_t s = r >> 5;
@@ -313,8 +315,10 @@ void spmv_csr(const ofg_matrix* A, const double* x, double* y, bool add)
 void spmv_sell(const ofg_matrix* A, const double* x, double* y, const int* skip)
 {
    if (!A->n) return;
+   int* worked = prof_begin();
    spmv_sell_kernel<false><<<grid_for(A->nslices * 32, 256, 8), 256, 0, stream()>>>(
-      A->n, A->nslices, A->sell_ptr.p, A->sell_col.p, A->sell_val.p, x, y, skip);
+      A->n, A->nslices, A->sell_ptr.p, A->sell_col.p, A->sell_val.p, x, y, skip, worked);
+   prof_end(PROF_SPMV64, 12.0 * A->nnz + 20.0 * A->n + 4.0);
    count_launch();
    OFG_LAUNCH_CHECK();
 }

@@ -1,13 +1,23 @@
-// mixed.cu -- mixed-precision solve: FP64 iterative refinement around a
-// preconditioned CG that runs in FP32 (or with BF16 matrix values).
+// mixed.cu -- mixed-precision solve: FP64 iterative refinement whose
+// correction is computed by preconditioned CG in FP32 (or with BF16 matrix
+// values and FP32 vectors).
 //
-//   r = b - A x                     FP64 SpMV + FP64 residual norm
-//   solve A d = r / ||r||           inner PCG, FP32 vectors, FP32/BF16 A,
-//                                   Jacobi preconditioner in FP32, FP64 dots
-//   x += ||r|| d                    FP64 update
-// until ||b - A x|| / ||b|| <= toler.  Only the true residual, the refinement
-// update and the Krylov dot products are FP64; the inner SpMV streams 8 (FP32)
-// or 6 (BF16) bytes per nonzero instead of 12.
+// Mode 0 (refinement with a kept Krylov direction): one PCG sequence runs in
+// FP32; whenever its recursive residual has fallen by `inner_tol` since the
+// last refinement, or predicts convergence, the host performs a refinement
+// step in FP64:
+//     x += x_lo;  x_lo = 0;  r = b - A x (FP64 SpMV);  r_lo = (float) r
+// and the FP32 recurrence continues from the true residual with its search
+// direction kept (the "reliable update" form of refinement: the Krylov space
+// is not thrown away at every refinement, so the iteration count stays that
+// of FP64 CG).
+// Mode 1 (classic restarted refinement): every refinement solves
+// A d = r / ||r|| from d = 0 to `inner_tol` and adds ||r|| d.
+//
+// FP64 is used only for b - A x, the refinement update x += ..., and the
+// accumulation of every Krylov dot product.  One FP32 CG iteration streams
+// 8*nnz + 56*n bytes (6*nnz + 56*n with BF16 values) against 12*nnz + 112*n
+// in FP64.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -19,10 +29,10 @@
 namespace ofg {
 namespace {
 
-struct IRState {
-   double bnorm, rnorm, rel;                  // outer
-   double rho, rho_old, alpha, res0, res;     // inner (FP64 scalars)
-   int it, done, pad0, pad1;
+struct MixState {
+   double bnorm, rel;                 // FP64 true residual
+   double rho, rho_new, alpha, rn, rmark, res0;
+   int it, pause, done, pad;
 };
 
 __device__ __forceinline__ float to_f(float v) { return v; }
@@ -36,9 +46,10 @@ __global__ void cast_values(int64_t total, const double* __restrict__ src, T* ds
       dst[i] = (T)src[i];
 }
 
-__global__ void __launch_bounds__(kRedBlock) ir_residual(int64_t n, const double* __restrict__ b,
+// r = b - q (FP64); ||r||, ||b|| (first call); convergence test
+__global__ void __launch_bounds__(kRedBlock) mx_residual(int64_t n, const double* __restrict__ b,
                                                          const double* __restrict__ q, double* r,
-                                                         IRState* S, double* partials,
+                                                         MixState* S, double* partials,
                                                          unsigned* counter, double tol, int first)
 {
    double v[2] = {0.0, 0.0};
@@ -54,51 +65,57 @@ __global__ void __launch_bounds__(kRedBlock) ir_residual(int64_t n, const double
       if (first) {
          S->bnorm = sqrt(t[1]);
          if (S->bnorm == 0.0) S->bnorm = 1.0;
+         S->it = 0;
       }
-      S->rnorm = sqrt(t[0]);
-      S->rel = S->rnorm / S->bnorm;
+      S->rel = sqrt(t[0]) / S->bnorm;
       S->done = S->rel <= tol ? 1 : 0;
    }
 }
 
-// inner start: rr = r/||r|| (FP32), x32 = 0, z = D rr, p = z, rho = (rr, z)
-__global__ void __launch_bounds__(kRedBlock) in_start(int64_t n, const double* __restrict__ r,
-                                                      const float* __restrict__ dinv, float* rr,
-                                                      float* p, float* d, IRState* S,
-                                                      double* partials, unsigned* counter)
+// r_lo = (float)(r * scale); rho_new = (r_lo, D r_lo); ||r_lo||; optionally
+// d = 0 and p = D r_lo (fresh start)
+__global__ void __launch_bounds__(kRedBlock) mx_load_residual(int64_t n,
+                                                              const double* __restrict__ r,
+                                                              double scale,
+                                                              const float* __restrict__ dinv,
+                                                              float* rr, float* p, float* d,
+                                                              int fresh, MixState* S,
+                                                              double* partials, unsigned* counter)
 {
-   const double sc = 1.0 / S->rnorm;
    double v[2] = {0.0, 0.0};
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-      const float ri = (float)(r[i] * sc);
+      const float ri = (float)(r[i] * scale);
       const float zi = ri * dinv[i];
       rr[i] = ri;
-      p[i] = zi;
       d[i] = 0.0f;
+      if (fresh) p[i] = zi;
       v[0] += (double)ri * (double)zi;
       v[1] += (double)ri * (double)ri;
    }
    double t[2];
    if (grid_reduce<2>(v, partials, counter, t)) {
-      S->rho = t[0];
-      S->res0 = sqrt(t[1]);
-      S->res = S->res0;
-      S->it = 0;
+      S->rho_new = t[0];
+      if (fresh) S->rho = t[0];
+      S->rn = sqrt(t[1]);
+      S->rmark = S->rn;
+      if (fresh) S->res0 = S->rn;
+      S->pause = 0;
    }
 }
 
 template <class T>
-__global__ void __launch_bounds__(kRedBlock) in_spmv(int64_t n, int64_t nslices,
+__global__ void __launch_bounds__(kRedBlock) mx_spmv(int64_t n, int64_t nslices,
                                                      const int32_t* __restrict__ sp,
                                                      const int32_t* __restrict__ scol,
                                                      const T* __restrict__ sval,
                                                      const float* __restrict__ p,
-                                                     float* __restrict__ q, IRState* S,
+                                                     float* __restrict__ q, MixState* S,
                                                      double* partials, unsigned* counter,
-                                                     const int* stop)
+                                                     int* worked)
 {
-   if (*stop) return;
+   if (S->pause) return;
+   prof_mark(worked);
    double v[1] = {0.0};
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
    for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < nslices * 32;
@@ -117,15 +134,17 @@ __global__ void __launch_bounds__(kRedBlock) in_spmv(int64_t n, int64_t nslices,
    if (grid_reduce<1>(v, partials, counter, t)) S->alpha = S->rho / t[0];
 }
 
-// d += alpha p, rr -= alpha q, z = D rr, rho' = (rr, z), ||rr||
-__global__ void __launch_bounds__(kRedBlock) in_update(int64_t n, float* d,
+// d += alpha p, r -= alpha q; ||r||, (r, D r); decides when the host must
+// refine (mode 0) or stop the inner solve (mode 1)
+__global__ void __launch_bounds__(kRedBlock) mx_update(int64_t n, float* d,
                                                        const float* __restrict__ p, float* rr,
                                                        const float* __restrict__ q,
-                                                       const float* __restrict__ dinv, IRState* S,
+                                                       const float* __restrict__ dinv, MixState* S,
                                                        double* partials, unsigned* counter,
-                                                       double inner_tol, int max_inner, int* stop)
+                                                       double delta, double tol, double scale,
+                                                       int max_inner, int mode)
 {
-   if (*stop) return;
+   if (S->pause) return;
    const float a = (float)S->alpha;
    double v[2] = {0.0, 0.0};
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -138,31 +157,45 @@ __global__ void __launch_bounds__(kRedBlock) in_update(int64_t n, float* d,
    }
    double t[2];
    if (grid_reduce<2>(v, partials, counter, t)) {
-      S->res = sqrt(t[0]);
+      S->rn = sqrt(t[0]);
+      S->rho_new = t[1];
       S->it += 1;
-      S->rho_old = S->rho;
-      S->rho = t[1];
-      if (S->res <= inner_tol * S->res0 || S->it >= max_inner) *stop = 1;
+      if (mode == 0) {
+         // refine when the residual fell by delta, or when the recurrence
+         // says the FP64 target is reached
+         if (S->rn <= delta * S->rmark || S->rn * scale <= tol * S->bnorm || S->it >= max_inner)
+            S->pause = 1;
+      }
+      else if (S->rn <= delta * S->res0 || S->it >= max_inner) {
+         S->pause = 1;
+      }
    }
 }
 
-__global__ void __launch_bounds__(kRedBlock) in_direction(int64_t n, const float* __restrict__ rr,
+__global__ void __launch_bounds__(kRedBlock) mx_direction(int64_t n, const float* __restrict__ rr,
                                                           const float* __restrict__ dinv, float* p,
-                                                          const IRState* S, const int* stop)
+                                                          MixState* S)
 {
-   if (*stop) return;
-   const float beta = (float)(S->rho / S->rho_old);
+   if (S->pause) return;
+   const float beta = (float)(S->rho_new / S->rho);
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
       p[i] = rr[i] * dinv[i] + beta * p[i];
 }
 
-__global__ void ir_correct(int64_t n, double* x, const float* __restrict__ d, const IRState* S)
+// rho <- rho_new, after every block of mx_direction has read rho
+__global__ void mx_rho_shift(MixState* S)
 {
-   const double sc = S->rnorm;
+   if (S->pause) return;
+   S->rho = S->rho_new;
+}
+
+// x += scale * d (FP64)
+__global__ void mx_correct(int64_t n, double* x, const float* __restrict__ d, double scale)
+{
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
-      x[i] += sc * (double)d[i];
+      x[i] += scale * (double)d[i];
 }
 
 __global__ void inv_diag32(int64_t n, const int32_t* dpos, const double* val, float* dinv, int* bad)
@@ -176,15 +209,23 @@ __global__ void inv_diag32(int64_t n, const int32_t* dpos, const double* val, fl
    }
 }
 
+__global__ void fill_ones(int64_t n, float* p)
+{
+   int64_t stride = (int64_t)gridDim.x * blockDim.x;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) p[i] = 1.0f;
+}
+
 }  // namespace
 
-void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, const double* b, double* x,
+void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const double* b, double* x,
                  int max_outer, int max_inner, double inner_tol, double tol, int* outer, int* inner,
                  double* true_res)
 {
    OFG_REQUIRE(prec_type == OFG_DIAG || prec_type == OFG_IDENT, OFG_ERR_ARG,
                "mixed-precision inner solver supports DIAG and IDENT");
    OFG_REQUIRE(inner_bits == 32 || inner_bits == 16, OFG_ERR_ARG, "inner_bits must be 32 or 16");
+   OFG_REQUIRE(mode == 0 || mode == 1, OFG_ERR_ARG, "mode must be 0 or 1");
+   OFG_REQUIRE(inner_tol > 0 && inner_tol < 1, OFG_ERR_ARG, "inner_tol must be in (0, 1)");
    const int64_t n = A->n;
    ensure_sell(A);
    ensure_dpos(A);
@@ -199,8 +240,8 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, const double* b, 
    }
    DBuf<float> dinv(n), rr(n), p(n), q(n), d(n);
    DBuf<double> r(n), q64(n);
-   DBuf<IRState> S(1);
-   DBuf<int> stop(1), bad(1);
+   DBuf<MixState> S(1);
+   DBuf<int> bad(1);
    bad.zero();
    DBuf<double> partials((size_t)grid_for(n, kRedBlock, 4) * 4 + 4);
    DBuf<unsigned> counter(1);
@@ -213,62 +254,75 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, const double* b, 
       OFG_REQUIRE(!h, OFG_ERR_PIVOT, "zero diagonal entry");
    }
    else {
-      std::vector<float> ones(n, 1.0f);
-      dinv.upload(ones.data(), n);
+      fill_ones<<<grid_for(n, 256), 256, 0, stream()>>>(n, dinv.p);
+      count_launch();
    }
    const unsigned g = grid_for(n, kRedBlock, 4);
    const unsigned gs = grid_for(A->nslices * 32, kRedBlock, 4);
-   spmv_sell(A, x, q64.p);
-   ir_residual<<<g, kRedBlock, 0, stream()>>>(n, b, q64.p, r.p, S.p, partials.p, counter.p, tol, 1);
-   count_launch();
-   OFG_LAUNCH_CHECK();
-   IRState h{};
-   S.download(&h, 1);
-   int n_outer = 0, n_inner = 0;
-   while (!h.done && n_outer < max_outer) {
-      stop.zero();
-      in_start<<<g, kRedBlock, 0, stream()>>>(n, r.p, dinv.p, rr.p, p.p, d.p, S.p, partials.p,
-                                              counter.p);
-      count_launch();
-      int hs = 0;
-      int batch = 8;
-      for (;;) {
-         // in_start left p = D rr; each step is spmv, update, new direction
-         for (int k = 0; k < batch; ++k) {
-            if (inner_bits == 32)
-               in_spmv<float><<<gs, kRedBlock, 0, stream()>>>(n, A->nslices, A->sell_ptr.p,
-                                                             A->sell_col.p, A->sell_val32.p, p.p,
-                                                             q.p, S.p, partials.p, counter.p,
-                                                             stop.p);
-            else
-               in_spmv<__nv_bfloat16><<<gs, kRedBlock, 0, stream()>>>(
-                  n, A->nslices, A->sell_ptr.p, A->sell_col.p, v16.p, p.p, q.p, S.p, partials.p,
-                  counter.p, stop.p);
-            in_update<<<g, kRedBlock, 0, stream()>>>(n, d.p, p.p, rr.p, q.p, dinv.p, S.p,
-                                                     partials.p, counter.p, inner_tol, max_inner,
-                                                     stop.p);
-            in_direction<<<g, kRedBlock, 0, stream()>>>(n, rr.p, dinv.p, p.p, S.p, stop.p);
-            count_launch(3);
-         }
-         OFG_LAUNCH_CHECK();
-         stop.download(&hs, 1);
-         if (hs) break;
-         batch = std::min(batch * 2, 64);
-      }
-      ir_correct<<<g, kRedBlock, 0, stream()>>>(n, x, d.p, S.p);
-      count_launch();
-      S.download(&h, 1);
-      n_inner += h.it;
-      n_outer++;
+   auto true_residual = [&](int first) {
       spmv_sell(A, x, q64.p);
-      ir_residual<<<g, kRedBlock, 0, stream()>>>(n, b, q64.p, r.p, S.p, partials.p, counter.p, tol,
-                                                 0);
+      mx_residual<<<g, kRedBlock, 0, stream()>>>(n, b, q64.p, r.p, S.p, partials.p, counter.p, tol,
+                                                 first);
       count_launch();
       OFG_LAUNCH_CHECK();
+   };
+   MixState h{};
+   true_residual(1);
+   S.download(&h, 1);
+   int n_outer = 0;
+   // mode 1 solves for d in units of ||r||; mode 0 keeps absolute units
+   double scale = 1.0;
+   bool fresh = true;
+   while (!h.done && n_outer < max_outer && h.it < max_inner) {
+      if (mode == 1) {
+         scale = h.rel * h.bnorm;
+         fresh = true;
+      }
+      mx_load_residual<<<g, kRedBlock, 0, stream()>>>(n, r.p, 1.0 / scale, dinv.p, rr.p, p.p, d.p,
+                                                      fresh ? 1 : 0, S.p, partials.p, counter.p);
+      count_launch();
+      if (!fresh) {
+         mx_direction<<<g, kRedBlock, 0, stream()>>>(n, rr.p, dinv.p, p.p, S.p);
+         mx_rho_shift<<<1, 1, 0, stream()>>>(S.p);
+         count_launch(2);
+      }
+      fresh = false;
+      int batch = 8;
+      for (;;) {
+         for (int k = 0; k < batch; ++k) {
+            int* worked = prof_begin();
+            if (inner_bits == 32)
+               mx_spmv<float><<<gs, kRedBlock, 0, stream()>>>(n, A->nslices, A->sell_ptr.p,
+                                                             A->sell_col.p, A->sell_val32.p, p.p,
+                                                             q.p, S.p, partials.p, counter.p,
+                                                             worked);
+            else
+               mx_spmv<__nv_bfloat16><<<gs, kRedBlock, 0, stream()>>>(
+                  n, A->nslices, A->sell_ptr.p, A->sell_col.p, v16.p, p.p, q.p, S.p, partials.p,
+                  counter.p, worked);
+            prof_end(inner_bits == 32 ? PROF_SPMV32 : PROF_SPMV16,
+                     (inner_bits == 32 ? 8.0 : 6.0) * A->nnz + 12.0 * n + 4.0);
+            mx_update<<<g, kRedBlock, 0, stream()>>>(n, d.p, p.p, rr.p, q.p, dinv.p, S.p,
+                                                     partials.p, counter.p, inner_tol, tol, scale,
+                                                     max_inner, mode);
+            mx_direction<<<g, kRedBlock, 0, stream()>>>(n, rr.p, dinv.p, p.p, S.p);
+            mx_rho_shift<<<1, 1, 0, stream()>>>(S.p);
+            count_launch(4);
+         }
+         OFG_LAUNCH_CHECK();
+         S.download(&h, 1);
+         if (h.pause) break;
+         batch = std::min(batch * 2, 64);
+      }
+      // refinement step in FP64
+      mx_correct<<<g, kRedBlock, 0, stream()>>>(n, x, d.p, scale);
+      count_launch();
+      true_residual(0);
       S.download(&h, 1);
+      n_outer++;
    }
    *outer = n_outer;
-   *inner = n_inner;
+   *inner = h.it;
    *true_res = h.rel;
 }
 
@@ -276,16 +330,17 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, const double* b, 
 
 using namespace ofg;
 
-extern "C" int ofg_solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, const double* b,
-                               double* x, int max_outer, int max_inner, double inner_tol,
-                               double toler, int* outer, int* inner, double* true_res)
+extern "C" int ofg_solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode,
+                               const double* b, double* x, int max_outer, int max_inner,
+                               double inner_tol, double toler, int* outer, int* inner,
+                               double* true_res)
 {
    return guarded("ofg_solve_mixed", [&] {
       OFG_REQUIRE(A && b && x && outer && inner && true_res, OFG_ERR_ARG, "null argument");
       In<double> db(b, A->n);
       InOut<double> dx(x, A->n, true);
-      solve_mixed(A, prec_type, inner_bits, db.d, dx.d, max_outer, max_inner, inner_tol, toler,
-                  outer, inner, true_res);
+      solve_mixed(A, prec_type, inner_bits, mode, db.d, dx.d, max_outer, max_inner, inner_tol,
+                  toler, outer, inner, true_res);
       dx.finish();
    });
 }

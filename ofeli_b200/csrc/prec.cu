@@ -58,6 +58,7 @@ struct SweepArgs {
    int* ticket;            // [0] next strand, [1] finished strands
    int* status;
    const int* skip;        // optional: the whole launch is a no-op while *skip != 0
+   int* worked;            // profiling flag
 };
 
 __device__ __forceinline__ bool is_sentinel(double v)
@@ -112,6 +113,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) sweep_kernel(SweepArgs g)
    const unsigned FULL = 0xffffffffu;
    const int64_t n = g.n;
    if (g.skip && *g.skip) return;
+   prof_mark(g.worked);
 
    for (;;) {
       int s = 0;
@@ -400,7 +402,9 @@ void launch_sweep(ofg_prec* P, SweepPlan& plan, SweepArgs g)
    int blocks = (int)std::min<int64_t>((plan.nstrands + kWarpsPerBlock - 1) / kWarpsPerBlock,
                                        (int64_t)P->grid);
    if (blocks < 1) blocks = 1;
+   g.worked = prof_begin();
    sweep_kernel<MODE><<<blocks, kWarpsPerBlock * 32, 0, stream()>>>(g);
+   prof_end(PROF_SWEEP, 0.0);
    count_launch();
    OFG_LAUNCH_CHECK();
 }

@@ -260,14 +260,15 @@ def GMRes(A, P, b, x, m, max_it, toler):
     return res.value
 
 
-def solve_mixed(A, b, x, prec=DIAG_PREC, inner_bits=32, toler=1e-10, max_outer=50,
-                max_inner=100000, inner_tol=1e-4):
-    """FP64 iterative refinement around an FP32 (or BF16-matrix) PCG.
-    Returns (outer steps, inner iterations, FP64 true relative residual)."""
+def solve_mixed(A, b, x, prec=DIAG_PREC, inner_bits=32, toler=1e-10, max_outer=200,
+                max_inner=1000000, inner_tol=0.05, mode=0):
+    """FP64 iterative refinement around an FP32 (or BF16-matrix) PCG; mode 0
+    keeps the CG direction across refinements, mode 1 restarts the inner CG.
+    Returns (refinement steps, inner iterations, FP64 true relative residual)."""
     b = _f64(b, A.n)
     o, i, r = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
-    _call("ofg_solve_mixed", A._h, prec, inner_bits, _ptr(b), _ptr(x), max_outer, max_inner,
-          inner_tol, toler, ctypes.byref(o), ctypes.byref(i), ctypes.byref(r))
+    _call("ofg_solve_mixed", A._h, prec, inner_bits, mode, _ptr(b), _ptr(x), max_outer,
+          max_inner, inner_tol, toler, ctypes.byref(o), ctypes.byref(i), ctypes.byref(r))
     return o.value, i.value, r.value
 
 

@@ -162,6 +162,33 @@ class KLaplace2DT3 : public Laplace2DT3 {
    size_t neq() const { return _nb_eq; }
 };
 
+// The same element with the setup of Equation(mesh,u) (Equation_impl.h
+// :75-85,111-122) done by hand, so that the matrix graph is built once (by
+// setSolver) instead of three times: Equa::setMesh (Equa.cpp:334-348) would
+// build SpMatrix(mesh) twice before the caller's setSolver builds it again.
+class BenchLaplace2DT3 : public Laplace2DT3 {
+ public:
+   BenchLaplace2DT3(Mesh& ms, Vect<real_t>& u) : Equation<3,3,2,2>(), Laplace2DT3()
+   {
+      _theMesh = &ms;
+      _theMesh->removeImposedDOF();
+      _nb_nodes = ms.getNbNodes();
+      _nb_sides = ms.getNbSides();
+      _nb_boundary_sides = ms.getNbBoundarySides();
+      _nb_el = ms.getNbElements();
+      _nb_dof_total = ms.getNbDOF();
+      _nb_eq = ms.getNbEq();
+      _nb_dof = 1;
+      _b = new Vect<real_t>(_nb_eq);
+      _uu.setSize(_nb_eq);
+      _u = &u;
+   }
+   Matrix<real_t>* mat() { return _A; }
+   Vect<real_t>* rhs() { return _b; }
+   Vect<real_t>& sol() { return _uu; }
+   size_t neq() const { return _nb_eq; }
+};
+
 // --- 3-D P1 diffusion (DC3DT4) with a per-element conductivity -------------
 class KDC3DT4 : public DC3DT4 {
  public:
@@ -301,6 +328,66 @@ int run_p2d(int argc, char** argv)
    info.set("norm_u", u.getNorm2());
    info.sets("solver", solver);
    info.sets("prec", argv[5]);
+   info.write(out);
+   return 0;
+}
+
+// Timed CPU baseline: graph once, then NSTEPS steps of {build, Prec, ITERS CG
+// iterations}; the caller extrapolates the per-iteration time to a full solve.
+int run_bench2d(int argc, char** argv)
+{
+   if (argc < 8) return 2;
+   size_t nx = std::stoul(argv[2]);
+   Preconditioner prec = parse_prec(argv[3]);
+   int iters = std::stoi(argv[4]);
+   int nsteps = std::stoi(argv[5]);
+   std::string in = argv[6], out = argv[7];
+   Info info;
+   double t0 = now_s();
+   Mesh ms(0., 1., 0., 1., nx, nx, 1, 1, 1, 1, TRIANGLE);
+   size_t nn = ms.getNbNodes();
+   double t_mesh = now_s() - t0;
+   std::vector<double> fv = read_f64(in + "/f.f64", nn);
+   Vect<real_t> u(ms), f(ms), bc(ms);
+   for (size_t i = 0; i < nn; ++i) f[i] = fv[i];
+   bc = 0;
+   BenchLaplace2DT3 eq(ms, u);
+   double t1 = now_s();
+   eq.setSolver(CG_SOLVER, prec);
+   double t_graph = now_s() - t1;
+   eq.setSource(f);
+   eq.setDirichlet(bc);
+   std::string sa, sp, si;
+   int it = 0;
+   for (int s = 0; s < nsteps; ++s) {
+      Vect<real_t>& b = *eq.rhs();
+      b.clear();
+      eq.sol().setSize(eq.neq());
+      eq.sol() = 0;
+      double ta = now_s();
+      eq.build();
+      double t_asm = now_s() - ta;
+      SpMatrix<real_t>& A = *dynamic_cast<SpMatrix<real_t>*>(eq.mat());
+      double tp = now_s();
+      Prec<real_t> P(A, prec);
+      double t_prec = now_s() - tp;
+      double tc = now_s();
+      it = CG(A, P, b, eq.sol(), iters, 1e-300);
+      double t_it = now_s() - tc;
+      char buf[96];
+      snprintf(buf, sizeof buf, "%s%.6f", s ? "," : "", t_asm); sa += buf;
+      snprintf(buf, sizeof buf, "%s%.6f", s ? "," : "", t_prec); sp += buf;
+      snprintf(buf, sizeof buf, "%s%.6f", s ? "," : "", t_it); si += buf;
+   }
+   info.seti("nodes", (long long)nn);
+   info.seti("n", (long long)eq.neq());
+   info.seti("iters", it);
+   info.set("t_mesh", t_mesh);
+   info.set("t_graph", t_graph);
+   info.sets("t_assembly_steps", sa);
+   info.sets("t_prec_steps", sp);
+   info.sets("t_iters_steps", si);
+   info.seti("iters_per_step", iters);
    info.write(out);
    return 0;
 }
@@ -467,6 +554,7 @@ int main(int argc, char** argv)
       if (mode == "p2d") return run_p2d(argc, argv);
       if (mode == "p3d") return run_p3d(argc, argv);
       if (mode == "cd2d") return run_cd2d(argc, argv);
+      if (mode == "bench2d") return run_bench2d(argc, argv);
    }
    catch (std::exception& e) {
       fprintf(stderr, "OFELI exception: %s\n", e.what());
