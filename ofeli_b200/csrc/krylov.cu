@@ -375,7 +375,7 @@ __global__ void __launch_bounds__(kRedBlock) res_kernel(int64_t n, const double*
    }
 }
 
-unsigned red_grid(int64_t n) { return grid_for(n, kRedBlock, 4); }
+unsigned red_grid(int64_t n) { return grid_for(n, kRedBlock, 8); }
 
 // Scratch of one Krylov call: reduction partials, counter, state.
 struct RedScratch {
@@ -383,7 +383,7 @@ struct RedScratch {
    DBuf<unsigned> counter;
    explicit RedScratch(int64_t n)
    {
-      partials.alloc((size_t)red_grid(n) * 4 + 4);
+      partials.alloc(((size_t)red_grid(n) + 1) * 4 + 4);
       counter.alloc(1);
       counter.zero();
    }
@@ -398,7 +398,7 @@ void cg_iteration(ofg_prec* P, int64_t n, double* x, double* r, double* p, doubl
    if (PT == PT_SWEEP) prec_apply_device(P, r, z, &S->rho, &S->done);
    cg_direction<PT><<<g, kRedBlock, 0, stream()>>>(n, r, P->pivot.p, z, p, S);
    int* worked = prof_begin();
-   cg_spmv<<<grid_for(A->nslices * 32, kRedBlock, 4), kRedBlock, 0, stream()>>>(
+   cg_spmv<<<grid_for(A->nslices * 32, kRedBlock, 8), kRedBlock, 0, stream()>>>(
       n, A->nslices, A->sell_ptr.p, A->sell_col.p, A->sell_val.p, p, q, S, rs.partials.p,
       rs.counter.p, worked);
    prof_end(PROF_SPMV64, 12.0 * A->nnz + 20.0 * A->n + 4.0);

@@ -243,7 +243,7 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
    DBuf<MixState> S(1);
    DBuf<int> bad(1);
    bad.zero();
-   DBuf<double> partials((size_t)grid_for(n, kRedBlock, 4) * 4 + 4);
+   DBuf<double> partials(((size_t)grid_for(n, kRedBlock, 8) + 1) * 4 + 4);
    DBuf<unsigned> counter(1);
    counter.zero();
    if (prec_type == OFG_DIAG) {
@@ -257,8 +257,8 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
       fill_ones<<<grid_for(n, 256), 256, 0, stream()>>>(n, dinv.p);
       count_launch();
    }
-   const unsigned g = grid_for(n, kRedBlock, 4);
-   const unsigned gs = grid_for(A->nslices * 32, kRedBlock, 4);
+   const unsigned g = grid_for(n, kRedBlock, 8);
+   const unsigned gs = grid_for(A->nslices * 32, kRedBlock, 8);
    auto true_residual = [&](int first) {
       spmv_sell(A, x, q64.p);
       mx_residual<<<g, kRedBlock, 0, stream()>>>(n, b, q64.p, r.p, S.p, partials.p, counter.p, tol,

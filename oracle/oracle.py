@@ -198,9 +198,10 @@ def read_info(outdir):
     return info
 
 
-def run_reference(args, inputs, flavour="o2", keep=None, timeout=None):
-    """Runs ofeli_ref with the given argument list (INDIR / OUTDIR appended)
-    and returns (info, outputs) with outputs loaded as numpy arrays."""
+def run_reference(args, inputs, flavour="o2", keep=None, timeout=None, extra=()):
+    """Runs ofeli_ref with the given argument list (INDIR / OUTDIR appended,
+    then `extra`) and returns (info, outputs) with outputs loaded as numpy
+    arrays."""
     tmp = keep or tempfile.mkdtemp(prefix="ofeli_ref_")
     indir, outdir = os.path.join(tmp, "in"), os.path.join(tmp, "out")
     os.makedirs(indir, exist_ok=True)
@@ -209,7 +210,7 @@ def run_reference(args, inputs, flavour="o2", keep=None, timeout=None):
         np.ascontiguousarray(arr, dtype=np.float64).tofile(os.path.join(indir, name + ".f64"))
     env = dict(os.environ)
     env["OFELI_PATH_MATERIAL"] = os.path.join(REF_DIR, "material")
-    cmd = [ref_binary(flavour)] + [str(a) for a in args] + [indir, outdir]
+    cmd = [ref_binary(flavour)] + [str(a) for a in args] + [indir, outdir] + [str(e) for e in extra]
     subprocess.run(cmd, check=True, env=env, timeout=timeout)
     info = read_info(outdir)
     out = {}

@@ -276,8 +276,14 @@ int run_p2d(int argc, char** argv)
    std::string in = argv[8], out = argv[9];
    Info info;
 
+   // optional boundary line codes cx0 cxN cy0 cyN after OUTDIR
+   int cx0 = 1, cxN = 1, cy0 = 1, cyN = 1;
+   if (argc >= 14) {
+      cx0 = std::stoi(argv[10]); cxN = std::stoi(argv[11]);
+      cy0 = std::stoi(argv[12]); cyN = std::stoi(argv[13]);
+   }
    double t0 = now_s();
-   Mesh ms(0., 1., 0., 1., nx, ny, 1, 1, 1, 1, TRIANGLE);
+   Mesh ms(0., 1., 0., 1., nx, ny, cx0, cxN, cy0, cyN, TRIANGLE);
    size_t nn = ms.getNbNodes(), ne = ms.getNbElements();
    if (file_exists(in + "/xy.f64")) {
       std::vector<double> xy = read_f64(in + "/xy.f64", 2 * nn);
@@ -294,6 +300,10 @@ int run_p2d(int argc, char** argv)
    Vect<real_t> u(ms), f(ms), bc(ms);
    for (size_t i = 0; i < nn; ++i) f[i] = fv[i];
    bc = 0;
+   if (file_exists(in + "/bc.f64")) {
+      std::vector<double> bv = read_f64(in + "/bc.f64", nn);
+      for (size_t i = 0; i < nn; ++i) bc[i] = bv[i];
+   }
    KLaplace2DT3 eq(ms, u);
    if (!kv.empty()) eq.k = kv.data();
    double t1 = now_s();

@@ -1,0 +1,150 @@
+"""Edge cases of the CUDA path: empty systems, zero right-hand sides,
+iteration caps, errors OFELI raises as exceptions, device-resident inputs,
+determinism."""
+import numpy as np
+import pytest
+
+from conftest import load_golden, rel_err
+from ofeli_b200 import capi, fields
+from ofeli_b200 import ofeli as F
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def small_system(nx=16, ny=11, seed=3):
+    xy, elem, code = O.mesh2d(nx, ny)
+    dof, n = O.number_equations(code)
+    rp, ci = O.node_graph(elem, 3, dof, n)
+    f = fields.uniform_pm1(seed, code.size)
+    a, b = O.assemble(2, xy, elem, dof, code, n, rp, ci, f=f, bc=np.zeros(code.size))
+    return rp, ci, a, b
+
+
+def test_mesh_without_unknowns(cuda):
+    # a single cell: every node is on the boundary, no equation
+    mesh = F.Mesh(0.0, 1.0, 0.0, 1.0, 1, 1)
+    assert mesh.neq == 0 and mesh.nn == 4 and mesh.ne == 2
+    eq = F.Laplace2DT3(mesh)
+    eq.setSolver(F.CG_SOLVER, F.DIAG_PREC)
+    eq.setSource(np.ones(4))
+    eq.setDirichlet(np.arange(4.0))
+    assert eq.run() == 0
+    assert np.array_equal(eq.u, np.arange(4.0))
+
+
+def test_zero_rhs_returns_zero_iterations(cuda):
+    rp, ci, a, b = small_system()
+    A = F.SpMatrix(rp, ci, a)
+    x = np.zeros(A.n)
+    for pt in (F.DIAG_PREC, F.ILU_PREC, F.SSOR_PREC):
+        assert F.CG(A, F.Prec(A, pt), np.zeros(A.n), x, 100, 1e-10) == 0
+        assert not x.any()
+    # GMRes reports it = 1 at its initial convergence test (GMRes.h:176-179)
+    assert F.GMRes(A, F.Prec(A, F.ILU_PREC), np.zeros(A.n), x, 10, 100, 1e-10) == 1
+
+
+@pytest.mark.parametrize("pt", [O.DIAG, O.ILU, O.SSOR])
+def test_iteration_cap_matches_oracle(cuda, pt):
+    rp, ci, a, b = small_system()
+    A = F.SpMatrix(rp, ci, a)
+    x0, it0 = O.cg(rp, ci, a, b, pt, 7, 1e-14)
+    x = np.zeros(A.n)
+    it = F.CG(A, F.Prec(A, pt), b, x, 7, 1e-14)
+    assert it == it0 == -8  # OFELI returns -(max_it+1) when the loop runs out
+    assert rel_err(x, x0) <= 1e-12
+    xg0, itg0 = O.gmres(rp, ci, a, b, pt, 4, 10, 1e-14)
+    xg = np.zeros(A.n)
+    itg = F.GMRes(A, F.Prec(A, pt), b, xg, 4, 10, 1e-14)
+    assert itg == itg0 < 0
+    assert rel_err(xg, xg0) <= 1e-12
+
+
+def test_initial_guess_is_used(cuda):
+    rp, ci, a, b = small_system()
+    A = F.SpMatrix(rp, ci, a)
+    xs = fields.uniform_pm1(8, A.n)
+    x0, it0 = O.cg(rp, ci, a, b, O.ILU, 500, 1e-10, x0=xs)
+    x = xs.copy()
+    it = F.CG(A, F.Prec(A, F.ILU_PREC), b, x, 500, 1e-10)
+    assert it == it0 and rel_err(x, x0) <= 1e-12
+
+
+def test_zero_pivot_raises(cuda):
+    rp, ci, a, b = small_system()
+    a = a.copy()
+    d = next(k for k in range(rp[0], rp[1]) if ci[k] == 1)
+    a[d] = 0.0
+    A = F.SpMatrix(rp, ci, a)
+    for pt in (F.DIAG_PREC, F.ILU_PREC, F.SSOR_PREC):
+        with pytest.raises(F.OFELIException, match="pivot"):
+            F.Prec(A, pt)
+
+
+def test_missing_diagonal_raises(cuda):
+    rp = np.array([0, 1, 2], dtype=np.int64)
+    ci = np.array([2, 1], dtype=np.int64)  # row 1 has only column 2
+    A = F.SpMatrix(rp, ci, np.array([1.0, 1.0]))
+    with pytest.raises(F.OFELIException):
+        F.Prec(A, F.ILU_PREC)
+
+
+def test_bad_pattern_raises(cuda):
+    with pytest.raises(F.OFELIException, match="col_ind"):
+        F.SpMatrix(np.array([0, 1, 2]), np.array([1, 3]))
+    with pytest.raises(F.OFELIException, match="row_ptr"):
+        F.SpMatrix(np.array([0, 2, 1]), np.array([1, 2]))
+
+
+def test_inverted_element_raises(cuda):
+    # Triang3 throws on a negative Jacobian; so does the assembly here
+    coords = np.array([0, 0, 1, 0, 0, 1, 1, 1.0])
+    elem = np.array([0, 1, 2, 1, 2, 3], dtype=np.int32)  # second triangle is clockwise
+    code = np.array([1, 1, 1, 0], dtype=np.int32)
+    mesh = F.Mesh.from_arrays(2, coords, elem, code)
+    eq = F.Laplace2DT3(mesh)
+    eq.setSolver(F.CG_SOLVER, F.DIAG_PREC)
+    with pytest.raises(F.OFELIException, match="Jacobian"):
+        eq.build()
+
+
+def test_general_mesh_equals_structured(cuda):
+    xy, elem, code = O.mesh2d(9, 7)
+    m1 = F.Mesh(0.0, 1.0, 0.0, 1.0, 9, 7)
+    m2 = F.Mesh.from_arrays(2, xy, elem, code)
+    assert F.SpMatrix(m1).pattern()[1].tolist() == F.SpMatrix(m2).pattern()[1].tolist()
+
+
+def test_device_tensors_and_determinism(cuda):
+    import torch
+    g, info = load_golden("p2d_65")
+    A = F.SpMatrix(g["row_ptr"], g["col_ind"], g["a"])
+    b = torch.from_numpy(g["b"]).to(cuda)
+    outs = []
+    for _ in range(2):
+        x = torch.zeros(A.n, dtype=torch.float64, device=cuda)
+        it = F.CG(A, F.Prec(A, F.ILU_PREC), b, x, 5000, 1e-10)
+        torch.cuda.synchronize()
+        outs.append(x.cpu().numpy())
+        assert it == info["runs"]["CG_DILU"]["iters"]
+    assert np.array_equal(outs[0], outs[1])  # bitwise reproducible
+    assert rel_err(outs[0], g["x_CG_DILU"]) <= 1e-12
+
+
+def test_values_update_refactorises(cuda):
+    rp, ci, a, b = small_system()
+    A = F.SpMatrix(rp, ci, a)
+    P = F.Prec(A, F.ILU_PREC)
+    A.set_values(2.0 * a)
+    x = np.zeros(A.n)
+    x0, it0 = O.cg(rp, ci, 2.0 * a, b, O.ILU, 500, 1e-10)
+    it = F.CG(A, P, b, x, 500, 1e-10)
+    assert it == it0 and rel_err(x, x0) <= 1e-12
+
+
+def test_kernels_are_launched(cuda):
+    before = capi.launch_count()
+    rp, ci, a, b = small_system()
+    A = F.SpMatrix(rp, ci, a)
+    F.CG(A, F.Prec(A, F.ILU_PREC), b, np.zeros(A.n), 100, 1e-10)
+    assert capi.launch_count() - before > 10

@@ -1,0 +1,99 @@
+"""Full-size checks at the benchmark configuration (2049x2049 nodes, 4.19M
+unknowns, 29.3M nonzeros) and the 3-D one (129^3 Kuhn cube): the pattern
+bit-exact against the oracle's NodeGraph, values / SpMV / preconditioner
+applications against the oracle, linearity, and the FP64 accuracy of the
+solves."""
+import numpy as np
+import pytest
+
+from conftest import rel_err
+from ofeli_b200 import fields
+from ofeli_b200 import ofeli as F
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+NX = 2048
+
+
+@pytest.fixture(scope="module")
+def big(cuda):
+    xy, elem, code = O.mesh2d(NX, NX)
+    dof, n = O.number_equations(code)
+    rp, ci = O.node_graph(elem, 3, dof, n)
+    f = fields.uniform_pm1(1234, code.size)
+    a, b = O.assemble(2, xy, elem, dof, code, n, rp, ci, f=f, bc=np.zeros(code.size))
+    mesh = F.Mesh(0.0, 1.0, 0.0, 1.0, NX, NX)
+    eq = F.Laplace2DT3(mesh)
+    eq.setSolver(F.CG_SOLVER, F.DIAG_PREC)
+    eq.setSource(f)
+    eq.setDirichlet(np.zeros(mesh.nn))
+    eq.build()
+    return dict(rp=rp, ci=ci, a=a, b=b, eq=eq, A=eq.getMatrix(), n=n)
+
+
+def test_bench_config_sizes(big):
+    assert big["n"] == 4190209 and big["A"].nnz == 29315089
+
+
+def test_pattern_and_values_full_size(big):
+    rp, ci = big["A"].pattern()
+    assert np.array_equal(rp, big["rp"]) and np.array_equal(ci, big["ci"])
+    assert rel_err(big["A"].values(), big["a"]) <= 1e-12
+    assert rel_err(big["eq"].getRHS(), big["b"]) <= 1e-12
+
+
+def test_spmv_and_linearity_full_size(big):
+    A = big["A"]
+    x = fields.uniform_pm1(1, A.n)
+    y = fields.uniform_pm1(2, A.n)
+    Ax = A.Mult(x)
+    assert rel_err(Ax, O.spmv(big["rp"], big["ci"], big["a"], x)) <= 1e-14
+    lhs = A.Mult(2.5 * x + y)
+    assert rel_err(lhs, 2.5 * Ax + A.Mult(y)) <= 1e-13
+
+
+def test_dilu_full_size(big):
+    A = big["A"]
+    idv, piv = O.prec_setup(O.ILU, big["rp"], big["ci"], big["a"])
+    P = F.Prec(A, F.ILU_PREC)
+    assert np.array_equal(P.getPivot(), piv)
+    r = fields.uniform_pm1(4, A.n)
+    assert rel_err(P.solve(r), O.prec_apply(O.ILU, big["rp"], big["ci"], big["a"], idv, piv, r)) <= 1e-12
+
+
+def test_mixed_solve_full_size(big):
+    A = big["A"]
+    x = np.zeros(A.n)
+    outer, inner, res = F.solve_mixed(A, big["b"], x, prec=F.DIAG_PREC, inner_bits=32, toler=1e-10)
+    assert res <= 1e-10 and F.residual(A, big["b"], x) <= 1e-10
+    x64 = np.zeros(A.n)
+    it = F.CG(A, F.Prec(A, F.DIAG_PREC), big["b"], x64, 100000, 1e-10)
+    assert it > 0 and F.residual(A, big["b"], x64) <= 1.01e-10
+    # both solutions meet the same residual bound; they agree to the
+    # conditioning-limited accuracy of that bound
+    assert rel_err(x, x64) <= 1e-5
+
+
+def test_kuhn_129_pattern_and_values(cuda):
+    M = 128
+    xyz, elem, code = O.mesh3d(M)
+    dof, n = O.number_equations(code)
+    assert n == 2048383
+    rp, ci = O.node_graph(elem, 4, dof, n)
+    assert rp[-1] == 30340171
+    cent = xyz.reshape(-1, 3)[elem.reshape(-1, 4)].mean(axis=1)
+    k = fields.lognormal_k(3, cent, 1.5, 0.1, grid=64)
+    f = fields.uniform_pm1(3, code.size)
+    a, b = O.assemble(3, xyz, elem, dof, code, n, rp, ci, k=k, f=f, bc=np.zeros(code.size))
+    mesh = F.Mesh.kuhn(M)
+    eq = F.DC3DT4(mesh)
+    eq.setSolver(F.CG_SOLVER, F.ILU_PREC)
+    eq.setSource(f)
+    eq.setDirichlet(np.zeros(mesh.nn))
+    eq.setElementCoefficient(k)
+    eq.build()
+    A = eq.getMatrix()
+    rp2, ci2 = A.pattern()
+    assert np.array_equal(rp2, rp) and np.array_equal(ci2, ci)
+    assert rel_err(A.values(), a) <= 1e-12 and rel_err(eq.getRHS(), b) <= 1e-12

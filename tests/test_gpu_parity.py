@@ -1,0 +1,261 @@
+"""Parity of the CUDA path (through the C ABI) with the reference OFELI's
+golden vectors (tests/golden, produced by OFELI itself) and with the oracle.
+
+Bars: CSR pattern bit-exact; assembled values, RHS and solutions within
+1e-12 relative (max-norm, relative to the reference's max entry); iteration
+counts within +-2 of the reference's (they come out equal); D-ILU pivots
+bit-exact (the factorisation keeps the reference's operation order)."""
+import numpy as np
+import pytest
+
+from conftest import load_golden, rel_err
+from ofeli_b200 import fields
+from ofeli_b200 import ofeli as F
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+VAL_TOL = 1e-12
+SOL_TOL = 1e-12
+IT_TOL = 2
+PRECS = {"IDENT": F.IDENT_PREC, "DIAG": F.DIAG_PREC, "DILU": F.DILU_PREC, "ILU": F.ILU_PREC,
+         "SSOR": F.SSOR_PREC}
+
+
+def centroids(coords, elem, dim):
+    return coords.reshape(-1, dim)[elem.reshape(-1, dim + 1)].mean(axis=1)
+
+
+@pytest.fixture(scope="module")
+def p2d65(cuda):
+    g, info = load_golden("p2d_65")
+    mesh = F.Mesh(0.0, 1.0, 0.0, 1.0, 64, 64, 1, 1, 1, 1)
+    eq = F.Laplace2DT3(mesh)
+    eq.setSolver(F.CG_SOLVER, F.DIAG_PREC)
+    eq.setSource(fields.uniform_pm1(1234, mesh.nn))
+    eq.setDirichlet(np.zeros(mesh.nn))
+    eq.build()
+    return g, info, mesh, eq
+
+
+def test_mesh_matches_reference_generator(p2d65):
+    _, _, mesh, _ = p2d65
+    xy, elem, code = O.mesh2d(64, 64)
+    c2, e2, code2, dof2 = mesh.arrays()
+    assert np.array_equal(c2, xy)  # coordinates accumulated as the reference does
+    assert np.array_equal(e2, elem) and np.array_equal(code2, code)
+    dof, n = O.number_equations(code)
+    assert np.array_equal(dof2, dof) and mesh.neq == n == 3969
+
+
+def test_pattern_bit_exact(p2d65):
+    g, info, _, eq = p2d65
+    rp, ci = eq.getMatrix().pattern()
+    assert np.array_equal(rp, g["row_ptr"]) and np.array_equal(ci, g["col_ind"])
+    assert eq.getMatrix().nnz == info["nnz"] == 27281
+
+
+def test_assembly_matches_reference(p2d65):
+    g, _, _, eq = p2d65
+    assert rel_err(eq.getMatrix().values(), g["a"]) <= VAL_TOL
+    assert rel_err(eq.getRHS(), g["b"]) <= VAL_TOL
+
+
+@pytest.mark.parametrize("key", ["CG_IDENT", "CG_DIAG", "CG_DILU", "CG_SSOR"])
+def test_cg_matches_reference(p2d65, key):
+    g, info, _, eq = p2d65
+    prec = key.split("_")[1]
+    A = eq.getMatrix()
+    x = np.zeros(A.n)
+    it = F.CG(A, F.Prec(A, PRECS[prec]), g["b"], x, 20000, 1e-10)
+    assert abs(it - info["runs"][key]["iters"]) <= IT_TOL
+    assert rel_err(x, g["x_" + key]) <= SOL_TOL
+
+
+def test_ilu_equals_dilu(p2d65):
+    g, info, _, eq = p2d65
+    A = eq.getMatrix()
+    x1, x2 = np.zeros(A.n), np.zeros(A.n)
+    i1 = F.CG(A, F.Prec(A, F.ILU_PREC), g["b"], x1, 20000, 1e-10)
+    i2 = F.CG(A, F.Prec(A, F.DILU_PREC), g["b"], x2, 20000, 1e-10)
+    assert i1 == i2 == info["runs"]["CG_DILU"]["iters"]
+    assert np.array_equal(x1, x2)
+
+
+@pytest.mark.parametrize("key", ["GMRES30_ILU", "GMRES30_DIAG", "GMRES10_SSOR"])
+def test_gmres_matches_reference(p2d65, key):
+    g, info, _, eq = p2d65
+    solver, prec = key.split("_")
+    A = eq.getMatrix()
+    x = np.zeros(A.n)
+    it = F.GMRes(A, F.Prec(A, PRECS[prec]), g["b"], x, int(solver[5:]), 20000, 1e-10)
+    assert abs(it - info["runs"][key]["iters"]) <= IT_TOL
+    assert rel_err(x, g["x_" + key]) <= SOL_TOL
+
+
+def test_cg_residual_history_matches_oracle(p2d65):
+    g, _, _, eq = p2d65
+    A = eq.getMatrix()
+    rp, ci = g["row_ptr"].astype(np.int64), g["col_ind"].astype(np.int64)
+    _, it0, h0 = O.cg(rp, ci, g["a"], g["b"], O.ILU, 200, 1e-10, history=True)
+    x = np.zeros(A.n)
+    it, h = F.CG(A, F.Prec(A, F.ILU_PREC), g["b"], x, 200, 1e-10, history=True)
+    assert it == it0
+    assert np.abs(h[1:it + 1] / h0[1:it0 + 1] - 1).max() < 1e-9
+
+
+def test_pivots_bit_exact(p2d65):
+    g, _, _, eq = p2d65
+    A = eq.getMatrix()
+    rp, ci = g["row_ptr"].astype(np.int64), g["col_ind"].astype(np.int64)
+    for pt in (O.DIAG, O.DILU, O.SSOR):
+        _, piv = O.prec_setup(pt, rp, ci, g["a"])
+        assert np.array_equal(F.Prec(A, pt).getPivot(), piv)
+
+
+def test_prec_apply_matches_oracle(p2d65):
+    g, _, _, eq = p2d65
+    A = eq.getMatrix()
+    rp, ci = g["row_ptr"].astype(np.int64), g["col_ind"].astype(np.int64)
+    r = fields.uniform_pm1(77, A.n)
+    for pt in (O.DIAG, O.DILU, O.SSOR):
+        idv, piv = O.prec_setup(pt, rp, ci, g["a"])
+        z0 = O.prec_apply(pt, rp, ci, g["a"], idv, piv, r)
+        P = F.Prec(A, pt)
+        z1 = P.solve(r)
+        z2 = P.solve(r)  # buffers are reusable
+        assert rel_err(z1, z0) <= 1e-13 and np.array_equal(z1, z2)
+
+
+def test_spmv_matches_oracle(p2d65):
+    g, _, _, eq = p2d65
+    A = eq.getMatrix()
+    rp, ci = g["row_ptr"].astype(np.int64), g["col_ind"].astype(np.int64)
+    x = fields.uniform_pm1(5, A.n)
+    y0 = O.spmv(rp, ci, g["a"], x)
+    assert rel_err(A.Mult(x), y0) <= 1e-14
+    y = np.ones(A.n)
+    assert rel_err(A.MultAdd(x, y), y0 + 1.0) <= 1e-14
+
+
+def test_jittered_variable_k():
+    g, info = load_golden("p2d_jitter_25")
+    nx = info["nx"]
+    xy, elem, code = O.mesh2d(nx, nx)
+    xyj = fields.jitter_2d(5, xy, code, nx, nx)
+    k = fields.lognormal_k(5, centroids(xyj, elem, 2), 1.0, 0.1, grid=128)
+    mesh = F.Mesh(0.0, 1.0, 0.0, 1.0, nx, nx)
+    mesh.setCoords(xyj)
+    eq = F.Laplace2DT3(mesh)
+    eq.setSolver(F.CG_SOLVER, F.ILU_PREC)
+    eq.setSource(fields.uniform_pm1(5, mesh.nn))
+    eq.setDirichlet(np.zeros(mesh.nn))
+    eq.setElementCoefficient(k)
+    eq.getLinearSolver().setTolerance(1e-10)
+    eq.getLinearSolver().setMaxIter(20000)
+    ret = eq.run()
+    A = eq.getMatrix()
+    rp, ci = A.pattern()
+    assert ret == 0
+    assert np.array_equal(rp, g["row_ptr"]) and np.array_equal(ci, g["col_ind"])
+    assert rel_err(A.values(), g["a"]) <= VAL_TOL and rel_err(eq.getRHS(), g["b"]) <= VAL_TOL
+    assert rel_err(eq.x, g["x"]) <= SOL_TOL and rel_err(eq.u, g["u"]) <= SOL_TOL
+    assert abs(eq.getLinearSolver().getNbIter() - info["iters"]) <= IT_TOL
+
+
+def test_ragged_mesh_with_imposed_values():
+    g, info = load_golden("p2d_ragged")
+    mesh = F.Mesh(0.0, 1.0, 0.0, 1.0, info["nx"], info["ny"], *info["codes"])
+    xy = mesh.arrays()[0].reshape(-1, 2)
+    bc = 1.0 + xy[:, 0] + 2.0 * xy[:, 1]
+    eq = F.Laplace2DT3(mesh)
+    eq.setSolver(F.CG_SOLVER, F.DIAG_PREC)
+    eq.getLinearSolver().setTolerance(1e-10)
+    eq.getLinearSolver().setMaxIter(20000)
+    eq.setSource(fields.uniform_pm1(9, mesh.nn))
+    eq.setDirichlet(bc)
+    eq.run()
+    A = eq.getMatrix()
+    rp, ci = A.pattern()
+    assert np.array_equal(rp, g["row_ptr"]) and np.array_equal(ci, g["col_ind"])
+    assert rel_err(A.values(), g["a"]) <= VAL_TOL and rel_err(eq.getRHS(), g["b"]) <= VAL_TOL
+    assert rel_err(eq.u, g["u"]) <= SOL_TOL
+    assert abs(eq.getLinearSolver().getNbIter() - info["iters"]) <= IT_TOL
+
+
+def test_kuhn_3d_variable_k():
+    g, info = load_golden("p3d_kuhn_9")
+    M = info["M"]
+    xyz, elem, code = O.mesh3d(M)
+    k = fields.lognormal_k(7, centroids(xyz, elem, 3), 1.5, 0.1, grid=32)
+    mesh = F.Mesh.kuhn(M)
+    c2, e2, code2, _ = mesh.arrays()
+    assert np.array_equal(c2, xyz) and np.array_equal(e2, elem) and np.array_equal(code2, code)
+    eq = F.DC3DT4(mesh)
+    eq.setSolver(F.CG_SOLVER, F.ILU_PREC)
+    eq.setSource(fields.uniform_pm1(99, mesh.nn))
+    eq.setDirichlet(np.zeros(mesh.nn))
+    eq.setElementCoefficient(k)
+    eq.build()
+    A = eq.getMatrix()
+    rp, ci = A.pattern()
+    assert np.array_equal(rp, g["row_ptr"]) and np.array_equal(ci, g["col_ind"])
+    assert rel_err(A.values(), g["a"]) <= VAL_TOL and rel_err(eq.getRHS(), g["b"]) <= VAL_TOL
+    for prec in ("ILU", "DIAG"):
+        x = np.zeros(A.n)
+        it = F.CG(A, F.Prec(A, PRECS[prec]), eq.getRHS(), x, 20000, 1e-10)
+        assert abs(it - info["runs"][prec]["iters"]) <= IT_TOL
+        assert rel_err(x, g["x_" + prec]) <= SOL_TOL
+
+
+def test_transient_convection_diffusion():
+    g, info = load_golden("cd2d_17")
+    nx = info["nx"]
+    mesh = F.Mesh(0.0, 1.0, 0.0, 1.0, nx, nx)
+    xy, _, code, _ = mesh.arrays()
+    P = xy.reshape(-1, 2)
+    u0 = np.exp(-((P[:, 0] - 0.3) ** 2 + (P[:, 1] - 0.5) ** 2) / (2 * 0.05 ** 2))
+    u0[code > 0] = 0.0
+    v = np.stack([-(P[:, 1] - 0.5), P[:, 0] - 0.5], axis=1).reshape(-1)
+    eq = F.DC2DT3(mesh, u0, v, info["eps"], info["dt"])
+    eq.setDirichlet(np.zeros(mesh.nn))
+    A, b = eq.build()
+    rp, ci = A.pattern()
+    assert np.array_equal(rp, g["row_ptr"]) and np.array_equal(ci, g["col_ind"])
+    assert rel_err(A.values(), g["a0"]) <= VAL_TOL and rel_err(b, g["b0"]) <= VAL_TOL
+    eq2 = F.DC2DT3(mesh, u0, v, info["eps"], info["dt"])
+    eq2.setDirichlet(np.zeros(mesh.nn))
+    its = [eq2.step(prec=F.ILU_PREC, m=info["m"], max_it=2000, toler=info["tol"])
+           for _ in range(info["steps"])]
+    assert all(abs(a - b) <= IT_TOL for a, b in zip(its, g["iters"]))
+    assert rel_err(eq2.u, g["u"]) <= SOL_TOL
+
+
+def test_linear_solver_gmres_uses_ofeli_restart(p2d65):
+    # LinearSolver::solve with GMRES_SOLVER restarts every n/5 iterations
+    g, _, _, eq = p2d65
+    A = eq.getMatrix()
+    rp, ci = g["row_ptr"].astype(np.int64), g["col_ind"].astype(np.int64)
+    x0, it0 = O.gmres(rp, ci, g["a"], g["b"], O.ILU, A.n // 5, 1000, 1e-8)
+    x = np.zeros(A.n)
+    ls = F.LinearSolver(A, g["b"], x)
+    ls.setTolerance(1e-8)
+    ret = ls.solve(F.GMRES_SOLVER, F.ILU_PREC)
+    assert ret == 0 and abs(ls.getNbIter() - it0) <= IT_TOL
+    assert rel_err(x, x0) <= 1e-11
+
+
+@pytest.mark.parametrize("bits,mode", [(32, 0), (16, 0), (32, 1)])
+def test_mixed_precision_reaches_fp64_accuracy(p2d65, bits, mode):
+    """FP64 true residual <= 1e-10; the error against the FP64 solution of
+    the same system (oracle, residual 1e-13) is reported in the assert."""
+    g, _, _, eq = p2d65
+    A = eq.getMatrix()
+    rp, ci = g["row_ptr"].astype(np.int64), g["col_ind"].astype(np.int64)
+    xref, _ = O.cg(rp, ci, g["a"], g["b"], O.DIAG, 20000, 1e-13)
+    x = np.zeros(A.n)
+    outer, inner, res = F.solve_mixed(A, g["b"], x, prec=F.DIAG_PREC, inner_bits=bits,
+                                      toler=1e-10, mode=mode)
+    assert res <= 1e-10 and F.residual(A, g["b"], x) <= 1e-10
+    err = rel_err(x, xref)
+    assert err <= 1e-7, "error vs FP64 solution %.2e" % err
