@@ -36,7 +36,7 @@ TOL = 1e-10
 # OFELI's own CG + ILU (= diagonal ILU) on this problem converges in this
 # many iterations (run to convergence with the reference built from its
 # sources, tol 1e-10); used to extrapolate the bounded CPU samples.
-REF_ITERS_2049_ILU = None
+REF_ITERS_2049_ILU = 2030
 
 
 def parse():

@@ -9,8 +9,8 @@
 //     x += x_lo;  x_lo = 0;  r = b - A x (FP64 SpMV);  r_lo = (float) r
 // and the FP32 recurrence continues from the true residual with its search
 // direction kept (the "reliable update" form of refinement: the Krylov space
-// is not thrown away at every refinement, so the iteration count stays that
-// of FP64 CG).
+// is not thrown away at every refinement, so the iteration count stays close
+// to that of FP64 CG).
 // Mode 1 (classic restarted refinement): every refinement solves
 // A d = r / ||r|| from d = 0 to `inner_tol` and adds ||r|| d.
 //
@@ -18,6 +18,11 @@
 // accumulation of every Krylov dot product.  One FP32 CG iteration streams
 // 8*nnz + 56*n bytes (6*nnz + 56*n with BF16 values) against 12*nnz + 112*n
 // in FP64.
+//
+// The FP32 vectors are padded to the SELL row count (a multiple of 32) with
+// zeros, so every inner kernel moves 16-byte vectors: a thread owns four
+// consecutive rows, reads their SELL slots as float4/int4 (four adjacent
+// lanes of one slice column) and gathers x for the four rows.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -30,13 +35,11 @@ namespace ofg {
 namespace {
 
 struct MixState {
-   double bnorm, rel;                 // FP64 true residual
-   double rho, rho_new, alpha, rn, rmark, res0;
+   double bnorm, rel;          // FP64 true residual
+   double rho[2];              // rho of the last two iterations, indexed by it & 1
+   double alpha, rn, rmark, res0;
    int it, pause, done, pad;
 };
-
-__device__ __forceinline__ float to_f(float v) { return v; }
-__device__ __forceinline__ float to_f(__nv_bfloat16 v) { return __bfloat162float(v); }
 
 template <class T>
 __global__ void cast_values(int64_t total, const double* __restrict__ src, T* dst)
@@ -72,9 +75,9 @@ __global__ void __launch_bounds__(kRedBlock) mx_residual(int64_t n, const double
    }
 }
 
-// r_lo = (float)(r * scale); rho_new = (r_lo, D r_lo); ||r_lo||; optionally
-// d = 0 and p = D r_lo (fresh start)
-__global__ void __launch_bounds__(kRedBlock) mx_load_residual(int64_t n,
+// r_lo = (float)(r * scale) (zero in the padding); rho = (r_lo, D r_lo),
+// ||r_lo||; x_lo = 0; on a fresh start also p = D r_lo
+__global__ void __launch_bounds__(kRedBlock) mx_load_residual(int64_t n, int64_t npad,
                                                               const double* __restrict__ r,
                                                               double scale,
                                                               const float* __restrict__ dinv,
@@ -84,8 +87,8 @@ __global__ void __launch_bounds__(kRedBlock) mx_load_residual(int64_t n,
 {
    double v[2] = {0.0, 0.0};
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
-   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-      const float ri = (float)(r[i] * scale);
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < npad; i += stride) {
+      const float ri = i < n ? (float)(r[i] * scale) : 0.0f;
       const float zi = ri * dinv[i];
       rr[i] = ri;
       d[i] = 0.0f;
@@ -95,8 +98,7 @@ __global__ void __launch_bounds__(kRedBlock) mx_load_residual(int64_t n,
    }
    double t[2];
    if (grid_reduce<2>(v, partials, counter, t)) {
-      S->rho_new = t[0];
-      if (fresh) S->rho = t[0];
+      S->rho[S->it & 1] = t[0];
       S->rn = sqrt(t[1]);
       S->rmark = S->rn;
       if (fresh) S->res0 = S->rn;
@@ -104,9 +106,20 @@ __global__ void __launch_bounds__(kRedBlock) mx_load_residual(int64_t n,
    }
 }
 
+__device__ __forceinline__ float4 load_vals(const float* p) { return *reinterpret_cast<const float4*>(p); }
+
+__device__ __forceinline__ float4 load_vals(const __nv_bfloat16* p)
+{
+   const uint2 u = *reinterpret_cast<const uint2*>(p);
+   const __nv_bfloat162 a = *reinterpret_cast<const __nv_bfloat162*>(&u.x);
+   const __nv_bfloat162 b = *reinterpret_cast<const __nv_bfloat162*>(&u.y);
+   const float2 fa = __bfloat1622float2(a), fb = __bfloat1622float2(b);
+   return make_float4(fa.x, fa.y, fb.x, fb.y);
+}
+
+// q = A p over four rows per thread, (p, q) -> alpha
 template <class T>
-__global__ void __launch_bounds__(kRedBlock) mx_spmv(int64_t n, int64_t nslices,
-                                                     const int32_t* __restrict__ sp,
+__global__ void __launch_bounds__(kRedBlock) mx_spmv(int64_t nquads, const int32_t* __restrict__ sp,
                                                      const int32_t* __restrict__ scol,
                                                      const T* __restrict__ sval,
                                                      const float* __restrict__ p,
@@ -118,25 +131,35 @@ __global__ void __launch_bounds__(kRedBlock) mx_spmv(int64_t n, int64_t nslices,
    prof_mark(worked);
    double v[1] = {0.0};
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
-   for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < nslices * 32;
-        row += stride) {
-      const int64_t s = row >> 5;
-      const int lane = (int)(row & 31);
-      const int32_t beg = sp[s], end = sp[s + 1];
-      float acc = 0.0f;
-      for (int32_t k = beg + lane; k < end; k += 32) acc += to_f(sval[k]) * __ldg(p + scol[k]);
-      if (row < n) {
-         q[row] = acc;
-         v[0] += (double)p[row] * (double)acc;
+   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nquads; t += stride) {
+      const int64_t r0 = t * 4;
+      const int64_t s = r0 >> 5;
+      const int lane0 = (int)(r0 & 31);
+      const int32_t beg = sp[s], w = (sp[s + 1] - beg) >> 5;
+      float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+      const int32_t* cp = scol + beg + lane0;
+      const T* vp = sval + beg + lane0;
+#pragma unroll 4
+      for (int32_t k = 0; k < w; ++k) {
+         const int4 c = *reinterpret_cast<const int4*>(cp + k * 32);
+         const float4 a = load_vals(vp + k * 32);
+         acc.x += a.x * __ldg(p + c.x);
+         acc.y += a.y * __ldg(p + c.y);
+         acc.z += a.z * __ldg(p + c.z);
+         acc.w += a.w * __ldg(p + c.w);
       }
+      *reinterpret_cast<float4*>(q + r0) = acc;
+      const float4 pr = *reinterpret_cast<const float4*>(p + r0);
+      v[0] += (double)pr.x * acc.x + (double)pr.y * acc.y + (double)pr.z * acc.z +
+              (double)pr.w * acc.w;
    }
    double t[1];
-   if (grid_reduce<1>(v, partials, counter, t)) S->alpha = S->rho / t[0];
+   if (grid_reduce<1>(v, partials, counter, t)) S->alpha = S->rho[S->it & 1] / t[0];
 }
 
 // d += alpha p, r -= alpha q; ||r||, (r, D r); decides when the host must
 // refine (mode 0) or stop the inner solve (mode 1)
-__global__ void __launch_bounds__(kRedBlock) mx_update(int64_t n, float* d,
+__global__ void __launch_bounds__(kRedBlock) mx_update(int64_t nquads, float* d,
                                                        const float* __restrict__ p, float* rr,
                                                        const float* __restrict__ q,
                                                        const float* __restrict__ dinv, MixState* S,
@@ -148,46 +171,62 @@ __global__ void __launch_bounds__(kRedBlock) mx_update(int64_t n, float* d,
    const float a = (float)S->alpha;
    double v[2] = {0.0, 0.0};
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
-   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-      d[i] += a * p[i];
-      const float ri = rr[i] - a * q[i];
-      rr[i] = ri;
-      v[0] += (double)ri * (double)ri;
-      v[1] += (double)ri * (double)(ri * dinv[i]);
+   float4* d4 = reinterpret_cast<float4*>(d);
+   float4* r4 = reinterpret_cast<float4*>(rr);
+   const float4* p4 = reinterpret_cast<const float4*>(p);
+   const float4* q4 = reinterpret_cast<const float4*>(q);
+   const float4* m4 = reinterpret_cast<const float4*>(dinv);
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nquads; i += stride) {
+      const float4 pi = p4[i], qi = q4[i], mi = m4[i];
+      float4 di = d4[i], ri = r4[i];
+      di.x += a * pi.x; di.y += a * pi.y; di.z += a * pi.z; di.w += a * pi.w;
+      ri.x -= a * qi.x; ri.y -= a * qi.y; ri.z -= a * qi.z; ri.w -= a * qi.w;
+      d4[i] = di;
+      r4[i] = ri;
+      v[0] += (double)ri.x * ri.x + (double)ri.y * ri.y + (double)ri.z * ri.z + (double)ri.w * ri.w;
+      v[1] += (double)ri.x * (ri.x * mi.x) + (double)ri.y * (ri.y * mi.y) +
+              (double)ri.z * (ri.z * mi.z) + (double)ri.w * (ri.w * mi.w);
    }
    double t[2];
    if (grid_reduce<2>(v, partials, counter, t)) {
       S->rn = sqrt(t[0]);
-      S->rho_new = t[1];
-      S->it += 1;
+      const int it = S->it + 1;
+      S->rho[it & 1] = t[1];
+      S->it = it;
       if (mode == 0) {
          // refine when the residual fell by delta, or when the recurrence
          // says the FP64 target is reached
-         if (S->rn <= delta * S->rmark || S->rn * scale <= tol * S->bnorm || S->it >= max_inner)
+         if (S->rn <= delta * S->rmark || S->rn * scale <= tol * S->bnorm || it >= max_inner)
             S->pause = 1;
       }
-      else if (S->rn <= delta * S->res0 || S->it >= max_inner) {
+      else if (S->rn <= delta * S->res0 || it >= max_inner) {
          S->pause = 1;
       }
    }
 }
 
-__global__ void __launch_bounds__(kRedBlock) mx_direction(int64_t n, const float* __restrict__ rr,
+// p = D r + beta p, beta = rho_it / rho_{it-1}
+__global__ void __launch_bounds__(kRedBlock) mx_direction(int64_t nquads,
+                                                          const float* __restrict__ rr,
                                                           const float* __restrict__ dinv, float* p,
-                                                          MixState* S)
+                                                          const MixState* S)
 {
    if (S->pause) return;
-   const float beta = (float)(S->rho_new / S->rho);
+   const int it = S->it;
+   const float beta = (float)(S->rho[it & 1] / S->rho[(it + 1) & 1]);
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
-   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
-      p[i] = rr[i] * dinv[i] + beta * p[i];
-}
-
-// rho <- rho_new, after every block of mx_direction has read rho
-__global__ void mx_rho_shift(MixState* S)
-{
-   if (S->pause) return;
-   S->rho = S->rho_new;
+   float4* p4 = reinterpret_cast<float4*>(p);
+   const float4* r4 = reinterpret_cast<const float4*>(rr);
+   const float4* m4 = reinterpret_cast<const float4*>(dinv);
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nquads; i += stride) {
+      const float4 ri = r4[i], mi = m4[i];
+      float4 pi = p4[i];
+      pi.x = ri.x * mi.x + beta * pi.x;
+      pi.y = ri.y * mi.y + beta * pi.y;
+      pi.z = ri.z * mi.z + beta * pi.z;
+      pi.w = ri.w * mi.w + beta * pi.w;
+      p4[i] = pi;
+   }
 }
 
 // x += scale * d (FP64)
@@ -198,21 +237,25 @@ __global__ void mx_correct(int64_t n, double* x, const float* __restrict__ d, do
       x[i] += scale * (double)d[i];
 }
 
-__global__ void inv_diag32(int64_t n, const int32_t* dpos, const double* val, float* dinv, int* bad)
+// D^{-1} in FP32, zero in the padding; IDENT: ones
+__global__ void inv_diag32(int64_t n, int64_t npad, const int32_t* dpos, const double* val,
+                           float* dinv, int ident, int* bad)
 {
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
-   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < npad; i += stride) {
+      if (i >= n) {
+         dinv[i] = 0.0f;
+         continue;
+      }
+      if (ident) {
+         dinv[i] = 1.0f;
+         continue;
+      }
       const int32_t k = dpos[i];
       const double a = k >= 0 ? val[k] : 0.0;
       if (a == 0.0) atomicOr(bad, 1);
       dinv[i] = (float)(1.0 / a);
    }
-}
-
-__global__ void fill_ones(int64_t n, float* p)
-{
-   int64_t stride = (int64_t)gridDim.x * blockDim.x;
-   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) p[i] = 1.0f;
 }
 
 }  // namespace
@@ -230,6 +273,7 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
    ensure_sell(A);
    ensure_dpos(A);
    OFG_REQUIRE(A->dpos_complete, OFG_ERR_PIVOT, "a row has no diagonal entry");
+   const int64_t npad = A->nslices * 32, nquads = npad / 4;
    DBuf<__nv_bfloat16> v16;
    if (inner_bits == 32) ensure_sell32(A);
    else {
@@ -238,31 +282,29 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
          A->sell_val.n, A->sell_val.p, v16.p);
       count_launch();
    }
-   DBuf<float> dinv(n), rr(n), p(n), q(n), d(n);
-   DBuf<double> r(n), q64(n);
+   const int64_t nv = npad > 0 ? npad : 4;
+   DBuf<float> dinv(nv), rr(nv), p(nv), q(nv), d(nv);
+   DBuf<double> r(n > 0 ? n : 1), q64(n > 0 ? n : 1);
    DBuf<MixState> S(1);
    DBuf<int> bad(1);
    bad.zero();
-   DBuf<double> partials(((size_t)grid_for(n, kRedBlock, 8) + 1) * 4 + 4);
+   p.zero();
+   const unsigned g = grid_for(std::max<int64_t>(n, nquads), kRedBlock, 8);
+   DBuf<double> partials(((size_t)g + 1) * 4 + 4);
    DBuf<unsigned> counter(1);
    counter.zero();
-   if (prec_type == OFG_DIAG) {
-      inv_diag32<<<grid_for(n, 256), 256, 0, stream()>>>(n, A->dpos.p, A->val.p, dinv.p, bad.p);
-      count_launch();
-      int h = 0;
-      bad.download(&h, 1);
-      OFG_REQUIRE(!h, OFG_ERR_PIVOT, "zero diagonal entry");
-   }
-   else {
-      fill_ones<<<grid_for(n, 256), 256, 0, stream()>>>(n, dinv.p);
-      count_launch();
-   }
-   const unsigned g = grid_for(n, kRedBlock, 8);
-   const unsigned gs = grid_for(A->nslices * 32, kRedBlock, 8);
+   inv_diag32<<<grid_for(nv, 256), 256, 0, stream()>>>(n, npad, A->dpos.p, A->val.p, dinv.p,
+                                                        prec_type == OFG_IDENT ? 1 : 0, bad.p);
+   count_launch();
+   int hb = 0;
+   bad.download(&hb, 1);
+   OFG_REQUIRE(!hb, OFG_ERR_PIVOT, "zero diagonal entry");
+   const unsigned gq = grid_for(nquads, kRedBlock, 8);
+   const unsigned gn = grid_for(n, kRedBlock, 8);
    auto true_residual = [&](int first) {
       spmv_sell(A, x, q64.p);
-      mx_residual<<<g, kRedBlock, 0, stream()>>>(n, b, q64.p, r.p, S.p, partials.p, counter.p, tol,
-                                                 first);
+      mx_residual<<<gn, kRedBlock, 0, stream()>>>(n, b, q64.p, r.p, S.p, partials.p, counter.p,
+                                                  tol, first);
       count_launch();
       OFG_LAUNCH_CHECK();
    };
@@ -273,18 +315,18 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
    // mode 1 solves for d in units of ||r||; mode 0 keeps absolute units
    double scale = 1.0;
    bool fresh = true;
-   while (!h.done && n_outer < max_outer && h.it < max_inner) {
+   while (!h.done && n_outer < max_outer && h.it < max_inner && n > 0) {
       if (mode == 1) {
          scale = h.rel * h.bnorm;
          fresh = true;
       }
-      mx_load_residual<<<g, kRedBlock, 0, stream()>>>(n, r.p, 1.0 / scale, dinv.p, rr.p, p.p, d.p,
-                                                      fresh ? 1 : 0, S.p, partials.p, counter.p);
+      mx_load_residual<<<gq, kRedBlock, 0, stream()>>>(n, npad, r.p, 1.0 / scale, dinv.p, rr.p,
+                                                       p.p, d.p, fresh ? 1 : 0, S.p, partials.p,
+                                                       counter.p);
       count_launch();
       if (!fresh) {
-         mx_direction<<<g, kRedBlock, 0, stream()>>>(n, rr.p, dinv.p, p.p, S.p);
-         mx_rho_shift<<<1, 1, 0, stream()>>>(S.p);
-         count_launch(2);
+         mx_direction<<<gq, kRedBlock, 0, stream()>>>(nquads, rr.p, dinv.p, p.p, S.p);
+         count_launch();
       }
       fresh = false;
       int batch = 8;
@@ -292,22 +334,20 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
          for (int k = 0; k < batch; ++k) {
             int* worked = prof_begin();
             if (inner_bits == 32)
-               mx_spmv<float><<<gs, kRedBlock, 0, stream()>>>(n, A->nslices, A->sell_ptr.p,
-                                                             A->sell_col.p, A->sell_val32.p, p.p,
-                                                             q.p, S.p, partials.p, counter.p,
-                                                             worked);
+               mx_spmv<float><<<gq, kRedBlock, 0, stream()>>>(nquads, A->sell_ptr.p, A->sell_col.p,
+                                                             A->sell_val32.p, p.p, q.p, S.p,
+                                                             partials.p, counter.p, worked);
             else
-               mx_spmv<__nv_bfloat16><<<gs, kRedBlock, 0, stream()>>>(
-                  n, A->nslices, A->sell_ptr.p, A->sell_col.p, v16.p, p.p, q.p, S.p, partials.p,
+               mx_spmv<__nv_bfloat16><<<gq, kRedBlock, 0, stream()>>>(
+                  nquads, A->sell_ptr.p, A->sell_col.p, v16.p, p.p, q.p, S.p, partials.p,
                   counter.p, worked);
             prof_end(inner_bits == 32 ? PROF_SPMV32 : PROF_SPMV16,
                      (inner_bits == 32 ? 8.0 : 6.0) * A->nnz + 12.0 * n + 4.0);
-            mx_update<<<g, kRedBlock, 0, stream()>>>(n, d.p, p.p, rr.p, q.p, dinv.p, S.p,
-                                                     partials.p, counter.p, inner_tol, tol, scale,
-                                                     max_inner, mode);
-            mx_direction<<<g, kRedBlock, 0, stream()>>>(n, rr.p, dinv.p, p.p, S.p);
-            mx_rho_shift<<<1, 1, 0, stream()>>>(S.p);
-            count_launch(4);
+            mx_update<<<gq, kRedBlock, 0, stream()>>>(nquads, d.p, p.p, rr.p, q.p, dinv.p, S.p,
+                                                      partials.p, counter.p, inner_tol, tol, scale,
+                                                      max_inner, mode);
+            mx_direction<<<gq, kRedBlock, 0, stream()>>>(nquads, rr.p, dinv.p, p.p, S.p);
+            count_launch(3);
          }
          OFG_LAUNCH_CHECK();
          S.download(&h, 1);
@@ -315,7 +355,7 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
          batch = std::min(batch * 2, 64);
       }
       // refinement step in FP64
-      mx_correct<<<g, kRedBlock, 0, stream()>>>(n, x, d.p, scale);
+      mx_correct<<<gn, kRedBlock, 0, stream()>>>(n, x, d.p, scale);
       count_launch();
       true_residual(0);
       S.download(&h, 1);

@@ -32,6 +32,7 @@ namespace ofg {
 namespace {
 
 constexpr int kWarpsPerBlock = 4;
+constexpr int kPre = 8;  // dependency entries per row fetched together
 constexpr int kMinStrand = 32;
 constexpr int kMaxStrand = 1 << 16;
 constexpr long long kSpinFast = 2048;
@@ -140,7 +141,54 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) sweep_kernel(SweepArgs g)
          double sext = 0.0, m1 = 0.0;
          bool other_intra = false;
          if (MODE == FACTOR) sext = valid ? g.val[dk] : 0.0;
-         for (int32_t k = kb; k < ke; ++k) {
+         // the first kPre entries: all loads (matrix and earlier results)
+         // are issued before any is consumed, so their latencies overlap
+         int32_t pc[kPre];
+         double pa[kPre], pz[kPre];
+#pragma unroll
+         for (int q = 0; q < kPre; ++q) {
+            const int32_t k = kb + q;
+            pc[q] = -1;
+            if (k < ke) {
+               pc[q] = g.col[k];
+               pa[q] = g.val[k];
+            }
+         }
+#pragma unroll
+         for (int q = 0; q < kPre; ++q) {
+            pz[q] = 0.0;
+            if (pc[q] >= 0) {
+               const int64_t lj = FWD ? pc[q] : n - 1 - pc[q];
+               if (lj < s0 && !(lj == s0 - 1 && have_carry)) pz[q] = ld_relaxed(g.out + pc[q]);
+            }
+         }
+#pragma unroll
+         for (int q = 0; q < kPre; ++q) {
+            if (pc[q] < 0) continue;
+            const int64_t j = pc[q];
+            const int64_t lj = FWD ? j : n - 1 - j;
+            const double a = pa[q];
+            double v = 0.0;
+            if (lj < s0) {
+               v = (lj == s0 - 1 && have_carry) ? carry
+                                                : (is_sentinel(pz[q]) ? wait_value_slow(g.out + j, g.status) : pz[q]);
+            }
+            if (MODE == FACTOR) {
+               const int32_t tp = g.tpos[kb + q];
+               if (tp < 0) continue;
+               if (lj >= s0) { other_intra = true; continue; }
+               sext = __dsub_rn(sext, __dmul_rn(__dmul_rn(a, v), g.val[tp]));
+            }
+            else {
+               if (lj >= s0) {
+                  if (lj == rho - 1) m1 = a;
+                  else other_intra = true;
+                  continue;
+               }
+               sext += a * v;
+            }
+         }
+         for (int32_t k = kb + kPre; k < ke; ++k) {
             const int64_t j = g.col[k];
             const int64_t lj = FWD ? j : n - 1 - j;
             const double a = g.val[k];

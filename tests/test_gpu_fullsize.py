@@ -97,3 +97,17 @@ def test_kuhn_129_pattern_and_values(cuda):
     rp2, ci2 = A.pattern()
     assert np.array_equal(rp2, rp) and np.array_equal(ci2, ci)
     assert rel_err(A.values(), a) <= 1e-12 and rel_err(eq.getRHS(), b) <= 1e-12
+
+
+def test_plain_cg_ilu_matches_reference_at_full_size(big):
+    """OFELI's own CG + ILU run to convergence on this problem (pins in
+    tests/golden/p2d_2049_pins.npz): same iteration count, same solution."""
+    from conftest import load_golden
+    pins, info = load_golden("p2d_2049_pins")
+    A = big["A"]
+    x = np.zeros(A.n)
+    it = F.CG(A, F.Prec(A, F.ILU_PREC), big["b"], x, 100000, info["tol"])
+    assert abs(it - info["iters"]) <= 2
+    assert abs(np.linalg.norm(x) / info["x_norm2"] - 1) <= 1e-12
+    sample = x[::info["x_sample_stride"]]
+    assert rel_err(sample, pins["x_sample"]) <= 1e-11
