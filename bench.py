@@ -274,7 +274,6 @@ def run_ours(args):
 
     # ------------------------------------------------ timed: device-resident
     launches0 = capi.launch_count()
-    capi.profile_enable(4)  # every 4th launch of a kernel family timed with events
     clocks = ClockSampler(local)
     clocks.start()
     time.sleep(0.4)
@@ -292,9 +291,15 @@ def run_ours(args):
     ms = e0.elapsed_time(e1)
     clk = clocks.stop()
     launches = capi.launch_count() - launches0
+    ms = max_over_ranks(ms)
+    # the dominant kernel's launches timed with CUDA events on the library
+    # stream (every 4th launch), over one more step of the same workload;
+    # kept out of the timed steps so the events do not perturb them
+    capi.profile_enable(4)
+    step_device()
+    torch.cuda.synchronize()
     prof = {k: capi.profile_read(k) for k in ("spmv32", "spmv16", "spmv64", "assembly")}
     capi.profile_enable(0)
-    ms = max_over_ranks(ms)
     worst_res = max(s[2] for s in stats)
     if worst_res > TOL:
         raise SystemExit("solve missed the FP64 target: %.3e" % worst_res)

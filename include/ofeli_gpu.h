@@ -93,6 +93,14 @@ int ofg_spmv_add(const ofg_matrix* A, const double* x, double* y);
 /* Device-only SpMV with an explicit layout choice, for measurement:
  * kind 0 = CSR warp-segment kernel, 1 = SELL-32 kernel. */
 int ofg_spmv_device(const ofg_matrix* A, int kind, const double* d_x, double* d_y);
+/* Device-only SpMV with the FP32 copy of the values and FP32 vectors of
+ * nslices*32 entries (the row count rounded up to a multiple of 32), for
+ * measurement of the thread-to-row mappings of the SELL-32 layout:
+ * kind 0 = one row per thread, 1 = four adjacent rows per thread (16-byte
+ * loads), 2 = four rows from four consecutive slices per thread, 3 = two
+ * adjacent rows per thread (8-byte loads).  blocks_per_sm (0 = 8) caps the
+ * grid at that many 256-thread blocks per SM. */
+int ofg_spmv32_device(ofg_matrix* A, int kind, int blocks_per_sm, const float* d_x, float* d_y);
 
 /* -------------------------------------------------------------- P1 meshes */
 /* Mesh(xmin,xmax,ymin,ymax,nx,ny,cx0,cxN,cy0,cyN,TRIANGLE) --

@@ -45,6 +45,7 @@ SIGNATURES = {
     "ofg_spmv": (_i32, [_p, _p, _p]),
     "ofg_spmv_add": (_i32, [_p, _p, _p]),
     "ofg_spmv_device": (_i32, [_p, _i32, _p, _p]),
+    "ofg_spmv32_device": (_i32, [_p, _i32, _i32, _p, _p]),
     "ofg_mesh_create_rect": (_i32, [_d, _d, _d, _d, _i64, _i64, _i32, _i32, _i32, _i32, _pp]),
     "ofg_mesh_create_kuhn": (_i32, [_i64, _pp]),
     "ofg_mesh_create": (_i32, [_i32, _i64, _p, _i64, _p, _p, _pp]),

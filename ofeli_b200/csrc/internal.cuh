@@ -59,6 +59,16 @@ struct SweepPlan {
    DBuf<int32_t> start;       // logical row where each strand starts, nstrands+1
    DBuf<double> strand_dot;   // per-strand partial dot products
    DBuf<int> ticket;          // [0] next strand, [1] finished strands
+   // per-segment slot layout of the dependency entries: segment s of strand
+   // t (t's rows in 32-row groups) owns slots seg_off[s] .. seg_off[s+1],
+   // stored column-major (slot k of lane l at seg_off[s] + 32 k + l), in
+   // the CSR's column order
+   int64_t nseg = 0;
+   DBuf<int32_t> tseg;        // first segment of each strand, nstrands+1
+   DBuf<int32_t> seg_off;     // nseg+1
+   DBuf<int32_t> sl_col;      // physical column, -1 for padding
+   DBuf<int32_t> sl_src;      // CSR index of the value, -1 for padding
+   DBuf<double> sl_val;
 };
 }  // namespace ofg
 

@@ -40,7 +40,7 @@ __device__ __forceinline__ double zval(int64_t i, const double* r, const double*
 }
 
 template <int PT>
-__global__ void __launch_bounds__(kRedBlock) cg_init(int64_t n, const double* __restrict__ b,
+__global__ void __launch_bounds__(kRedBlock, 8) cg_init(int64_t n, const double* __restrict__ b,
                                                      const double* __restrict__ q, double* r,
                                                      const double* __restrict__ piv, CGState* S,
                                                      double* partials, unsigned* counter, double tol)
@@ -70,7 +70,7 @@ __global__ void __launch_bounds__(kRedBlock) cg_init(int64_t n, const double* __
 }
 
 template <int PT>
-__global__ void __launch_bounds__(kRedBlock) cg_direction(int64_t n, const double* __restrict__ r,
+__global__ void __launch_bounds__(kRedBlock, 8) cg_direction(int64_t n, const double* __restrict__ r,
                                                           const double* __restrict__ piv,
                                                           const double* __restrict__ z, double* p,
                                                           const CGState* S)
@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(kRedBlock) cg_direction(int64_t n, const doubl
    }
 }
 
-__global__ void __launch_bounds__(kRedBlock) cg_spmv(int64_t n, int64_t nslices,
+__global__ void __launch_bounds__(kRedBlock, 8) cg_spmv(int64_t n, int64_t nslices,
                                                      const int32_t* __restrict__ sp,
                                                      const int32_t* __restrict__ scol,
                                                      const double* __restrict__ sval,
@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(kRedBlock) cg_spmv(int64_t n, int64_t nslices,
 }
 
 template <int PT>
-__global__ void __launch_bounds__(kRedBlock) cg_update(int64_t n, double* x,
+__global__ void __launch_bounds__(kRedBlock, 8) cg_update(int64_t n, double* x,
                                                        const double* __restrict__ p, double* r,
                                                        const double* __restrict__ q,
                                                        const double* __restrict__ piv, CGState* S,
@@ -160,7 +160,7 @@ struct GMState {
    int it, done, stop, conv_i, result, pad;
 };
 
-__global__ void __launch_bounds__(kRedBlock) gm_residual(int64_t n, const double* __restrict__ b,
+__global__ void __launch_bounds__(kRedBlock, 8) gm_residual(int64_t n, const double* __restrict__ b,
                                                          const double* __restrict__ q, double* r,
                                                          GMState* S, double* partials,
                                                          unsigned* counter, int first)
@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(kRedBlock) gm_residual(int64_t n, const double
 
 // beta = ||r||; first call: the initial convergence test of GMRes.h:169-179,
 // later calls: the restart test of :222-233.
-__global__ void __launch_bounds__(kRedBlock) gm_beta(int64_t n, const double* __restrict__ r,
+__global__ void __launch_bounds__(kRedBlock, 8) gm_beta(int64_t n, const double* __restrict__ r,
                                                      GMState* S, double* partials,
                                                      unsigned* counter, double tol, int first,
                                                      int max_it)
@@ -230,7 +230,7 @@ __global__ void gm_start(int64_t n, const double* __restrict__ r, double* v0, do
 
 // Modified Gram-Schmidt step k of column i: w -= h_{k-1} v_{k-1} (k > 0),
 // then h_k = (w, v_k).
-__global__ void __launch_bounds__(kRedBlock) gm_mgs(int64_t n, double* w,
+__global__ void __launch_bounds__(kRedBlock, 8) gm_mgs(int64_t n, double* w,
                                                     const double* __restrict__ vprev,
                                                     const double* hprev,
                                                     const double* __restrict__ vk, double* hk,
@@ -254,7 +254,7 @@ __global__ void __launch_bounds__(kRedBlock) gm_mgs(int64_t n, double* w,
 }
 
 // last projection w -= h_i v_i and H(i+1,i) = ||w||
-__global__ void __launch_bounds__(kRedBlock) gm_mgs_last(int64_t n, double* w,
+__global__ void __launch_bounds__(kRedBlock, 8) gm_mgs_last(int64_t n, double* w,
                                                          const double* __restrict__ vi,
                                                          const double* hi, double* hnext,
                                                          double* partials, unsigned* counter,
@@ -356,7 +356,7 @@ __global__ void gm_update_x(int64_t n, double* x, const double* __restrict__ V,
    }
 }
 
-__global__ void __launch_bounds__(kRedBlock) res_kernel(int64_t n, const double* __restrict__ b,
+__global__ void __launch_bounds__(kRedBlock, 8) res_kernel(int64_t n, const double* __restrict__ b,
                                                         const double* __restrict__ q,
                                                         double* out, double* partials,
                                                         unsigned* counter)

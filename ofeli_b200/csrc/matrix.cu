@@ -151,7 +151,7 @@ __global__ void sell_values(int64_t total, const int32_t* ssrc, const double* va
 
 // ------------------------------------------------------------------ SpMV --
 template <bool ADD>
-__global__ void __launch_bounds__(256) spmv_sell_kernel(int64_t n, int64_t nslices,
+__global__ void __launch_bounds__(256, 8) spmv_sell_kernel(int64_t n, int64_t nslices,
                                                         const int32_t* __restrict__ sp,
                                                         const int32_t* __restrict__ scol,
                                                         const double* __restrict__ sval,
@@ -169,6 +169,118 @@ __global__ void __launch_bounds__(256) spmv_sell_kernel(int64_t n, int64_t nslic
       double acc = 0.0;
       for (int32_t k = beg + lane; k < end; k += 32) acc += sval[k] * __ldg(x + scol[k]);
       if (r < n) y[r] = ADD ? y[r] + acc : acc;
+   }
+}
+
+// ---------------------------------------------------- FP32 SELL variants --
+// y = A x with FP32 values and vectors, four thread-to-row mappings over the
+// same SELL-32 arrays:
+//   kind 0: one row per thread (a warp = one slice, 128-byte lines);
+//   kind 1: four adjacent rows per thread, float4/int4 loads;
+//   kind 2: four rows per thread taken from four consecutive slices (one
+//           row per slice, scalar loads, four independent chains);
+//   kind 3: two adjacent rows per thread, float2/int2 loads.
+// y and x must hold nslices*32 entries (padding rows produce 0).
+__global__ void __launch_bounds__(256) spmv32_row(int64_t nslices, const int32_t* __restrict__ sp,
+                                                  const int32_t* __restrict__ scol,
+                                                  const float* __restrict__ sval,
+                                                  const float* __restrict__ x, float* __restrict__ y)
+{
+   int64_t stride = (int64_t)gridDim.x * blockDim.x;
+   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nslices * 32; r += stride) {
+      const int64_t s = r >> 5;
+      const int lane = (int)(r & 31);
+      const int32_t beg = sp[s], end = sp[s + 1];
+      float acc = 0.f;
+#pragma unroll 8
+      for (int32_t k = beg + lane; k < end; k += 32) acc += sval[k] * __ldg(x + scol[k]);
+      y[r] = acc;
+   }
+}
+
+__global__ void __launch_bounds__(256) spmv32_vec4(int64_t nslices, const int32_t* __restrict__ sp,
+                                                   const int32_t* __restrict__ scol,
+                                                   const float* __restrict__ sval,
+                                                   const float* __restrict__ x,
+                                                   float* __restrict__ y)
+{
+   int64_t stride = (int64_t)gridDim.x * blockDim.x;
+   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nslices * 8; t += stride) {
+      const int64_t r0 = t * 4, s = r0 >> 5;
+      const int32_t beg = sp[s], w = (sp[s + 1] - beg) >> 5;
+      const int32_t* cp = scol + beg + (r0 & 31);
+      const float* vp = sval + beg + (r0 & 31);
+      float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll 8
+      for (int32_t k = 0; k < w; ++k) {
+         const int4 c = *reinterpret_cast<const int4*>(cp + k * 32);
+         const float4 a = *reinterpret_cast<const float4*>(vp + k * 32);
+         acc.x += a.x * __ldg(x + c.x);
+         acc.y += a.y * __ldg(x + c.y);
+         acc.z += a.z * __ldg(x + c.z);
+         acc.w += a.w * __ldg(x + c.w);
+      }
+      *reinterpret_cast<float4*>(y + r0) = acc;
+   }
+}
+
+__global__ void __launch_bounds__(256) spmv32_slices4(int64_t nslices,
+                                                      const int32_t* __restrict__ sp,
+                                                      const int32_t* __restrict__ scol,
+                                                      const float* __restrict__ sval,
+                                                      const float* __restrict__ x,
+                                                      float* __restrict__ y)
+{
+   // warp w owns slices 4w .. 4w+3; lane l owns row l of each
+   const int lane = threadIdx.x & 31;
+   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+   for (int64_t s4 = warp * 4; s4 < nslices; s4 += nw * 4) {
+      int32_t beg[4], w[4];
+      float acc[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+         const int64_t s = min(s4 + q, nslices - 1);
+         beg[q] = sp[s];
+         w[q] = s4 + q < nslices ? (sp[s + 1] - beg[q]) >> 5 : 0;
+         acc[q] = 0.f;
+      }
+      const int32_t wmax = max(max(w[0], w[1]), max(w[2], w[3]));
+      for (int32_t k = 0; k < wmax; ++k) {
+#pragma unroll
+         for (int q = 0; q < 4; ++q)
+            if (k < w[q]) {
+               const int32_t idx = beg[q] + k * 32 + lane;
+               acc[q] += sval[idx] * __ldg(x + scol[idx]);
+            }
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+         if (s4 + q < nslices) y[(s4 + q) * 32 + lane] = acc[q];
+   }
+}
+
+__global__ void __launch_bounds__(256) spmv32_vec2(int64_t nslices, const int32_t* __restrict__ sp,
+                                                   const int32_t* __restrict__ scol,
+                                                   const float* __restrict__ sval,
+                                                   const float* __restrict__ x,
+                                                   float* __restrict__ y)
+{
+   int64_t stride = (int64_t)gridDim.x * blockDim.x;
+   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nslices * 16; t += stride) {
+      const int64_t r0 = t * 2, s = r0 >> 5;
+      const int32_t beg = sp[s], w = (sp[s + 1] - beg) >> 5;
+      const int32_t* cp = scol + beg + (r0 & 31);
+      const float* vp = sval + beg + (r0 & 31);
+      float2 acc = make_float2(0.f, 0.f);
+#pragma unroll 8
+      for (int32_t k = 0; k < w; ++k) {
+         const int2 c = *reinterpret_cast<const int2*>(cp + k * 32);
+         const float2 a = *reinterpret_cast<const float2*>(vp + k * 32);
+         acc.x += a.x * __ldg(x + c.x);
+         acc.y += a.y * __ldg(x + c.y);
+      }
+      *reinterpret_cast<float2*>(y + r0) = acc;
    }
 }
 
@@ -470,6 +582,41 @@ int ofg_spmv_add(const ofg_matrix* A, const double* x, double* y)
       InOut<double> dy(y, A->n, true);
       spmv_csr(A, dx.d, dy.d, true);
       dy.finish();
+   });
+}
+
+int ofg_spmv32_device(ofg_matrix* A, int kind, int blocks_per_sm, const float* d_x, float* d_y)
+{
+   return guarded("ofg_spmv32_device", [&] {
+      OFG_REQUIRE(A && d_x && d_y, OFG_ERR_ARG, "null argument");
+      OFG_REQUIRE(kind >= 0 && kind <= 3, OFG_ERR_ARG, "kind must be 0..3");
+      ensure_sell32(A);
+      if (!A->n) return;
+      const int bps = blocks_per_sm > 0 ? blocks_per_sm : 8;
+      const int64_t ns = A->nslices;
+      int* worked = prof_begin();
+      if (worked) OFG_CUDA(cudaMemsetAsync(worked, 1, sizeof(int), stream()));
+      switch (kind) {
+         case 0:
+            spmv32_row<<<grid_for(ns * 32, 256, bps), 256, 0, stream()>>>(
+               ns, A->sell_ptr.p, A->sell_col.p, A->sell_val32.p, d_x, d_y);
+            break;
+         case 1:
+            spmv32_vec4<<<grid_for(ns * 8, 256, bps), 256, 0, stream()>>>(
+               ns, A->sell_ptr.p, A->sell_col.p, A->sell_val32.p, d_x, d_y);
+            break;
+         case 2:
+            spmv32_slices4<<<grid_for(ns * 8, 256, bps), 256, 0, stream()>>>(
+               ns, A->sell_ptr.p, A->sell_col.p, A->sell_val32.p, d_x, d_y);
+            break;
+         default:
+            spmv32_vec2<<<grid_for(ns * 16, 256, bps), 256, 0, stream()>>>(
+               ns, A->sell_ptr.p, A->sell_col.p, A->sell_val32.p, d_x, d_y);
+            break;
+      }
+      prof_end(PROF_SPMV32, 8.0 * A->nnz + 12.0 * A->n + 4.0);
+      count_launch();
+      OFG_LAUNCH_CHECK();
    });
 }
 

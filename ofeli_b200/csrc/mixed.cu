@@ -50,7 +50,7 @@ __global__ void cast_values(int64_t total, const double* __restrict__ src, T* ds
 }
 
 // r = b - q (FP64); ||r||, ||b|| (first call); convergence test
-__global__ void __launch_bounds__(kRedBlock) mx_residual(int64_t n, const double* __restrict__ b,
+__global__ void __launch_bounds__(kRedBlock, 8) mx_residual(int64_t n, const double* __restrict__ b,
                                                          const double* __restrict__ q, double* r,
                                                          MixState* S, double* partials,
                                                          unsigned* counter, double tol, int first)
@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(kRedBlock) mx_residual(int64_t n, const double
 
 // r_lo = (float)(r * scale) (zero in the padding); rho = (r_lo, D r_lo),
 // ||r_lo||; x_lo = 0; on a fresh start also p = D r_lo
-__global__ void __launch_bounds__(kRedBlock) mx_load_residual(int64_t n, int64_t npad,
+__global__ void __launch_bounds__(kRedBlock, 8) mx_load_residual(int64_t n, int64_t npad,
                                                               const double* __restrict__ r,
                                                               double scale,
                                                               const float* __restrict__ dinv,
@@ -119,7 +119,7 @@ __device__ __forceinline__ float4 load_vals(const __nv_bfloat16* p)
 
 // q = A p over four rows per thread, (p, q) -> alpha
 template <class T>
-__global__ void __launch_bounds__(kRedBlock) mx_spmv(int64_t nquads, const int32_t* __restrict__ sp,
+__global__ void __launch_bounds__(kRedBlock, 8) mx_spmv(int64_t nquads, const int32_t* __restrict__ sp,
                                                      const int32_t* __restrict__ scol,
                                                      const T* __restrict__ sval,
                                                      const float* __restrict__ p,
@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(kRedBlock) mx_spmv(int64_t nquads, const int32
       float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
       const int32_t* cp = scol + beg + lane0;
       const T* vp = sval + beg + lane0;
-#pragma unroll 4
+#pragma unroll 8
       for (int32_t k = 0; k < w; ++k) {
          const int4 c = *reinterpret_cast<const int4*>(cp + k * 32);
          const float4 a = load_vals(vp + k * 32);
@@ -159,7 +159,7 @@ __global__ void __launch_bounds__(kRedBlock) mx_spmv(int64_t nquads, const int32
 
 // d += alpha p, r -= alpha q; ||r||, (r, D r); decides when the host must
 // refine (mode 0) or stop the inner solve (mode 1)
-__global__ void __launch_bounds__(kRedBlock) mx_update(int64_t nquads, float* d,
+__global__ void __launch_bounds__(kRedBlock, 8) mx_update(int64_t nquads, float* d,
                                                        const float* __restrict__ p, float* rr,
                                                        const float* __restrict__ q,
                                                        const float* __restrict__ dinv, MixState* S,
@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(kRedBlock) mx_update(int64_t nquads, float* d,
 }
 
 // p = D r + beta p, beta = rho_it / rho_{it-1}
-__global__ void __launch_bounds__(kRedBlock) mx_direction(int64_t nquads,
+__global__ void __launch_bounds__(kRedBlock, 8) mx_direction(int64_t nquads,
                                                           const float* __restrict__ rr,
                                                           const float* __restrict__ dinv, float* p,
                                                           const MixState* S)

@@ -357,6 +357,230 @@ __global__ void transpose_positions(int64_t n, const int32_t* rp, const int32_t*
    }
 }
 
+// ------------------------------------------------------- solve sweeps ----
+// The forward / backward sweeps of DILUSolve and SSORSolve over the slot
+// layout.  Per segment a lane holds one row: its dependency slots (column,
+// value) arrive as coalesced lines, the next segment's slots, b and pivot
+// are fetched while the current segment waits for its earlier-row values.
+constexpr int kSlots = 8;  // slots held in registers; wider rows take a slow loop
+
+struct SolveArgs {
+   int64_t n;
+   const int32_t* tseg;
+   const int32_t* seg_off;
+   const int32_t* sl_col;
+   const double* sl_val;
+   const double* piv;
+   const double* in;
+   double* out;
+   double* reset;
+   const double* dot_with;
+   double* strand_dot;
+   double* dot_out;
+   const int32_t* sstart;
+   int64_t nstrands;
+   int* ticket;
+   int* status;
+   const int* skip;
+   int* worked;
+};
+
+struct SegRegs {
+   int32_t off, w;
+   int32_t c[kSlots];
+   double a[kSlots];
+   double b, pv;
+};
+
+template <bool FWD>
+__device__ __forceinline__ void load_segment(const SolveArgs& g, int64_t s, int64_t s0, int64_t end,
+                                             int lane, SegRegs& R)
+{
+   R.off = g.seg_off[s];
+   R.w = (g.seg_off[s + 1] - R.off) >> 5;
+#pragma unroll
+   for (int k = 0; k < kSlots; ++k) {
+      R.c[k] = -1;
+      R.a[k] = 0.0;
+      if (k < R.w) {
+         R.c[k] = g.sl_col[R.off + k * 32 + lane];
+         R.a[k] = g.sl_val[R.off + k * 32 + lane];
+      }
+   }
+   const int64_t rho = s0 + lane;
+   R.b = 0.0;
+   R.pv = 1.0;
+   if (rho < end) {
+      const int64_t row = FWD ? rho : g.n - 1 - rho;
+      R.b = g.in[row];
+      R.pv = g.piv[row];
+   }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) solve_sweep(SolveArgs g)
+{
+   constexpr bool FWD = (MODE == FWD_DILU || MODE == FWD_SSOR);
+   __shared__ double segv[kWarpsPerBlock][32];
+   const int lane = threadIdx.x & 31;
+   const int w = threadIdx.x >> 5;
+   const unsigned FULL = 0xffffffffu;
+   const int64_t n = g.n;
+   if (g.skip && *g.skip) return;
+   prof_mark(g.worked);
+
+   for (;;) {
+      int t = 0;
+      if (lane == 0) t = atomicAdd(&g.ticket[0], 1);
+      t = __shfl_sync(FULL, t, 0);
+      if (t >= g.nstrands) break;
+      const int64_t beg = g.sstart[t], end = g.sstart[t + 1];
+      const int64_t sfirst = g.tseg[t], slast = g.tseg[t + 1];
+      double carry = 0.0;
+      bool have_carry = false;
+      double dotp = 0.0;
+      SegRegs cur, nxt;
+      load_segment<FWD>(g, sfirst, beg, end, lane, cur);
+      for (int64_t s = sfirst; s < slast; ++s) {
+         const int64_t s0 = beg + 32 * (s - sfirst);
+         if (s + 1 < slast) load_segment<FWD>(g, s + 1, s0 + 32, end, lane, nxt);
+         const int64_t rho = s0 + lane;
+         const bool valid = rho < end;
+         // earlier-row values: all loads issued, then consumed in slot order
+         double z[kSlots];
+#pragma unroll
+         for (int k = 0; k < kSlots; ++k) {
+            z[k] = 0.0;
+            const int32_t c = cur.c[k];
+            if (c >= 0) {
+               const int64_t lj = FWD ? c : n - 1 - c;
+               if (lj < s0 && !(lj == s0 - 1 && have_carry)) z[k] = ld_relaxed(g.out + c);
+            }
+         }
+         double sext = 0.0, m1 = 0.0;
+         bool other_intra = false;
+#pragma unroll
+         for (int k = 0; k < kSlots; ++k) {
+            const int32_t c = cur.c[k];
+            if (c < 0) continue;
+            const int64_t lj = FWD ? c : n - 1 - c;
+            if (lj >= s0) {
+               if (lj == rho - 1) m1 = cur.a[k];
+               else other_intra = true;
+               continue;
+            }
+            double v;
+            if (lj == s0 - 1 && have_carry) v = carry;
+            else v = is_sentinel(z[k]) ? wait_value_slow(g.out + c, g.status) : z[k];
+            sext += cur.a[k] * v;
+         }
+         for (int k = kSlots; k < cur.w; ++k) {  // rows wider than the register slots
+            const int32_t c = g.sl_col[cur.off + k * 32 + lane];
+            if (c < 0) continue;
+            const double a = g.sl_val[cur.off + k * 32 + lane];
+            const int64_t lj = FWD ? c : n - 1 - c;
+            if (lj >= s0) {
+               if (lj == rho - 1) m1 = a;
+               else other_intra = true;
+               continue;
+            }
+            const double v = (lj == s0 - 1 && have_carry) ? carry : wait_value(g.out + c, g.status);
+            sext += a * v;
+         }
+         const double bi = cur.b, pv = cur.pv;
+         double zr;
+         if (!__any_sync(FULL, other_intra)) {
+            double C, M;
+            if (MODE == FWD_DILU) { C = pv * (bi - sext); M = -pv * m1; }
+            else if (MODE == FWD_SSOR) { C = (bi - sext) / pv; M = -m1 / pv; }
+            else if (MODE == BWD_DILU) { C = bi - pv * sext; M = -pv * m1; }
+            else { C = bi - sext / pv; M = -m1 / pv; }
+            if (!valid) { C = 0.0; M = 0.0; }
+            if (lane == 0) M = 0.0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+               const double Cp = __shfl_up_sync(FULL, C, o);
+               const double Mp = __shfl_up_sync(FULL, M, o);
+               if (lane >= o) {
+                  C = C + M * Cp;
+                  M = M * Mp;
+               }
+            }
+            zr = C;
+         }
+         else {
+            // exact wave over the intra-segment couplings
+            segv[w][lane] = sentinel_value();
+            __syncwarp();
+            bool done = !valid;
+            zr = 0.0;
+            for (int round = 0; round < 32; ++round) {
+               if (!done) {
+                  bool ready = true;
+                  double acc = sext;
+                  // (re-read from the slot arrays: indexing the register
+                  // copies with a run-time k would move them to local memory)
+                  for (int k = 0; k < cur.w && ready; ++k) {
+                     const int32_t c = g.sl_col[cur.off + k * 32 + lane];
+                     if (c < 0) continue;
+                     const int64_t lj = FWD ? c : n - 1 - c;
+                     if (lj < s0) continue;
+                     const double v = segv[w][lj - s0];
+                     if (is_sentinel(v)) { ready = false; break; }
+                     acc += g.sl_val[cur.off + k * 32 + lane] * v;
+                  }
+                  if (ready) {
+                     zr = finish_row<MODE>(acc, bi, pv);
+                     done = true;
+                  }
+               }
+               __syncwarp();
+               if (done && valid) segv[w][lane] = zr;
+               __syncwarp();
+               if (__all_sync(FULL, done)) break;
+            }
+            if (!__all_sync(FULL, done) && lane == 0) atomicOr(g.status, 2);
+         }
+         if (valid) {
+            const int64_t row = FWD ? rho : n - 1 - rho;
+            st_relaxed(g.out + row, zr);
+            if (g.reset) g.reset[row] = sentinel_value();
+            if (g.dot_with) dotp += g.dot_with[row] * zr;
+         }
+         const int64_t last = min((int64_t)31, end - 1 - s0);
+         carry = __shfl_sync(FULL, zr, (int)last);
+         have_carry = true;
+         if (s + 1 < slast) cur = nxt;
+      }
+      if (g.dot_with) {
+         dotp = warp_sum(dotp);
+         int lastw = 0;
+         if (lane == 0) {
+            g.strand_dot[t] = dotp;
+            __threadfence();
+            lastw = atomicAdd(&g.ticket[1], 1) == (int)g.nstrands - 1;
+         }
+         lastw = __shfl_sync(FULL, lastw, 0);
+         if (lastw) {
+            __threadfence();
+            double acc = 0.0;
+            for (int64_t q = lane; q < g.nstrands; q += 32) acc += ld_relaxed(g.strand_dot + q);
+            acc = warp_sum(acc);
+            if (lane == 0) *g.dot_out = acc;
+         }
+      }
+   }
+}
+
+__global__ void slot_values(int64_t total, const int32_t* src, const double* val, double* out)
+{
+   int64_t stride = (int64_t)gridDim.x * blockDim.x;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+      const int32_t s = src[i];
+      out[i] = s >= 0 ? val[s] : 0.0;
+   }
+}
+
 // chain[rho] = 1 when logical row rho depends on logical row rho-1
 __global__ void chain_flags(int64_t n, const int32_t* rp, const int32_t* col, const int32_t* dpos,
                             int fwd, int8_t* chain)
@@ -421,6 +645,100 @@ void build_plan(ofg_matrix* A, bool fwd, SweepPlan& plan)
    plan.start.upload(starts.data(), starts.size());
    plan.strand_dot.alloc(plan.nstrands > 0 ? plan.nstrands : 1);
    plan.ticket.alloc(4);
+
+   // slot layout: one 32-row segment per warp step, dependency entries
+   // column-major in CSR column order
+   std::vector<int32_t> rp = A->row_ptr.to_host(n + 1);
+   std::vector<int32_t> col = A->col.to_host(A->nnz);
+   std::vector<int32_t> dp = A->dpos.to_host(n);
+   auto dep_range = [&](int64_t rho, int32_t& kb, int32_t& ke) {
+      const int64_t r = fwd ? rho : n - 1 - rho;
+      if (fwd) { kb = rp[r]; ke = dp[r]; }
+      else { kb = dp[r] + 1; ke = rp[r + 1]; }
+   };
+   std::vector<int32_t> tseg(plan.nstrands + 1, 0), seg_off(1, 0);
+   for (int64_t t = 0; t < plan.nstrands; ++t) {
+      const int64_t b = starts[t], e = starts[t + 1];
+      for (int64_t s0 = b; s0 < e; s0 += 32) {
+         int32_t wmax = 0;
+         for (int64_t rho = s0; rho < std::min(e, s0 + 32); ++rho) {
+            int32_t kb, ke;
+            dep_range(rho, kb, ke);
+            wmax = std::max(wmax, ke - kb);
+         }
+         seg_off.push_back(seg_off.back() + 32 * wmax);
+      }
+      tseg[t + 1] = (int32_t)(seg_off.size() - 1);
+   }
+   const int64_t nslot = seg_off.back();
+   OFG_REQUIRE(nslot < (int64_t(1) << 31), OFG_ERR_PATTERN, "sweep layout exceeds 2^31 slots");
+   std::vector<int32_t> slc(nslot > 0 ? nslot : 1, -1), sls(nslot > 0 ? nslot : 1, -1);
+   for (int64_t t = 0, s = 0; t < plan.nstrands; ++t) {
+      const int64_t b = starts[t], e = starts[t + 1];
+      for (int64_t s0 = b; s0 < e; s0 += 32, ++s) {
+         for (int64_t rho = s0; rho < std::min(e, s0 + 32); ++rho) {
+            int32_t kb, ke;
+            dep_range(rho, kb, ke);
+            for (int32_t k = kb; k < ke; ++k) {
+               const int64_t slot = seg_off[s] + (int64_t)(k - kb) * 32 + (rho - s0);
+               slc[slot] = col[k];
+               sls[slot] = k;
+            }
+         }
+      }
+   }
+   plan.nseg = (int64_t)seg_off.size() - 1;
+   plan.tseg.alloc(tseg.size());
+   plan.tseg.upload(tseg.data(), tseg.size());
+   plan.seg_off.alloc(seg_off.size());
+   plan.seg_off.upload(seg_off.data(), seg_off.size());
+   plan.sl_col.alloc(slc.size());
+   plan.sl_col.upload(slc.data(), slc.size());
+   plan.sl_src.alloc(sls.size());
+   plan.sl_src.upload(sls.data(), sls.size());
+   plan.sl_val.alloc(sls.size());
+   OFG_CUDA(cudaStreamSynchronize(stream()));
+}
+
+void fill_slot_values(ofg_matrix* A, SweepPlan& plan)
+{
+   const int64_t total = plan.sl_val.n;
+   slot_values<<<grid_for(total, 256), 256, 0, stream()>>>(total, plan.sl_src.p, A->val.p,
+                                                           plan.sl_val.p);
+   count_launch();
+   OFG_LAUNCH_CHECK();
+}
+
+SolveArgs solve_args(ofg_prec* P, const SweepPlan& plan)
+{
+   SolveArgs g{};
+   g.n = P->A->n;
+   g.tseg = plan.tseg.p;
+   g.seg_off = plan.seg_off.p;
+   g.sl_col = plan.sl_col.p;
+   g.sl_val = plan.sl_val.p;
+   g.piv = P->pivot.p;
+   g.sstart = plan.start.p;
+   g.nstrands = plan.nstrands;
+   g.ticket = plan.ticket.p;
+   g.strand_dot = plan.strand_dot.p;
+   g.status = P->status.p;
+   return g;
+}
+
+template <int MODE>
+void launch_solve(ofg_prec* P, SweepPlan& plan, SolveArgs g)
+{
+   if (!plan.nstrands) return;
+   OFG_CUDA(cudaMemsetAsync(plan.ticket.p, 0, 4 * sizeof(int), stream()));
+   int blocks = (int)std::min<int64_t>((plan.nstrands + kWarpsPerBlock - 1) / kWarpsPerBlock,
+                                       (int64_t)P->grid);
+   if (blocks < 1) blocks = 1;
+   g.worked = prof_begin();
+   solve_sweep<MODE><<<blocks, kWarpsPerBlock * 32, 0, stream()>>>(g);
+   prof_end(PROF_SWEEP, 0.0);
+   count_launch();
+   OFG_LAUNCH_CHECK();
 }
 
 SweepArgs base_args(ofg_prec* P, const SweepPlan& plan)
@@ -509,6 +827,8 @@ void prec_setup(ofg_prec* P)
    }
    P->status.zero();
    fill_sentinel(P->t.p, n);
+   fill_slot_values(A, P->fwd);
+   fill_slot_values(A, P->bwd);
    if (P->type == OFG_DILU || P->type == OFG_ILU) {
       if (!P->tpos.p) {
          P->tpos.alloc(A->nnz > 0 ? A->nnz : 1);
@@ -548,15 +868,15 @@ void prec_apply_device(ofg_prec* P, const double* r, double* z, double* rz, cons
    }
    const bool dilu = (P->type != OFG_SSOR);
    // forward: t = L-solve(r); clears z for the backward sweep
-   SweepArgs f = base_args(P, P->fwd);
+   SolveArgs f = solve_args(P, P->fwd);
    f.in = r;
    f.out = P->t.p;
    f.reset = z;
    f.skip = skip;
-   if (dilu) launch_sweep<FWD_DILU>(P, P->fwd, f);
-   else launch_sweep<FWD_SSOR>(P, P->fwd, f);
+   if (dilu) launch_solve<FWD_DILU>(P, P->fwd, f);
+   else launch_solve<FWD_SSOR>(P, P->fwd, f);
    // backward: z = U-solve(t); clears t for the next application
-   SweepArgs b = base_args(P, P->bwd);
+   SolveArgs b = solve_args(P, P->bwd);
    b.in = P->t.p;
    b.out = z;
    b.reset = P->t.p;
@@ -565,8 +885,8 @@ void prec_apply_device(ofg_prec* P, const double* r, double* z, double* rz, cons
       b.dot_with = r;
       b.dot_out = rz;
    }
-   if (dilu) launch_sweep<BWD_DILU>(P, P->bwd, b);
-   else launch_sweep<BWD_SSOR>(P, P->bwd, b);
+   if (dilu) launch_solve<BWD_DILU>(P, P->bwd, b);
+   else launch_solve<BWD_SSOR>(P, P->bwd, b);
 }
 
 }  // namespace ofg
