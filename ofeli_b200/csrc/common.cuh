@@ -180,6 +180,31 @@ struct InOut {
    }
 };
 
+// ----------------------------------------------- programmatic dependent launch
+// A kernel launched with launch_pdl may start while the previous kernel of
+// the stream drains; it must call pdl_wait() before touching anything the
+// previous kernels write (pdl_wait returns once they completed and their
+// memory is visible), and calls pdl_release() to let its own successor start.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;"); }
+
+template <typename... KArgs, typename... Args>
+void launch_pdl(void (*kernel)(KArgs...), unsigned grid, unsigned block, Args... args)
+{
+   cudaLaunchConfig_t cfg = {};
+   cfg.gridDim = dim3(grid);
+   cfg.blockDim = dim3(block);
+   cfg.dynamicSmemBytes = 0;
+   cfg.stream = stream();
+   cudaLaunchAttribute attr[1];
+   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+   attr[0].val.programmaticStreamSerializationAllowed = 1;
+   cfg.attrs = attr;
+   cfg.numAttrs = 1;
+   OFG_CUDA(cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...));
+   count_launch();
+}
+
 inline unsigned grid_for(int64_t work, int block, int max_blocks_per_sm = 8)
 {
    int64_t g = (work + block - 1) / block;

@@ -75,6 +75,8 @@ __global__ void __launch_bounds__(kRedBlock, 8) cg_direction(int64_t n, const do
                                                           const double* __restrict__ z, double* p,
                                                           const CGState* S)
 {
+   pdl_wait();
+   pdl_release();
    if (S->done) return;
    const bool first = S->it == 0;
    const double beta = first ? 0.0 : S->rho / S->rho_old;
@@ -94,6 +96,8 @@ __global__ void __launch_bounds__(kRedBlock, 8) cg_spmv(int64_t n, int64_t nslic
                                                      double* partials, unsigned* counter,
                                                      int* worked)
 {
+   pdl_wait();
+   pdl_release();
    if (S->done) return;
    prof_mark(worked);
    double v[1] = {0.0};
@@ -122,6 +126,8 @@ __global__ void __launch_bounds__(kRedBlock, 8) cg_update(int64_t n, double* x,
                                                        double* partials, unsigned* counter,
                                                        double tol, int max_it, double* hist)
 {
+   pdl_wait();
+   pdl_release();
    if (S->done) return;
    const double a = S->alpha;
    double v[2] = {0.0, 0.0};
@@ -396,15 +402,16 @@ void cg_iteration(ofg_prec* P, int64_t n, double* x, double* r, double* p, doubl
    ofg_matrix* A = P->A;
    const unsigned g = red_grid(n);
    if (PT == PT_SWEEP) prec_apply_device(P, r, z, &S->rho, &S->done);
-   cg_direction<PT><<<g, kRedBlock, 0, stream()>>>(n, r, P->pivot.p, z, p, S);
+   // programmatic dependent launch: each kernel's blocks start while the
+   // previous kernel drains its reduction tail
+   launch_pdl(cg_direction<PT>, g, kRedBlock, n, r, P->pivot.p, z, p, S);
    int* worked = prof_begin();
-   cg_spmv<<<grid_for(A->nslices * 32, kRedBlock, 8), kRedBlock, 0, stream()>>>(
-      n, A->nslices, A->sell_ptr.p, A->sell_col.p, A->sell_val.p, p, q, S, rs.partials.p,
-      rs.counter.p, worked);
+   launch_pdl(cg_spmv, grid_for(A->nslices * 32, kRedBlock, 8), kRedBlock, n, A->nslices,
+              A->sell_ptr.p, A->sell_col.p, A->sell_val.p, p, q, S, rs.partials.p, rs.counter.p,
+              worked);
    prof_end(PROF_SPMV64, 12.0 * A->nnz + 20.0 * A->n + 4.0);
-   cg_update<PT><<<g, kRedBlock, 0, stream()>>>(n, x, p, r, q, P->pivot.p, S, rs.partials.p,
-                                                rs.counter.p, tol, max_it, hist);
-   count_launch(3);
+   launch_pdl(cg_update<PT>, g, kRedBlock, n, x, p, r, q, P->pivot.p, S, rs.partials.p,
+              rs.counter.p, tol, max_it, hist);
    OFG_LAUNCH_CHECK();
 }
 

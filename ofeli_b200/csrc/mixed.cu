@@ -127,6 +127,8 @@ __global__ void __launch_bounds__(kRedBlock, 8) mx_spmv(int64_t nquads, const in
                                                      double* partials, unsigned* counter,
                                                      int* worked)
 {
+   pdl_wait();
+   pdl_release();
    if (S->pause) return;
    prof_mark(worked);
    double v[1] = {0.0};
@@ -167,6 +169,8 @@ __global__ void __launch_bounds__(kRedBlock, 8) mx_update(int64_t nquads, float*
                                                        double delta, double tol, double scale,
                                                        int max_inner, int mode)
 {
+   pdl_wait();
+   pdl_release();
    if (S->pause) return;
    const float a = (float)S->alpha;
    double v[2] = {0.0, 0.0};
@@ -211,6 +215,8 @@ __global__ void __launch_bounds__(kRedBlock, 8) mx_direction(int64_t nquads,
                                                           const float* __restrict__ dinv, float* p,
                                                           const MixState* S)
 {
+   pdl_wait();
+   pdl_release();
    if (S->pause) return;
    const int it = S->it;
    const float beta = (float)(S->rho[it & 1] / S->rho[(it + 1) & 1]);
@@ -332,22 +338,21 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
       int batch = 8;
       for (;;) {
          for (int k = 0; k < batch; ++k) {
+            // the three kernels of an iteration chain with programmatic
+            // dependent launch: each one's blocks start while the previous
+            // one drains its reduction tail
             int* worked = prof_begin();
             if (inner_bits == 32)
-               mx_spmv<float><<<gq, kRedBlock, 0, stream()>>>(nquads, A->sell_ptr.p, A->sell_col.p,
-                                                             A->sell_val32.p, p.p, q.p, S.p,
-                                                             partials.p, counter.p, worked);
+               launch_pdl(mx_spmv<float>, gq, kRedBlock, nquads, A->sell_ptr.p, A->sell_col.p,
+                          A->sell_val32.p, p.p, q.p, S.p, partials.p, counter.p, worked);
             else
-               mx_spmv<__nv_bfloat16><<<gq, kRedBlock, 0, stream()>>>(
-                  nquads, A->sell_ptr.p, A->sell_col.p, v16.p, p.p, q.p, S.p, partials.p,
-                  counter.p, worked);
+               launch_pdl(mx_spmv<__nv_bfloat16>, gq, kRedBlock, nquads, A->sell_ptr.p,
+                          A->sell_col.p, v16.p, p.p, q.p, S.p, partials.p, counter.p, worked);
             prof_end(inner_bits == 32 ? PROF_SPMV32 : PROF_SPMV16,
                      (inner_bits == 32 ? 8.0 : 6.0) * A->nnz + 12.0 * n + 4.0);
-            mx_update<<<gq, kRedBlock, 0, stream()>>>(nquads, d.p, p.p, rr.p, q.p, dinv.p, S.p,
-                                                      partials.p, counter.p, inner_tol, tol, scale,
-                                                      max_inner, mode);
-            mx_direction<<<gq, kRedBlock, 0, stream()>>>(nquads, rr.p, dinv.p, p.p, S.p);
-            count_launch(3);
+            launch_pdl(mx_update, gq, kRedBlock, nquads, d.p, p.p, rr.p, q.p, dinv.p, S.p,
+                       partials.p, counter.p, inner_tol, tol, scale, max_inner, mode);
+            launch_pdl(mx_direction, gq, kRedBlock, nquads, rr.p, dinv.p, p.p, S.p);
          }
          OFG_LAUNCH_CHECK();
          S.download(&h, 1);

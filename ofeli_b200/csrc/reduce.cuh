@@ -43,9 +43,12 @@ __device__ __forceinline__ bool grid_reduce(double (&v)[NV], double* partials, u
    double t[NV];
 #pragma unroll
    for (int i = 0; i < NV; ++i) t[i] = 0.0;
+   // L2 loads (the partials were published before the counter), unrolled so
+   // that they are in flight together
+#pragma unroll 4
    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
 #pragma unroll
-      for (int i = 0; i < NV; ++i) t[i] += ld_relaxed(partials + (size_t)b * NV + i);
+      for (int i = 0; i < NV; ++i) t[i] += __ldcg(partials + (size_t)b * NV + i);
    __syncthreads();
 #pragma unroll
    for (int i = 0; i < NV; ++i) {
