@@ -201,6 +201,22 @@ int ofg_solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, cons
 /* FP64 true relative residual ||b - A x|| / ||b|| on the device. */
 int ofg_residual(const ofg_matrix* A, const double* b, const double* x, double* rel);
 
+/* Jacobi-preconditioned CG (the DIAG case of ofg_cg, same arguments and
+ * return convention) for callers that cannot allocate device memory while
+ * running -- services that reserve their whole memory budget at start-up,
+ * or host frameworks that own the allocator.  No counterpart in OFELI.
+ * Everything is passed as device memory: the CSR matrix with int32 0-based
+ * row_ptr (n+1) and col, FP64 values, b, and x (initial guess in, solution
+ * out).  The solve allocates nothing: its scratch is one fixed device array
+ * inside the library, held by every GPU that loads it until the process
+ * exits.  Limit: n <= 131072 rows (larger systems are rejected with
+ * OFG_ERR_SIZE).  Calls that overlap on the GPU share that array and race;
+ * serialise them.  The first call on a device looks the array up
+ * (cudaGetSymbolAddress) and should come before any stream capture. */
+int ofg_cg_diag_noalloc(int64_t n, const int32_t* row_ptr, const int32_t* col, const double* val,
+                        const double* b, double* x, int max_it, double toler, int* result,
+                        double* res);
+
 #ifdef __cplusplus
 }
 #endif

@@ -68,6 +68,7 @@ SIGNATURES = {
     "ofg_solve_mixed": (_i32, [_p, _i32, _i32, _i32, _p, _p, _i32, _i32, _d, _d, _pi32, _pi32,
                                _pd]),
     "ofg_residual": (_i32, [_p, _p, _p, _pd]),
+    "ofg_cg_diag_noalloc": (_i32, [_i64, _p, _p, _p, _p, _p, _i32, _d, _pi32, _pd]),
 }
 
 _lib = None
