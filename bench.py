@@ -30,6 +30,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 
 METRIC = "FP64-accurate solves/sec (2-D P1 Poisson 2049x2049, true rel. residual <= 1e-10)"
+METRIC_3D = "FP64-accurate solves/sec (3-D P1 variable-k diffusion 129^3, true rel. residual <= 1e-10)"
 UNIT = "solves/s"
 SEED = 1234
 TOL = 1e-10
@@ -46,6 +47,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nx", type=int, default=2048, help="cells per side (nodes = nx+1)")
+    ap.add_argument("--workload", default="poisson2d", choices=["poisson2d", "kuhn3d"],
+                    help="poisson2d: the headline 2-D problem; kuhn3d: the 3-D "
+                         "variable-coefficient problem (129^3 Kuhn cube, lognormal k)")
+    ap.add_argument("--m3d", type=int, default=128, help="kuhn3d cells per side")
     ap.add_argument("--inner-bits", type=int, default=32, choices=[32, 16])
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 CG+D-ILU solve")
     ap.add_argument("--cpu-iters", type=int, default=10, help="CG iterations per CPU sample")
@@ -153,6 +158,33 @@ def cpu_baseline_port(nx, iters):
             "host_cores": os.cpu_count()}
 
 
+def cpu_baseline_port3d(M, iters, full_iters):
+    """The oracle port, 1 thread, on the 3-D problem: assembly + D-ILU setup
+    + `iters` CG iterations, extrapolated to the CG + ILU iteration count of
+    the full solve (the GPU plain path's count, which equals OFELI's wherever
+    both were run)."""
+    from oracle import oracle as O
+    from ofeli_b200 import fields
+    xyz, elem, code = O.mesh3d(M)
+    cent = xyz.reshape(-1, 3)[elem.reshape(-1, 4)].mean(axis=1)
+    k = fields.lognormal_k(SEED, cent, 1.5, 0.1, grid=256)
+    f = fields.uniform_pm1(SEED, code.size)
+    dof, n = O.number_equations(code)
+    rp, ci = O.node_graph(elem, 4, dof, n)
+    t0 = time.perf_counter()
+    a, b = O.assemble(3, xyz, elem, dof, code, n, rp, ci, k=k, f=f, bc=np.zeros(code.size))
+    t1 = time.perf_counter()
+    O.cg(rp, ci, a, b, O.ILU, iters, 1e-300)
+    t2 = time.perf_counter()
+    per_it = (t2 - t1) / iters
+    t_solve = (t1 - t0) + per_it * abs(full_iters)
+    return {"value": 1.0 / t_solve, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": "oracle port, 1 thread: assembly + D-ILU setup + %d CG iterations on the "
+                      "%d^3 Kuhn cube, solve extrapolated to %d iterations (%.3f s assembly, "
+                      "%.4f s/iter)" % (iters, M + 1, abs(full_iters), t1 - t0, per_it),
+            "host_cores": os.cpu_count()}
+
+
 # --------------------------------------------------------- reference arm ----
 def run_reference(args):
     from oracle import oracle as O
@@ -225,11 +257,25 @@ def run_ours(args):
     torch.cuda.set_stream(work_stream)
     capi.call("ofg_set_stream", ctypes.c_void_p(work_stream.cuda_stream))
     nx = args.nx
-    mesh = F.Mesh(0.0, 1.0, 0.0, 1.0, nx, nx, 1, 1, 1, 1)
+    dev = torch.device("cuda", local)
+    k_dev = None
+    if args.workload == "kuhn3d":
+        M = args.m3d
+        mesh = F.Mesh.kuhn(M)
+        coords, elem, _, _ = mesh.arrays()
+        cent = coords.reshape(-1, 3)[elem.reshape(-1, 4)].mean(axis=1)
+        k_host = fields.lognormal_k(SEED, cent, 1.5, 0.1, grid=256)
+        del coords, elem, cent
+        k_dev = torch.from_numpy(k_host).to(dev)
+        workload = ("3-D P1 diffusion -div(k grad u) = f, Kuhn cube %d^3 nodes (%d tetrahedra), "
+                    "k = exp(g), g Gaussian (sigma 1.5, corr. length 0.1), contrast %.1e"
+                    % (M + 1, 6 * M ** 3, k_host.max() / k_host.min()))
+    else:
+        mesh = F.Mesh(0.0, 1.0, 0.0, 1.0, nx, nx, 1, 1, 1, 1)
+        workload = "2-D P1 Poisson, %dx%d nodes" % (nx + 1, nx + 1)
     A = F.SpMatrix(mesh)
     n, nn = A.n, mesh.nn
     f_host = fields.uniform_pm1(SEED, nn)
-    dev = torch.device("cuda", local)
     f_dev = torch.from_numpy(f_host).to(dev)
     b_dev = torch.zeros(n, dtype=torch.float64, device=dev)
     x_dev = torch.zeros(n, dtype=torch.float64, device=dev)
@@ -238,19 +284,20 @@ def run_ours(args):
     stream = work_stream
 
     def step_device():
-        capi.call("ofg_assemble_p1", mesh._h, A._h, None, P(f_dev), None, P(b_dev))
+        capi.call("ofg_assemble_p1", mesh._h, A._h, P(k_dev), P(f_dev), None, P(b_dev))
         x_dev.zero_()
         o, i, r = F.solve_mixed(A, b_dev, x_dev, prec=F.DIAG_PREC, inner_bits=args.inner_bits,
                                 toler=TOL)
         capi.call("ofg_insert_bc", mesh._h, P(x_dev), None, P(u_dev))
         return o, i, r
 
+    k_pin = k_dev.cpu().pin_memory() if k_dev is not None else None
     f_pin = torch.from_numpy(f_host).pin_memory()
     u_pin = torch.zeros(nn, dtype=torch.float64).pin_memory()
 
     def step_e2e():
         # public API with host buffers: f goes up, u comes back, every step
-        capi.call("ofg_assemble_p1", mesh._h, A._h, None, P(f_pin), None, P(b_dev))
+        capi.call("ofg_assemble_p1", mesh._h, A._h, P(k_pin), P(f_pin), None, P(b_dev))
         x_dev.zero_()
         o, i, r = F.solve_mixed(A, b_dev, x_dev, prec=F.DIAG_PREC, inner_bits=args.inner_bits,
                                 toler=TOL)
@@ -325,7 +372,7 @@ def run_ours(args):
     # ------------------------------------------------ plain FP64 CG + D-ILU
     plain = None
     if not args.no_plain and rank == 0:
-        capi.call("ofg_assemble_p1", mesh._h, A._h, None, P(f_dev), None, P(b_dev))
+        capi.call("ofg_assemble_p1", mesh._h, A._h, P(k_dev), P(f_dev), None, P(b_dev))
         Pc = F.Prec(A, F.ILU_PREC)
         x_dev.zero_()
         torch.cuda.synchronize()
@@ -365,20 +412,26 @@ def run_ours(args):
     avg_us = tot_ms / max(cnt, 1) * 1e3
     achieved = (tot_bytes / max(cnt, 1)) / (avg_us * 1e-6) / 1e9 if cnt else None
     traffic = ncu_traffic("mx_spmv_f32" if args.inner_bits == 32 else "mx_spmv_bf16")
-    cpu = cpu_baseline_port(nx, args.cpu_iters) if world == 1 else None
+    if args.workload != "poisson2d":
+        traffic = None  # the committed capture is of the 2-D matrix
+    cpu = None
+    if world == 1 and args.workload == "poisson2d":
+        cpu = cpu_baseline_port(nx, args.cpu_iters)
+    elif world == 1 and plain:
+        cpu = cpu_baseline_port3d(args.m3d, args.cpu_iters, plain["iterations"])
     outer = sum(s[0] for s in stats) / len(stats)
     inner = sum(s[1] for s in stats) / len(stats)
     value = world * args.steps / (ms / 1e3)
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "metric": METRIC if args.workload == "poisson2d" else METRIC_3D, "value": value,
+        "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
         "dtype": "f64 (refinement, residual, dots) / f32 (inner CG: SpMV, Jacobi, vectors)"
         if args.inner_bits == 32 else "f64 refinement / bf16 matrix values, f32 vectors",
         "data": "synthetic",
-        "config": {"workload": "2-D P1 Poisson, %dx%d nodes (%d unknowns, %d nonzeros), "
-                               "assembly + solve to FP64 true rel. residual <= 1e-10"
-                               % (nx + 1, nx + 1, n, A.nnz),
+        "config": {"workload": "%s (%d unknowns, %d nonzeros), assembly + solve to FP64 "
+                               "true rel. residual <= 1e-10" % (workload, n, A.nnz),
                    "solver": "FP64 refinement around FP32 Jacobi-PCG (direction kept)",
                    "seed": SEED, "inputs_larger_than_l2": True,
                    "refinements_per_solve": outer, "inner_iterations_per_solve": inner},
