@@ -52,6 +52,9 @@ def parse():
                          "variable-coefficient problem (129^3 Kuhn cube, lognormal k)")
     ap.add_argument("--m3d", type=int, default=128, help="kuhn3d cells per side")
     ap.add_argument("--inner-bits", type=int, default=32, choices=[32, 16])
+    ap.add_argument("--prec", default="jacobi", choices=["jacobi", "learned"],
+                    help="preconditioner of the FP32 inner iteration (learned: kuhn3d only; "
+                         "the network is trained first, outside the timed region)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 CG+D-ILU solve")
     ap.add_argument("--cpu-iters", type=int, default=10, help="CG iterations per CPU sample")
     return ap.parse_args()
@@ -282,12 +285,28 @@ def run_ours(args):
     u_dev = torch.zeros(nn, dtype=torch.float64, device=dev)
     P = F._ptr
     stream = work_stream
+    PL, train_info, fell_back = None, None, []
+    if args.prec == "learned":
+        if args.workload != "kuhn3d":
+            raise SystemExit("--prec learned runs on the kuhn3d workload")
+        from ofeli_b200 import learned as LN
+        net, train_info = LN.train_default()
+        capi.call("ofg_assemble_p1", mesh._h, A._h, P(k_dev), P(f_dev), None, P(b_dev))
+        PL = F.Prec(A, F.LEARNED_PREC, net=net)
+
+    def solve():
+        if PL is not None:
+            PL.setMatrix()  # the network runs on the newly assembled values
+            o, i, r, fb = F.fcg_learned(PL, b_dev, x_dev, inner_bits=args.inner_bits, toler=TOL)
+            fell_back.append(fb)
+            return o, i, r
+        return F.solve_mixed(A, b_dev, x_dev, prec=F.DIAG_PREC, inner_bits=args.inner_bits,
+                             toler=TOL)
 
     def step_device():
         capi.call("ofg_assemble_p1", mesh._h, A._h, P(k_dev), P(f_dev), None, P(b_dev))
         x_dev.zero_()
-        o, i, r = F.solve_mixed(A, b_dev, x_dev, prec=F.DIAG_PREC, inner_bits=args.inner_bits,
-                                toler=TOL)
+        o, i, r = solve()
         capi.call("ofg_insert_bc", mesh._h, P(x_dev), None, P(u_dev))
         return o, i, r
 
@@ -299,8 +318,7 @@ def run_ours(args):
         # public API with host buffers: f goes up, u comes back, every step
         capi.call("ofg_assemble_p1", mesh._h, A._h, P(k_pin), P(f_pin), None, P(b_dev))
         x_dev.zero_()
-        o, i, r = F.solve_mixed(A, b_dev, x_dev, prec=F.DIAG_PREC, inner_bits=args.inner_bits,
-                                toler=TOL)
+        o, i, r = solve()
         capi.call("ofg_insert_bc", mesh._h, P(x_dev), None, P(u_pin))
         return o, i, r
 
@@ -345,8 +363,45 @@ def run_ours(args):
     capi.profile_enable(4)
     step_device()
     torch.cuda.synchronize()
-    prof = {k: capi.profile_read(k) for k in ("spmv32", "spmv16", "spmv64", "assembly")}
+    prof = {k: capi.profile_read(k) for k in ("spmv32", "spmv16", "spmv64", "assembly",
+                                              "network_gemm", "learned_apply")}
     capi.profile_enable(0)
+    learned = None
+    if PL is not None:
+        # the network's forward pass alone (one per assembled matrix)
+        for _ in range(2):
+            PL.setMatrix()
+        torch.cuda.synchronize()
+        n0 = torch.cuda.Event(enable_timing=True)
+        n1 = torch.cuda.Event(enable_timing=True)
+        n0.record(stream)
+        for _ in range(5):
+            PL.setMatrix()
+        n1.record(stream)
+        torch.cuda.synchronize()
+        net_ms = n0.elapsed_time(n1) / 5
+        capi.profile_enable(1)
+        PL.setMatrix()
+        torch.cuda.synchronize()
+        g_cnt, g_ms, g_bytes = capi.profile_read("network_gemm")
+        capi.profile_enable(0)
+        g_us = g_ms / max(g_cnt, 1) * 1e3
+        g_flops = 2.0 * n * 128 * 64  # one layer product, [n x 128] x [128 x 64]
+        a_cnt, a_ms, a_bytes = prof["learned_apply"]
+        learned = dict(train_info)
+        learned.update({
+            "network_forward_ms": net_ms,
+            "layer_gemm": {"kernel": "gemm_tc (tcgen05.mma kind::f16, BF16 -> FP32 in TMEM)",
+                           "launches": g_cnt, "avg_us": g_us,
+                           "GB/s": (g_bytes / max(g_cnt, 1)) / (g_us * 1e-6) / 1e9 if g_cnt else None,
+                           "TFLOP/s": g_flops / (g_us * 1e-6) / 1e12 if g_cnt else None},
+            "factor_apply": {"kernels": "lg_lower + lg_upper (FP32 SELL-32 products with G, G^T)",
+                             "launches": a_cnt,
+                             "avg_us": a_ms / max(a_cnt, 1) * 1e3,
+                             "GB/s": (a_bytes / max(a_cnt, 1)) / (a_ms / max(a_cnt, 1) * 1e-3) / 1e9
+                             if a_cnt else None},
+            "fell_back_steps": int(sum(1 for f in fell_back if f)),
+        })
     worst_res = max(s[2] for s in stats)
     if worst_res > TOL:
         raise SystemExit("solve missed the FP64 target: %.3e" % worst_res)
@@ -432,7 +487,9 @@ def run_ours(args):
         "data": "synthetic",
         "config": {"workload": "%s (%d unknowns, %d nonzeros), assembly + solve to FP64 "
                                "true rel. residual <= 1e-10" % (workload, n, A.nnz),
-                   "solver": "FP64 refinement around FP32 Jacobi-PCG (direction kept)",
+                   "solver": "FP64 refinement around FP32 Jacobi-PCG (direction kept)"
+                   if PL is None else "FP64 refinement around FP32 flexible CG with the learned "
+                   "preconditioner M = G^T G (network run per assembled matrix, inside the step)",
                    "seed": SEED, "inputs_larger_than_l2": True,
                    "refinements_per_solve": outer, "inner_iterations_per_solve": inner},
         "gpu_launches": launches,
@@ -448,6 +505,7 @@ def run_ours(args):
         "spmv_fp64": {"us": spmv64_us, "GB/s": spmv64_bytes / (spmv64_us * 1e-6) / 1e9,
                       "frac_of_peak": spmv64_bytes / (spmv64_us * 1e-6) / 1e9 / peak},
         "plain": plain,
+        "learned": learned,
         "cpu_baseline": cpu,
         "clocks": clk,
     }

@@ -45,11 +45,14 @@ extern "C" {
 #define OFG_ERR_NOMEM (-7)
 #define OFG_ERR_SIZE (-8)       /* size beyond a stated maximum */
 
-enum { OFG_IDENT = 0, OFG_DIAG = 1, OFG_DILU = 2, OFG_ILU = 3, OFG_SSOR = 4 };
+/* OFG_LEARNED (5) has no OFELI counterpart: M = G^T G with G predicted by a
+ * trained network (ofg_prec_create_learned). */
+enum { OFG_IDENT = 0, OFG_DIAG = 1, OFG_DILU = 2, OFG_ILU = 3, OFG_SSOR = 4, OFG_LEARNED = 5 };
 
 typedef struct ofg_matrix ofg_matrix;
 typedef struct ofg_mesh ofg_mesh;
 typedef struct ofg_prec ofg_prec;
+typedef struct ofg_learned ofg_learned;
 
 /* ---------------------------------------------------------------- runtime */
 const char* ofg_last_error(void);
@@ -63,7 +66,10 @@ int64_t ofg_launch_count(void);
  * disabling) resets the totals; while enabled (on >= 1), every on-th launch
  * of an instrumented kernel is bracketed by events on the library stream.  Families: "spmv64", "spmv32",
  * "spmv16" (SELL SpMV in FP64 / FP32 / BF16 values, inside the solvers too),
- * "sweep" (triangular sweeps), "assembly" (element colour launches).
+ * "sweep" (triangular sweeps), "assembly" (element colour launches),
+ * "network_gemm" (tensor-core layer products of the learned preconditioner's
+ * network), "learned_apply" (the two FP32 factor products inside
+ * ofg_fcg_learned).
  * *bytes = algorithmic bytes summed over the counted launches (0 when the
  * family has no bandwidth model).  Launches that found their stop flag set
  * are not counted.  No counterpart in OFELI (its Timer is wall clock). */
@@ -216,6 +222,62 @@ int ofg_residual(const ofg_matrix* A, const double* b, const double* x, double* 
 int ofg_cg_diag_noalloc(int64_t n, const int32_t* row_ptr, const int32_t* col, const double* val,
                         const double* b, double* x, int max_it, double toler, int* result,
                         double* res);
+
+/* ------------------------------------------- learned preconditioner -----
+ * No counterpart in OFELI.  A message-passing network over the matrix graph
+ * (4 layers of width 64, BF16 activations and tensor-core layer products,
+ * FP32 accumulation and FP32 master weights) predicts a lower-triangular G
+ * on the pattern of A with a positive diagonal; the preconditioner is
+ * M = G^T G (symmetric positive definite), applied as two sparse products.
+ * With freshly created parameters M is Jacobi.  The parameter vector has
+ * ofg_learned_num_params() floats (layout: W_in 4x64, b_in 64, W_l 4x(128x64),
+ * b_l 4x64, u 64, v 64, c 1). */
+int ofg_learned_create(uint64_t seed, ofg_learned** out);
+int ofg_learned_destroy(ofg_learned* L);
+int ofg_learned_num_params(void); /* returns the count, not a status */
+/* Checkpoint: parameters, Adam moments (may be NULL) and the Adam step. */
+int ofg_learned_get_params(const ofg_learned* L, float* params, float* adam_m, float* adam_v,
+                           int64_t* step);
+int ofg_learned_set_params(ofg_learned* L, const float* params, const float* adam_m,
+                           const float* adam_v, int64_t step);
+/* Training objective: 1 (default) the Kaporin number of M A,
+ * (tr(MA)/n) / det(MA)^(1/n), with the trace estimated on the pairs (scale
+ * invariant; its minimiser over the pattern is the factorised sparse
+ * approximate inverse; the pairs' errors should be spectrally flat, e.g.
+ * x* - x0 for random starting guesses x0); 0 the direct fit
+ * mean_p ||M r_p - e_p||^2 / ||e_p||^2. */
+int ofg_learned_set_loss(ofg_learned* L, int kind);
+/* Layer products on the tensor cores (default 1) or on CUDA cores (0). */
+int ofg_learned_set_tensor_cores(ofg_learned* L, int on);
+/* `steps` Adam steps (learning rate lr, batches of `batch` pairs taken in
+ * turn) on the selected objective.  R and E hold
+ * npairs residual / error vectors of length n, pair-major (FP32).
+ * loss_history (may be NULL) receives each step's batch loss (host). */
+int ofg_learned_train(ofg_learned* L, ofg_matrix* A, const float* R, const float* E, int npairs,
+                      int steps, int batch, float lr, float* loss_history);
+/* Loss and its gradient (ofg_learned_num_params floats, may be NULL) over
+ * all pairs, and the predicted factor at A's CSR positions (nnz floats,
+ * lower part, may be NULL). */
+int ofg_learned_grad(ofg_learned* L, ofg_matrix* A, const float* R, const float* E, int npairs,
+                     double* loss, float* grads, float* factor);
+/* One layer product X (rows x 128, BF16 bit patterns) times layer `layer`'s
+ * weights, on the tensor cores (out_tc) and on CUDA cores (out_cc). */
+int ofg_learned_gemm_check(ofg_learned* L, int layer, int64_t rows, const uint16_t* X,
+                           float* out_tc, float* out_cc);
+/* Preconditioner of type OFG_LEARNED for A (runs the network once; again
+ * after A's values change).  Usable with ofg_cg, ofg_gmres, ofg_prec_apply;
+ * the network must outlive it. */
+int ofg_prec_create_learned(ofg_learned* L, ofg_matrix* A, ofg_prec** out);
+/* Flexible CG with the learned preconditioner, in FP32 (inner_bits 32) or
+ * with BF16 matrix values (16), inside FP64 iterative refinement; the
+ * arguments and results are those of ofg_solve_mixed.  When the learned
+ * iteration stagnates (residual not halved in 500 iterations, not finite, or
+ * three refinements without a 10% gain) the solve continues with the plain
+ * Jacobi iteration from the last verified x and *fell_back = 1.  Converged
+ * only on the FP64 true residual. */
+int ofg_fcg_learned(ofg_prec* P, int inner_bits, const double* b, double* x, int max_outer,
+                    int max_inner, double inner_tol, double toler, int* outer, int* inner,
+                    double* true_res, int* fell_back);
 
 #ifdef __cplusplus
 }

@@ -69,6 +69,18 @@ SIGNATURES = {
                                _pd]),
     "ofg_residual": (_i32, [_p, _p, _p, _pd]),
     "ofg_cg_diag_noalloc": (_i32, [_i64, _p, _p, _p, _p, _p, _i32, _d, _pi32, _pd]),
+    "ofg_learned_create": (_i32, [ctypes.c_uint64, _pp]),
+    "ofg_learned_destroy": (_i32, [_p]),
+    "ofg_learned_num_params": (_i32, []),
+    "ofg_learned_get_params": (_i32, [_p, _p, _p, _p, _pi64]),
+    "ofg_learned_set_params": (_i32, [_p, _p, _p, _p, _i64]),
+    "ofg_learned_set_tensor_cores": (_i32, [_p, _i32]),
+    "ofg_learned_set_loss": (_i32, [_p, _i32]),
+    "ofg_learned_train": (_i32, [_p, _p, _p, _p, _i32, _i32, _i32, ctypes.c_float, _p]),
+    "ofg_learned_grad": (_i32, [_p, _p, _p, _p, _i32, _pd, _p, _p]),
+    "ofg_learned_gemm_check": (_i32, [_p, _i32, _i64, _p, _p, _p]),
+    "ofg_prec_create_learned": (_i32, [_p, _p, _pp]),
+    "ofg_fcg_learned": (_i32, [_p, _i32, _p, _p, _i32, _i32, _d, _d, _pi32, _pi32, _pd, _pi32]),
 }
 
 _lib = None

@@ -70,7 +70,7 @@ void count_launch(int n = 1);
 // nullptr when profiling is off; prof_end(kind, algorithmic bytes) after the
 // launch.  Launches that found their stop flag set are not counted.
 enum { PROF_SPMV64 = 0, PROF_SPMV32 = 1, PROF_SPMV16 = 2, PROF_SWEEP = 3, PROF_ASSEMBLY = 4,
-       kProfKinds = 5 };
+       PROF_NET_GEMM = 5, PROF_LEARNED_APPLY = 6, kProfKinds = 7 };
 bool prof_on();
 int* prof_begin();
 void prof_end(int kind, double bytes);

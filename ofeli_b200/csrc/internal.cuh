@@ -84,6 +84,18 @@ struct ofg_prec {
    ofg::DBuf<int32_t> tpos;  // D-ILU: transposed position of each lower entry
    ofg::DBuf<double> dot;    // (r, z) of the last backward sweep that was asked for it
    int grid = 0;             // blocks of the persistent sweep launch
+   // LEARNED: the network that predicts the factor G, and G (lower rows) and
+   // G^T (upper rows) as matrices of their own; M = G^T G
+   ofg_learned* net = nullptr;
+   ofg_matrix* gl = nullptr;
+   ofg_matrix* gu = nullptr;
+   ofg::DBuf<double> partials;
+   ofg::DBuf<unsigned> counter;
+   ~ofg_prec()
+   {
+      delete gl;
+      delete gu;
+   }
 };
 
 namespace ofg {
@@ -111,5 +123,11 @@ void check_status(ofg_prec* P);
 // that IEEE arithmetic never produces (results are the canonical NaN).
 constexpr unsigned long long kSentinelBits = 0x7FF4DEADBEEF0001ULL;
 void fill_sentinel(double* p, int64_t n);
+
+// learned.cu: run the network on the matrix's current values and rebuild
+// G / G^T; z = G^T G r in FP64 (r and z may alias; rz as above when they
+// do not)
+void learned_setup(ofg_prec* P);
+void learned_apply(ofg_prec* P, const double* r, double* z, double* rz, const int* skip);
 
 }  // namespace ofg

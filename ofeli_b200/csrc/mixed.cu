@@ -38,6 +38,7 @@ struct MixState {
    double bnorm, rel;          // FP64 true residual
    double rho[2];              // rho of the last two iterations, indexed by it & 1
    double alpha, rn, rmark, res0;
+   double beta;                // learned preconditioner: next direction's beta
    int it, pause, done, pad;
 };
 
@@ -76,7 +77,8 @@ __global__ void __launch_bounds__(kRedBlock, 8) mx_residual(int64_t n, const dou
 }
 
 // r_lo = (float)(r * scale) (zero in the padding); rho = (r_lo, D r_lo),
-// ||r_lo||; x_lo = 0; on a fresh start also p = D r_lo
+// ||r_lo||; x_lo = 0; on a fresh start also p = D r_lo.  Without dinv (the
+// learned preconditioner) only r_lo, ||r_lo|| and x_lo.
 __global__ void __launch_bounds__(kRedBlock, 8) mx_load_residual(int64_t n, int64_t npad,
                                                               const double* __restrict__ r,
                                                               double scale,
@@ -89,16 +91,16 @@ __global__ void __launch_bounds__(kRedBlock, 8) mx_load_residual(int64_t n, int6
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < npad; i += stride) {
       const float ri = i < n ? (float)(r[i] * scale) : 0.0f;
-      const float zi = ri * dinv[i];
+      const float zi = dinv ? ri * dinv[i] : 0.0f;
       rr[i] = ri;
       d[i] = 0.0f;
-      if (fresh) p[i] = zi;
+      if (fresh && dinv) p[i] = zi;
       v[0] += (double)ri * (double)zi;
       v[1] += (double)ri * (double)ri;
    }
    double t[2];
    if (grid_reduce<2>(v, partials, counter, t)) {
-      S->rho[S->it & 1] = t[0];
+      if (dinv) S->rho[S->it & 1] = t[0];  // else set by the learned products
       S->rn = sqrt(t[1]);
       S->rmark = S->rn;
       if (fresh) S->res0 = S->rn;
@@ -159,8 +161,9 @@ __global__ void __launch_bounds__(kRedBlock, 8) mx_spmv(int64_t nquads, const in
    if (grid_reduce<1>(v, partials, counter, t)) S->alpha = S->rho[S->it & 1] / t[0];
 }
 
-// d += alpha p, r -= alpha q; ||r||, (r, D r); decides when the host must
-// refine (mode 0) or stop the inner solve (mode 1)
+// d += alpha p, r -= alpha q; ||r||, (r, D r) when JAC; decides when the
+// host must refine (mode 0) or stop the inner solve (mode 1)
+template <bool JAC>
 __global__ void __launch_bounds__(kRedBlock, 8) mx_update(int64_t nquads, float* d,
                                                        const float* __restrict__ p, float* rr,
                                                        const float* __restrict__ q,
@@ -181,21 +184,24 @@ __global__ void __launch_bounds__(kRedBlock, 8) mx_update(int64_t nquads, float*
    const float4* q4 = reinterpret_cast<const float4*>(q);
    const float4* m4 = reinterpret_cast<const float4*>(dinv);
    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nquads; i += stride) {
-      const float4 pi = p4[i], qi = q4[i], mi = m4[i];
+      const float4 pi = p4[i], qi = q4[i];
       float4 di = d4[i], ri = r4[i];
       di.x += a * pi.x; di.y += a * pi.y; di.z += a * pi.z; di.w += a * pi.w;
       ri.x -= a * qi.x; ri.y -= a * qi.y; ri.z -= a * qi.z; ri.w -= a * qi.w;
       d4[i] = di;
       r4[i] = ri;
       v[0] += (double)ri.x * ri.x + (double)ri.y * ri.y + (double)ri.z * ri.z + (double)ri.w * ri.w;
-      v[1] += (double)ri.x * (ri.x * mi.x) + (double)ri.y * (ri.y * mi.y) +
-              (double)ri.z * (ri.z * mi.z) + (double)ri.w * (ri.w * mi.w);
+      if (JAC) {
+         const float4 mi = m4[i];
+         v[1] += (double)ri.x * (ri.x * mi.x) + (double)ri.y * (ri.y * mi.y) +
+                 (double)ri.z * (ri.z * mi.z) + (double)ri.w * (ri.w * mi.w);
+      }
    }
    double t[2];
    if (grid_reduce<2>(v, partials, counter, t)) {
       S->rn = sqrt(t[0]);
       const int it = S->it + 1;
-      S->rho[it & 1] = t[1];
+      if (JAC) S->rho[it & 1] = t[1];
       S->it = it;
       if (mode == 0) {
          // refine when the residual fell by delta, or when the recurrence
@@ -235,6 +241,110 @@ __global__ void __launch_bounds__(kRedBlock, 8) mx_direction(int64_t nquads,
    }
 }
 
+// ---- learned preconditioner M = G^T G inside the FP32 iteration --------
+// G (lower rows) and G^T (upper rows) are SELL-32 matrices with FP32 values
+// on the same slices as A; a thread owns four consecutive rows.
+__device__ __forceinline__ float4 sell_quad(const int32_t* __restrict__ sp,
+                                            const int32_t* __restrict__ scol,
+                                            const float* __restrict__ sval,
+                                            const float* __restrict__ x, int64_t r0)
+{
+   const int64_t s = r0 >> 5;
+   const int lane0 = (int)(r0 & 31);
+   const int32_t beg = sp[s], w = (sp[s + 1] - beg) >> 5;
+   float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+   const int32_t* cp = scol + beg + lane0;
+   const float* vp = sval + beg + lane0;
+#pragma unroll 4
+   for (int32_t k = 0; k < w; ++k) {
+      const int4 c = *reinterpret_cast<const int4*>(cp + k * 32);
+      const float4 a = *reinterpret_cast<const float4*>(vp + k * 32);
+      acc.x += a.x * __ldg(x + c.x);
+      acc.y += a.y * __ldg(x + c.y);
+      acc.z += a.z * __ldg(x + c.z);
+      acc.w += a.w * __ldg(x + c.w);
+   }
+   return acc;
+}
+
+// t = G r
+__global__ void __launch_bounds__(kRedBlock, 8) lg_lower(int64_t nquads, const int32_t* __restrict__ sp,
+                                                      const int32_t* __restrict__ scol,
+                                                      const float* __restrict__ sval,
+                                                      const float* __restrict__ r, float* t,
+                                                      const MixState* S, int* worked)
+{
+   pdl_wait();
+   pdl_release();
+   if (S->pause) return;
+   prof_mark(worked);
+   int64_t stride = (int64_t)gridDim.x * blockDim.x;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nquads; i += stride)
+      *reinterpret_cast<float4*>(t + i * 4) = sell_quad(sp, scol, sval, r, i * 4);
+}
+
+// z = G^T t; rho = (r, z); beta of the next direction: flexible
+// (Polak-Ribiere) -alpha (z, q) / rho_old, or rho / rho_old right after a
+// refinement replaced r (fr = 1)
+__global__ void __launch_bounds__(kRedBlock, 8) lg_upper(int64_t nquads, const int32_t* __restrict__ sp,
+                                                      const int32_t* __restrict__ scol,
+                                                      const float* __restrict__ sval,
+                                                      const float* __restrict__ t, float* z,
+                                                      const float* __restrict__ r,
+                                                      const float* __restrict__ q, MixState* S,
+                                                      double* partials, unsigned* counter, int fr,
+                                                      int* worked)
+{
+   pdl_wait();
+   pdl_release();
+   if (S->pause) return;
+   prof_mark(worked);
+   double v[2] = {0.0, 0.0};
+   int64_t stride = (int64_t)gridDim.x * blockDim.x;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nquads; i += stride) {
+      const float4 zi = sell_quad(sp, scol, sval, t, i * 4);
+      *reinterpret_cast<float4*>(z + i * 4) = zi;
+      const float4 ri = *reinterpret_cast<const float4*>(r + i * 4);
+      const float4 qi = *reinterpret_cast<const float4*>(q + i * 4);
+      v[0] += (double)ri.x * zi.x + (double)ri.y * zi.y + (double)ri.z * zi.z + (double)ri.w * zi.w;
+      v[1] += (double)qi.x * zi.x + (double)qi.y * zi.y + (double)qi.z * zi.z + (double)qi.w * zi.w;
+   }
+   double tt[2];
+   if (grid_reduce<2>(v, partials, counter, tt)) {
+      const int it = S->it;
+      const double old = S->rho[(it + 1) & 1];
+      S->rho[it & 1] = tt[0];
+      S->beta = fr ? tt[0] / old : -S->alpha * tt[1] / old;
+   }
+}
+
+// p = z + beta p (p = z on a fresh start)
+__global__ void __launch_bounds__(kRedBlock, 8) lg_direction(int64_t nquads,
+                                                          const float* __restrict__ z, float* p,
+                                                          const MixState* S, int fresh)
+{
+   pdl_wait();
+   pdl_release();
+   if (S->pause) return;
+   const float beta = fresh ? 0.f : (float)S->beta;
+   int64_t stride = (int64_t)gridDim.x * blockDim.x;
+   float4* p4 = reinterpret_cast<float4*>(p);
+   const float4* z4 = reinterpret_cast<const float4*>(z);
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nquads; i += stride) {
+      const float4 zi = z4[i];
+      if (fresh) {
+         p4[i] = zi;
+         continue;
+      }
+      float4 pi = p4[i];
+      pi.x = zi.x + beta * pi.x;
+      pi.y = zi.y + beta * pi.y;
+      pi.z = zi.z + beta * pi.z;
+      pi.w = zi.w + beta * pi.w;
+      p4[i] = pi;
+   }
+}
+
 // x += scale * d (FP64)
 __global__ void mx_correct(int64_t n, double* x, const float* __restrict__ d, double scale)
 {
@@ -268,9 +378,10 @@ __global__ void inv_diag32(int64_t n, int64_t npad, const int32_t* dpos, const d
 
 void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const double* b, double* x,
                  int max_outer, int max_inner, double inner_tol, double tol, int* outer, int* inner,
-                 double* true_res)
+                 double* true_res, ofg_prec* LP, int* fell_back)
 {
-   OFG_REQUIRE(prec_type == OFG_DIAG || prec_type == OFG_IDENT, OFG_ERR_ARG,
+   const bool learned = LP != nullptr;
+   OFG_REQUIRE(learned || prec_type == OFG_DIAG || prec_type == OFG_IDENT, OFG_ERR_ARG,
                "mixed-precision inner solver supports DIAG and IDENT");
    OFG_REQUIRE(inner_bits == 32 || inner_bits == 16, OFG_ERR_ARG, "inner_bits must be 32 or 16");
    OFG_REQUIRE(mode == 0 || mode == 1, OFG_ERR_ARG, "mode must be 0 or 1");
@@ -279,6 +390,13 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
    ensure_sell(A);
    ensure_dpos(A);
    OFG_REQUIRE(A->dpos_complete, OFG_ERR_PIVOT, "a row has no diagonal entry");
+   if (learned) {
+      if (LP->version != A->version) prec_setup(LP);
+      ensure_sell32(LP->gl);
+      ensure_sell32(LP->gu);
+      OFG_REQUIRE(LP->gl->nslices == A->nslices && LP->gu->nslices == A->nslices, OFG_ERR_ARG,
+                  "learned factor does not match the matrix");
+   }
    const int64_t npad = A->nslices * 32, nquads = npad / 4;
    DBuf<__nv_bfloat16> v16;
    if (inner_bits == 32) ensure_sell32(A);
@@ -290,11 +408,13 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
    }
    const int64_t nv = npad > 0 ? npad : 4;
    DBuf<float> dinv(nv), rr(nv), p(nv), q(nv), d(nv);
+   DBuf<float> tz(learned ? nv : 1), zz(learned ? nv : 1);
    DBuf<double> r(n > 0 ? n : 1), q64(n > 0 ? n : 1);
    DBuf<MixState> S(1);
    DBuf<int> bad(1);
    bad.zero();
    p.zero();
+   q.zero();
    const unsigned g = grid_for(std::max<int64_t>(n, nquads), kRedBlock, 8);
    DBuf<double> partials(((size_t)g + 1) * 4 + 4);
    DBuf<unsigned> counter(1);
@@ -305,6 +425,7 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
    int hb = 0;
    bad.download(&hb, 1);
    OFG_REQUIRE(!hb, OFG_ERR_PIVOT, "zero diagonal entry");
+   const float* jac = learned ? nullptr : dinv.p;
    const unsigned gq = grid_for(nquads, kRedBlock, 8);
    const unsigned gn = grid_for(n, kRedBlock, 8);
    auto true_residual = [&](int first) {
@@ -314,6 +435,19 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
       count_launch();
       OFG_LAUNCH_CHECK();
    };
+   // z = G^T G r, rho, beta, then the new direction
+   auto learned_direction = [&](int fr, int fresh) {
+      int* worked = prof_begin();
+      launch_pdl(lg_lower, gq, kRedBlock, nquads, LP->gl->sell_ptr.p, LP->gl->sell_col.p,
+                 LP->gl->sell_val32.p, rr.p, tz.p, S.p, worked);
+      prof_end(PROF_LEARNED_APPLY, 8.0 * LP->gl->nnz + 8.0 * n);
+      worked = prof_begin();
+      launch_pdl(lg_upper, gq, kRedBlock, nquads, LP->gu->sell_ptr.p, LP->gu->sell_col.p,
+                 LP->gu->sell_val32.p, tz.p, zz.p, rr.p, q.p, S.p, partials.p, counter.p, fr,
+                 worked);
+      prof_end(PROF_LEARNED_APPLY, 8.0 * LP->gu->nnz + 16.0 * n);
+      launch_pdl(lg_direction, gq, kRedBlock, nquads, zz.p, p.p, S.p, fresh);
+   };
    MixState h{};
    true_residual(1);
    S.download(&h, 1);
@@ -321,26 +455,36 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
    // mode 1 solves for d in units of ||r||; mode 0 keeps absolute units
    double scale = 1.0;
    bool fresh = true;
+   // stagnation watch of the learned iteration: the recursive residual must
+   // halve within kStallIters iterations and stay finite, and the true
+   // residual must fall at every refinement
+   constexpr int kStallIters = 500;
+   bool stalled = false;
+   int no_gain = 0;
+   double last_rel = h.rel;
    while (!h.done && n_outer < max_outer && h.it < max_inner && n > 0) {
       if (mode == 1) {
          scale = h.rel * h.bnorm;
          fresh = true;
       }
-      mx_load_residual<<<gq, kRedBlock, 0, stream()>>>(n, npad, r.p, 1.0 / scale, dinv.p, rr.p,
-                                                       p.p, d.p, fresh ? 1 : 0, S.p, partials.p,
+      mx_load_residual<<<gq, kRedBlock, 0, stream()>>>(n, npad, r.p, 1.0 / scale, jac, rr.p, p.p,
+                                                       d.p, fresh ? 1 : 0, S.p, partials.p,
                                                        counter.p);
       count_launch();
-      if (!fresh) {
+      if (learned) learned_direction(fresh ? 0 : 1, fresh ? 1 : 0);
+      else if (!fresh) {
          mx_direction<<<gq, kRedBlock, 0, stream()>>>(nquads, rr.p, dinv.p, p.p, S.p);
          count_launch();
       }
       fresh = false;
+      int mark_it = h.it;
+      double mark_rn = h.rel * h.bnorm / scale;
       int batch = 8;
       for (;;) {
          for (int k = 0; k < batch; ++k) {
-            // the three kernels of an iteration chain with programmatic
-            // dependent launch: each one's blocks start while the previous
-            // one drains its reduction tail
+            // the kernels of an iteration chain with programmatic dependent
+            // launch: each one's blocks start while the previous one drains
+            // its reduction tail
             int* worked = prof_begin();
             if (inner_bits == 32)
                launch_pdl(mx_spmv<float>, gq, kRedBlock, nquads, A->sell_ptr.p, A->sell_col.p,
@@ -350,21 +494,59 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
                           A->sell_col.p, v16.p, p.p, q.p, S.p, partials.p, counter.p, worked);
             prof_end(inner_bits == 32 ? PROF_SPMV32 : PROF_SPMV16,
                      (inner_bits == 32 ? 8.0 : 6.0) * A->nnz + 12.0 * n + 4.0);
-            launch_pdl(mx_update, gq, kRedBlock, nquads, d.p, p.p, rr.p, q.p, dinv.p, S.p,
-                       partials.p, counter.p, inner_tol, tol, scale, max_inner, mode);
-            launch_pdl(mx_direction, gq, kRedBlock, nquads, rr.p, dinv.p, p.p, S.p);
+            if (learned) {
+               launch_pdl(mx_update<false>, gq, kRedBlock, nquads, d.p, p.p, rr.p, q.p, jac, S.p,
+                          partials.p, counter.p, inner_tol, tol, scale, max_inner, mode);
+               learned_direction(0, 0);
+            }
+            else {
+               launch_pdl(mx_update<true>, gq, kRedBlock, nquads, d.p, p.p, rr.p, q.p, dinv.p, S.p,
+                          partials.p, counter.p, inner_tol, tol, scale, max_inner, mode);
+               launch_pdl(mx_direction, gq, kRedBlock, nquads, rr.p, dinv.p, p.p, S.p);
+            }
          }
          OFG_LAUNCH_CHECK();
          S.download(&h, 1);
+         if (learned) {
+            if (!std::isfinite(h.rn)) stalled = true;
+            else if (h.it - mark_it >= kStallIters) {
+               if (h.rn > 0.5 * mark_rn) stalled = true;
+               mark_it = h.it;
+               mark_rn = h.rn;
+            }
+            if (stalled) break;
+         }
          if (h.pause) break;
          batch = std::min(batch * 2, 64);
       }
+      if (stalled) break;
       // refinement step in FP64
       mx_correct<<<gn, kRedBlock, 0, stream()>>>(n, x, d.p, scale);
       count_launch();
       true_residual(0);
       S.download(&h, 1);
       n_outer++;
+      if (learned) {
+         no_gain = (h.rel > 0.9 * last_rel) ? no_gain + 1 : 0;
+         last_rel = h.rel;
+         if (!std::isfinite(h.rel) || no_gain >= 3) {
+            stalled = true;
+            break;
+         }
+      }
+   }
+   if (learned && stalled && !h.done) {
+      // fallback: the plain Jacobi iteration from the last x whose FP64
+      // residual was measured (a non-finite x is reset to zero)
+      if (!std::isfinite(h.rel)) OFG_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), stream()));
+      if (fell_back) *fell_back = 1;
+      int o2 = 0, i2 = 0;
+      solve_mixed(A, OFG_DIAG, inner_bits, mode, b, x, std::max(1, max_outer - n_outer),
+                  std::max(1, max_inner - h.it), inner_tol, tol, &o2, &i2, true_res, nullptr,
+                  nullptr);
+      *outer = n_outer + o2;
+      *inner = h.it + i2;
+      return;
    }
    *outer = n_outer;
    *inner = h.it;
@@ -385,7 +567,28 @@ extern "C" int ofg_solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int
       In<double> db(b, A->n);
       InOut<double> dx(x, A->n, true);
       solve_mixed(A, prec_type, inner_bits, mode, db.d, dx.d, max_outer, max_inner, inner_tol,
-                  toler, outer, inner, true_res);
+                  toler, outer, inner, true_res, nullptr, nullptr);
+      dx.finish();
+   });
+}
+
+// Flexible CG with the learned preconditioner in FP32 inside FP64 iterative
+// refinement (mode 0); falls back to the plain Jacobi iteration when the
+// learned iteration stagnates (*fell_back = 1).  Convergence is declared on
+// the FP64 true residual only.
+extern "C" int ofg_fcg_learned(ofg_prec* P, int inner_bits, const double* b, double* x,
+                               int max_outer, int max_inner, double inner_tol, double toler,
+                               int* outer, int* inner, double* true_res, int* fell_back)
+{
+   return guarded("ofg_fcg_learned", [&] {
+      OFG_REQUIRE(P && b && x && outer && inner && true_res, OFG_ERR_ARG, "null argument");
+      OFG_REQUIRE(P->type == OFG_LEARNED, OFG_ERR_ARG, "not a learned preconditioner");
+      if (fell_back) *fell_back = 0;
+      ofg_matrix* A = P->A;
+      In<double> db(b, A->n);
+      InOut<double> dx(x, A->n, true);
+      solve_mixed(A, OFG_DIAG, inner_bits, 0, db.d, dx.d, max_outer, max_inner, inner_tol, toler,
+                  outer, inner, true_res, P, fell_back);
       dx.finish();
    });
 }

@@ -797,6 +797,10 @@ void prec_setup(ofg_prec* P)
                "a row has no diagonal entry");
    P->version = A->version;
    if (P->type == OFG_IDENT) return;
+   if (P->type == OFG_LEARNED) {
+      learned_setup(P);
+      return;
+   }
    P->pivot.reserve(n > 0 ? n : 1);
    DBuf<int> bad(1);
    int big = INT32_MAX;
@@ -864,6 +868,7 @@ void prec_apply_device(ofg_prec* P, const double* r, double* z, double* rz, cons
          count_launch();
          OFG_LAUNCH_CHECK();
          return;
+      case OFG_LEARNED: learned_apply(P, r, z, rz, skip); return;
       default: break;
    }
    const bool dilu = (P->type != OFG_SSOR);

@@ -140,7 +140,8 @@ void prof_collect()
    g_pending.clear();
 }
 
-static const char* kProfNames[kProfKinds] = {"spmv64", "spmv32", "spmv16", "sweep", "assembly"};
+static const char* kProfNames[kProfKinds] = {"spmv64", "spmv32",       "spmv16",       "sweep",
+                                             "assembly", "network_gemm", "learned_apply"};
 
 bool is_device_ptr(const void* p)
 {

@@ -22,9 +22,11 @@ import math
 
 import numpy as np
 
-from . import capi
+from . import capi, fields
 
 IDENT_PREC, DIAG_PREC, DILU_PREC, ILU_PREC, SSOR_PREC = 0, 1, 2, 3, 4
+# no OFELI counterpart: M = G^T G predicted by a trained network (LearnedNet)
+LEARNED_PREC = 5
 DIRECT_SOLVER, CG_SOLVER, CGS_SOLVER, BICG_SOLVER, BICG_STAB_SOLVER, GMRES_SOLVER = 1, 2, 3, 4, 5, 6
 OFELI_EPSMCH = 2.220446049250313e-16
 
@@ -121,7 +123,7 @@ class Mesh:
         _call("ofg_mesh_set_coords", self._h, _ptr(coords))
 
     def __del__(self):
-        if getattr(self, "_h", None) and capi._lib is not None:
+        if getattr(self, "_h", None) and capi is not None and capi._lib is not None:
             capi.lib().ofg_mesh_destroy(self._h)
             self._h = None
 
@@ -190,24 +192,31 @@ class SpMatrix:
         return self.Mult(x)
 
     def __del__(self):
-        if getattr(self, "_h", None) and capi._lib is not None:
+        if getattr(self, "_h", None) and capi is not None and capi._lib is not None:
             capi.lib().ofg_matrix_destroy(self._h)
             self._h = None
 
 
 class Prec:
-    """Prec<real_t>(A, type): DIAG, DILU/ILU (diagonal ILU), SSOR (SGS)."""
+    """Prec<real_t>(A, type): DIAG, DILU/ILU (diagonal ILU), SSOR (SGS); and
+    Prec(A, LEARNED_PREC, net=LearnedNet) for the learned M = G^T G."""
 
-    def __init__(self, A, type=DIAG_PREC):
+    def __init__(self, A, type=DIAG_PREC, net=None):
         self.A = A
         self.type = type
+        self.net = net
         h = ctypes.c_void_p()
-        _call("ofg_prec_create", A._h, type, ctypes.byref(h))
+        if type == LEARNED_PREC:
+            if net is None:
+                raise OFELIException("LEARNED_PREC needs a LearnedNet")
+            _call("ofg_prec_create_learned", net._h, A._h, ctypes.byref(h))
+        else:
+            _call("ofg_prec_create", A._h, type, ctypes.byref(h))
         self._h = h
 
     def setMatrix(self, A=None):
         if A is not None and A is not self.A:
-            self.__init__(A, self.type)
+            self.__init__(A, self.type, self.net)
         else:
             _call("ofg_prec_update", self._h)
 
@@ -224,7 +233,7 @@ class Prec:
         return p
 
     def __del__(self):
-        if getattr(self, "_h", None) and capi._lib is not None:
+        if getattr(self, "_h", None) and capi is not None and capi._lib is not None:
             capi.lib().ofg_prec_destroy(self._h)
             self._h = None
 
@@ -270,6 +279,113 @@ def solve_mixed(A, b, x, prec=DIAG_PREC, inner_bits=32, toler=1e-10, max_outer=2
     _call("ofg_solve_mixed", A._h, prec, inner_bits, mode, _ptr(b), _ptr(x), max_outer,
           max_inner, inner_tol, toler, ctypes.byref(o), ctypes.byref(i), ctypes.byref(r))
     return o.value, i.value, r.value
+
+
+class LearnedNet:
+    """The network of the learned preconditioner (4 message-passing layers of
+    width 64, BF16 tensor-core layer products, FP32 master weights, Adam).
+    loss 1 (default): Kaporin number of M A estimated on the pairs; loss 0:
+    mean ||M r - e||^2 / ||e||^2."""
+
+    def __init__(self, seed=1, loss=1):
+        h = ctypes.c_void_p()
+        _call("ofg_learned_create", ctypes.c_uint64(seed), ctypes.byref(h))
+        self._h = h
+        self.set_loss(loss)
+
+    @staticmethod
+    def num_params():
+        return int(capi.lib().ofg_learned_num_params())
+
+    def set_loss(self, kind):
+        _call("ofg_learned_set_loss", self._h, int(kind))
+
+    def set_tensor_cores(self, on):
+        _call("ofg_learned_set_tensor_cores", self._h, 1 if on else 0)
+
+    def get_params(self):
+        """(params, adam_m, adam_v, step): a checkpoint."""
+        k = self.num_params()
+        p, m, v = np.zeros(k, np.float32), np.zeros(k, np.float32), np.zeros(k, np.float32)
+        st = ctypes.c_int64()
+        _call("ofg_learned_get_params", self._h, _ptr(p), _ptr(m), _ptr(v), ctypes.byref(st))
+        return p, m, v, st.value
+
+    def set_params(self, params, adam_m=None, adam_v=None, step=0):
+        k = self.num_params()
+        f = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float32)
+        params, adam_m, adam_v = f(params), f(adam_m), f(adam_v)
+        if params.size != k:
+            raise OFELIException("expected %d parameters" % k)
+        _call("ofg_learned_set_params", self._h, _ptr(params), _ptr(adam_m), _ptr(adam_v),
+              int(step))
+
+    @staticmethod
+    def _pairs(A, R, E):
+        R = np.ascontiguousarray(R, dtype=np.float32) if not hasattr(R, "data_ptr") else R
+        E = np.ascontiguousarray(E, dtype=np.float32) if not hasattr(E, "data_ptr") else E
+        npairs = R.shape[0]
+        if tuple(R.shape) != (npairs, A.n) or tuple(E.shape) != (npairs, A.n):
+            raise OFELIException("pairs must be (npairs, n)")
+        return R, E, npairs
+
+    @staticmethod
+    def make_pairs(A, b, npairs, seed=0, toler=1e-12):
+        """Residual / error pairs from the plain solve of A x = b: the plain
+        Jacobi-CG gives x*; for random starting guesses x0 (white noise ten
+        times the size of x*) the pair is (r, e) = (b - A x0, x* - x0).
+        Returns R, E as (npairs, n) float32 arrays."""
+        n = A.n
+        b = _f64(b, n)
+        xs = np.zeros(n)
+        it = CG(A, DIAG_PREC, b, xs, 100000, toler)
+        if it < 0:
+            raise OFELIException("plain solve did not converge")
+        s = 10.0 * max(np.sqrt(np.mean(xs * xs)), 1e-30)
+        R = np.zeros((npairs, n), np.float32)
+        E = np.zeros((npairs, n), np.float32)
+        for p in range(npairs):
+            x0 = s * fields.normal(seed * 1000003 + p, n)
+            R[p] = b - A.Mult(x0)
+            E[p] = xs - x0
+        return R, E
+
+    def train(self, A, R, E, steps, batch=16, lr=1e-3):
+        """Adam steps on residual / error pairs (rows of R and E); returns the
+        per-step batch losses."""
+        R, E, npairs = self._pairs(A, R, E)
+        hist = np.zeros(steps, np.float32)
+        _call("ofg_learned_train", self._h, A._h, _ptr(R), _ptr(E), npairs, steps,
+              min(batch, npairs), ctypes.c_float(lr), _ptr(hist))
+        return hist
+
+    def grad(self, A, R, E):
+        """(loss, gradient, factor values at A's CSR positions)."""
+        R, E, npairs = self._pairs(A, R, E)
+        loss = ctypes.c_double()
+        g = np.zeros(self.num_params(), np.float32)
+        fac = np.zeros(A.nnz, np.float32)
+        _call("ofg_learned_grad", self._h, A._h, _ptr(R), _ptr(E), npairs, ctypes.byref(loss),
+              _ptr(g), _ptr(fac))
+        return loss.value, g, fac
+
+    def __del__(self):
+        if getattr(self, "_h", None) and capi is not None and capi._lib is not None:
+            capi.lib().ofg_learned_destroy(self._h)
+            self._h = None
+
+
+def fcg_learned(P, b, x, inner_bits=32, toler=1e-10, max_outer=200, max_inner=1000000,
+                inner_tol=0.05):
+    """Flexible CG with the learned preconditioner in FP32 inside FP64
+    refinement, falling back to the plain Jacobi iteration on stagnation.
+    Returns (refinement steps, inner iterations, FP64 true relative residual,
+    fell_back)."""
+    b = _f64(b, P.A.n)
+    o, i, r, fb = ctypes.c_int(), ctypes.c_int(), ctypes.c_double(), ctypes.c_int()
+    _call("ofg_fcg_learned", P._h, inner_bits, _ptr(b), _ptr(x), max_outer, max_inner, inner_tol,
+          toler, ctypes.byref(o), ctypes.byref(i), ctypes.byref(r), ctypes.byref(fb))
+    return o.value, i.value, r.value, bool(fb.value)
 
 
 def residual(A, b, x):
