@@ -72,6 +72,11 @@ struct SweepPlan {
 };
 }  // namespace ofg
 
+namespace ofg {
+// learned.cu: frees the network buffers kept for a learned preconditioner
+void learned_release(const ofg_prec* P);
+}  // namespace ofg
+
 struct ofg_prec {
    ofg_matrix* A = nullptr;
    int type = OFG_DIAG;
@@ -93,6 +98,7 @@ struct ofg_prec {
    ofg::DBuf<unsigned> counter;
    ~ofg_prec()
    {
+      if (type == OFG_LEARNED) ofg::learned_release(this);
       delete gl;
       delete gu;
    }

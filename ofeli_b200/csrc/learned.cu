@@ -27,13 +27,15 @@
 //     fit; with errors taken from CG iterates, which are dominated by smooth
 //     modes, it does not give a better CG preconditioner than Jacobi).
 //
-// The two dense layer products [rows x 128] x [128 x 64] and the backward
-// product [rows x 64] x [64 x 128] run on the tensor cores (tcgen05.mma,
-// kind::f16, BF16 x BF16 -> FP32 in tensor memory, operands staged in shared
-// memory in the K-major core-matrix layout, one elected thread issues, the
-// epilogue reads the accumulators with tcgen05.ld); a CUDA-core version of
-// the same product is kept as the checker (ofg_learned_gemm_check).  The
-// weight gradient X^T dZ (a reduction over all rows) runs on CUDA cores.
+// The layer products [rows x 128] x [128 x 64] (forward; the 128 inputs are
+// h and agg, read from their own arrays) and [rows x 64] x [64 x 128] (the
+// backward data product) run on the tensor cores: tcgen05.mma kind::f16,
+// BF16 x BF16 -> FP32 accumulators in tensor memory, operands staged in
+// shared memory in the K-major core-matrix layout, one elected thread
+// issues, the epilogue reads the accumulators with tcgen05.ld and applies
+// bias / ReLU / residual in registers.  A CUDA-core version of the same
+// product is kept as the checker (ofg_learned_gemm_check).  The weight
+// gradient X^T dZ (a reduction over all rows) runs on CUDA cores.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -65,6 +67,28 @@ __device__ __forceinline__ float bf2f(bf16 v) { return __bfloat162float(v); }
 __device__ __forceinline__ float to_f(bf16 v) { return __bfloat162float(v); }
 __device__ __forceinline__ float to_f(float v) { return v; }
 
+// eight BF16 values <-> eight floats through one 16-byte access
+__device__ __forceinline__ void load8(const bf16* p, float* f)
+{
+   const uint4 u = *reinterpret_cast<const uint4*>(p);
+   const __nv_bfloat162* b = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+   for (int q = 0; q < 4; ++q) {
+      const float2 t = __bfloat1622float2(b[q]);
+      f[2 * q] = t.x;
+      f[2 * q + 1] = t.y;
+   }
+}
+
+__device__ __forceinline__ void store8(bf16* p, const float* f)
+{
+   uint4 u;
+   __nv_bfloat162* b = reinterpret_cast<__nv_bfloat162*>(&u);
+#pragma unroll
+   for (int q = 0; q < 4; ++q) b[q] = __floats2bfloat162_rn(f[2 * q], f[2 * q + 1]);
+   *reinterpret_cast<uint4*>(p) = u;
+}
+
 // ------------------------------------------------------------ graph prep --
 // d_i = sqrt(|a_ii|)
 __global__ void lp_scale(int64_t n, const double* val, const int32_t* dpos, float* dsq)
@@ -76,7 +100,7 @@ __global__ void lp_scale(int64_t n, const double* val, const int32_t* dpos, floa
 
 // a~ (0 on the diagonal) and the node features
 __global__ void lp_features(int64_t n, const int32_t* rp, const int32_t* col, const double* val,
-                            const int32_t* dpos, const float* dsq, float* at, float* feat)
+                            const float* dsq, float* at, float* feat)
 {
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
@@ -140,8 +164,8 @@ __global__ void lp_transpose(int64_t n, const int32_t* rp, const int32_t* col, i
 }
 
 // ----------------------------------------------------------- layers (fwd) --
-// h0 = relu(f W_in + b_in); also z0 (pre-activation) for the backward pass
-__global__ void lp_embed(int64_t n, const float* feat, const float* P, bf16* h, bf16* z, bf16* cat)
+// h0 = relu(f W_in + b_in); also z0 (pre-activation) when z is given
+__global__ void lp_embed(int64_t n, const float* feat, const float* P, bf16* h, bf16* z)
 {
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n * HID; t += stride) {
@@ -150,16 +174,14 @@ __global__ void lp_embed(int64_t n, const float* feat, const float* P, bf16* h, 
       float s = P[P_BIN + c];
 #pragma unroll
       for (int q = 0; q < NFEAT; ++q) s += feat[i * NFEAT + q] * P[P_WIN + q * HID + c];
-      z[t] = __float2bfloat16(s);
-      const bf16 hv = __float2bfloat16(fmaxf(s, 0.f));
-      h[t] = hv;
-      cat[i * 2 * HID + c] = hv;
+      if (z) z[t] = __float2bfloat16(s);
+      h[t] = __float2bfloat16(fmaxf(s, 0.f));
    }
 }
 
-// cat[i, 64:128] = sum_{j != i} a~_ij h_j   (8 threads per row, 8 features each)
+// agg_i = sum_{j != i} a~_ij h_j   (8 threads per row, 8 features each)
 __global__ void lp_aggregate(int64_t n, const int32_t* rp, const int32_t* col, const float* at,
-                             const bf16* h, bf16* cat, int cat_stride, int cat_off)
+                             const bf16* h, bf16* agg)
 {
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n * 8; t += stride) {
@@ -169,52 +191,85 @@ __global__ void lp_aggregate(int64_t n, const int32_t* rp, const int32_t* col, c
       for (int32_t k = rp[i]; k < rp[i + 1]; ++k) {
          const float a = at[k];
          if (a == 0.f) continue;
-         const uint4 raw = *reinterpret_cast<const uint4*>(h + (int64_t)col[k] * HID + f0);
-         const bf16* hv = reinterpret_cast<const bf16*>(&raw);
+         float hv[8];
+         load8(h + (int64_t)col[k] * HID + f0, hv);
 #pragma unroll
-         for (int q = 0; q < 8; ++q) acc[q] += a * bf2f(hv[q]);
+         for (int q = 0; q < 8; ++q) acc[q] += a * hv[q];
       }
-      bf16 out[8];
-#pragma unroll
-      for (int q = 0; q < 8; ++q) out[q] = __float2bfloat16(acc[q]);
-      *reinterpret_cast<uint4*>(cat + i * cat_stride + cat_off + f0) = *reinterpret_cast<uint4*>(out);
+      store8(agg + i * HID + f0, acc);
    }
 }
 
-// Epilogue of a forward layer: z = acc + b; h_new = relu(z) + h_old; also
-// the left half of the next layer's input.
-struct FwdEpi {
+// ------------------------------------------------------- layer products ----
+// The A operand of a product: row m is [a0[m, 0:k0] | a1[m, 0:K-k0]] (a1
+// unused when k0 == K); row strides in elements.
+struct GemmA {
+   const bf16* a0;
+   int64_t lda0;
+   const bf16* a1;
+   int64_t lda1;
+   int k0;
+   __device__ __forceinline__ const bf16* at(int64_t m, int k) const
+   {
+      return k < k0 ? a0 + m * lda0 + k : a1 + m * lda1 + (k - k0);
+   }
+};
+
+// Epilogue of a forward layer, 16 columns of one row at a time:
+// z = acc + b; h_new = relu(z) + h_old (BF16); z kept when asked for.
+struct FwdFunctor {
+   static constexpr int kBytesPerCol = 6;  // h_old read, h_new written (BF16); z if kept
    const float* bias;
    const bf16* h_old;
-   bf16* z;
+   bf16* z;  // may be null
    bf16* h_new;
-   bf16* cat_next;  // may be null
-};
-
-__device__ __forceinline__ void fwd_epilogue(const FwdEpi& e, int64_t row, int c0, const float* v,
-                                             int cnt)
-{
-   for (int q = 0; q < cnt; ++q) {
-      const int c = c0 + q;
-      const float z = v[q] + e.bias[c];
-      const float h = fmaxf(z, 0.f) + bf2f(e.h_old[row * HID + c]);
-      e.z[row * HID + c] = __float2bfloat16(z);
-      const bf16 hb = __float2bfloat16(h);
-      e.h_new[row * HID + c] = hb;
-      if (e.cat_next) e.cat_next[row * 2 * HID + c] = hb;
+   __device__ __forceinline__ void operator()(int64_t row, int c0, const float* v) const
+   {
+      float ho[16], zz[16], hh[16];
+      load8(h_old + row * HID + c0, ho);
+      load8(h_old + row * HID + c0 + 8, ho + 8);
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+         zz[q] = v[q] + bias[c0 + q];
+         hh[q] = fmaxf(zz[q], 0.f) + ho[q];
+      }
+      if (z) {
+         store8(z + row * HID + c0, zz);
+         store8(z + row * HID + c0 + 8, zz + 8);
+      }
+      store8(h_new + row * HID + c0, hh);
+      store8(h_new + row * HID + c0 + 8, hh + 8);
    }
-}
-
-// Epilogue of the backward data product: dcat (FP32) for the 128 columns.
-struct BwdEpi {
-   float* dcat;
 };
 
-// ---------------------------------------------------- CUDA-core GEMM -----
-// C[rows x N] = A[rows x K] * Bt^T, Bt[N x K] (both row-major, BF16),
-// FP32 accumulation; the reference and the checker of the tensor-core path.
+// Epilogue of the backward data product: dcat (FP32, 128 columns).
+struct BwdFunctor {
+   static constexpr int kBytesPerCol = 4;
+   float* dcat;
+   __device__ __forceinline__ void operator()(int64_t row, int c0, const float* v) const
+   {
+      float4* o = reinterpret_cast<float4*>(dcat + row * 2 * HID + c0);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) o[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+   }
+};
+
+struct StoreFunctor {  // plain FP32 store, for the product check
+   static constexpr int kBytesPerCol = 4;
+   float* out;
+   int ld;
+   __device__ __forceinline__ void operator()(int64_t row, int c0, const float* v) const
+   {
+      float4* o = reinterpret_cast<float4*>(out + row * ld + c0);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) o[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+   }
+};
+
+// CUDA-core product: C[rows x N] = A[rows x K] * Bt^T, Bt[N x K] row-major
+// BF16, FP32 accumulation (the checker of the tensor-core path).
 template <int K, int N, class Epi>
-__global__ void __launch_bounds__(256) gemm_cc(int64_t rows, const bf16* A, const bf16* Bt, Epi epi)
+__global__ void __launch_bounds__(256) gemm_cc(int64_t rows, GemmA a, const bf16* Bt, Epi epi)
 {
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < rows * (N / 16);
@@ -225,22 +280,23 @@ __global__ void __launch_bounds__(256) gemm_cc(int64_t rows, const bf16* A, cons
 #pragma unroll
       for (int q = 0; q < 16; ++q) acc[q] = 0.f;
       for (int k = 0; k < K; ++k) {
-         const float a = bf2f(A[row * K + k]);
+         const float av = bf2f(*a.at(row, k));
 #pragma unroll
-         for (int q = 0; q < 16; ++q) acc[q] += a * bf2f(Bt[(c0 + q) * K + k]);
+         for (int q = 0; q < 16; ++q) acc[q] += av * bf2f(Bt[(c0 + q) * K + k]);
       }
-      epi(row, c0, acc, 16);
+      epi(row, c0, acc);
    }
 }
 
-// ---------------------------------------------------- tensor-core GEMM ---
-// One CTA (4 warps) per 128-row tile at a time (persistent over tiles).
-// Shared memory holds A (128 x K) and B (N x K) in the K-major core-matrix
-// layout without swizzle: element (m, k) at ((k/8)*(M/8) + m/8)*128 +
-// (m%8)*16 + (k%8)*2 bytes, so one MMA (K = 16) reads two 8-column chunks
-// with LBO = (M/8)*128 bytes between them and SBO = 128 bytes between
-// 8-row groups.  The accumulator (128 lanes x N FP32 columns) lives in
-// tensor memory; thread 0 issues the MMAs and commits to an mbarrier.
+// Tensor-core product.  One CTA (4 warps) per 128-row tile at a time
+// (persistent over tiles).  Shared memory holds A (128 x K) and B (N x K) in
+// the K-major core-matrix layout without swizzle: element (m, k) of an
+// M-row operand at (k/8)*(M/8)*128 + m*16 + (k%8)*2 bytes, so one MMA
+// (K = 16) reads two 8-column chunks LBO = M*16 bytes apart, with SBO = 128
+// bytes between 8-row groups.  Thread t stages row t of the A tile, 32
+// bytes at a time (one full sector), and a warp's stores cover 512
+// contiguous bytes.  The accumulator (128 lanes x N FP32 columns) lives in
+// tensor memory; thread 0 issues the MMAs and commits them to an mbarrier.
 __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
 {
    uint64_t d = 0;
@@ -285,10 +341,11 @@ __device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t phase)
 }
 
 template <int K, int N, class Epi>
-__global__ void __launch_bounds__(128, 4) gemm_tc(int64_t rows, const bf16* __restrict__ A,
+__global__ void __launch_bounds__(128, 4) gemm_tc(int64_t rows, GemmA a,
                                                   const bf16* __restrict__ Bt, Epi epi, int* status,
                                                   int* worked)
 {
+   static_assert(K % 16 == 0 && N % 16 == 0 && N >= 32 && N <= 256, "tile shape");
    prof_mark(worked);
    extern __shared__ __align__(1024) unsigned char smem[];
    unsigned char* sA = smem;                   // 128*K*2 bytes
@@ -297,11 +354,11 @@ __global__ void __launch_bounds__(128, 4) gemm_tc(int64_t rows, const bf16* __re
    uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 1);
    const int tid = threadIdx.x, warp = tid >> 5;
 
-   // B once per CTA
+   // B once per CTA: row nr of chunk c at c*N*16 + nr*16
    for (int piece = tid; piece < N * K / 8; piece += 128) {
-      const int nr = piece / (K / 8), c = piece % (K / 8);
+      const int nr = piece % N, c = piece / N;
       const uint4 v = *reinterpret_cast<const uint4*>(Bt + (int64_t)nr * K + c * 8);
-      *reinterpret_cast<uint4*>(sB + ((c * (N / 8) + nr / 8) * 8 + nr % 8) * 16) = v;
+      *reinterpret_cast<uint4*>(sB + c * N * 16 + nr * 16) = v;
    }
    if (tid == 0) {
       asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(1) : "memory");
@@ -327,12 +384,19 @@ __global__ void __launch_bounds__(128, 4) gemm_tc(int64_t rows, const bf16* __re
 
    for (int64_t tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
       const int64_t m0 = tile * 128;
-      for (int piece = tid; piece < 128 * K / 8; piece += 128) {
-         const int m = piece / (K / 8), c = piece % (K / 8);
-         const int64_t r = m0 + m;
-         uint4 v = make_uint4(0, 0, 0, 0);
-         if (r < rows) v = *reinterpret_cast<const uint4*>(A + r * K + c * 8);
-         *reinterpret_cast<uint4*>(sA + ((c * 16 + m / 8) * 8 + m % 8) * 16) = v;
+      {
+         const int64_t r = m0 + tid;
+#pragma unroll
+         for (int cp = 0; cp < K / 16; ++cp) {
+            uint4 v0 = make_uint4(0, 0, 0, 0), v1 = v0;
+            if (r < rows) {
+               const bf16* src = a.at(r, cp * 16);
+               v0 = *reinterpret_cast<const uint4*>(src);
+               v1 = *reinterpret_cast<const uint4*>(src + 8);
+            }
+            *reinterpret_cast<uint4*>(sA + (2 * cp) * 2048 + tid * 16) = v0;
+            *reinterpret_cast<uint4*>(sA + (2 * cp + 1) * 2048 + tid * 16) = v1;
+         }
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -341,8 +405,8 @@ __global__ void __launch_bounds__(128, 4) gemm_tc(int64_t rows, const bf16* __re
       if (tid == 0) {
 #pragma unroll
          for (int kk = 0; kk < K / 16; ++kk) {
-            const uint64_t ad = smem_desc(sa + kk * 2 * 16 * 128, 16 * 128, 128);
-            const uint64_t bd = smem_desc(sb + kk * 2 * (N / 8) * 128, (N / 8) * 128, 128);
+            const uint64_t ad = smem_desc(sa + kk * 2 * 2048, 2048, 128);
+            const uint64_t bd = smem_desc(sb + kk * 2 * N * 16, N * 16, 128);
             const uint32_t acc = kk > 0 ? 1u : 0u;
             asm volatile(
                "{\n\t.reg .pred p;\n\t"
@@ -383,7 +447,7 @@ __global__ void __launch_bounds__(128, 4) gemm_tc(int64_t rows, const bf16* __re
             float v[16];
 #pragma unroll
             for (int q = 0; q < 16; ++q) v[q] = __uint_as_float(r[q]);
-            if (row < rows) epi(row, cb, v, 16);
+            if (row < rows) epi(row, cb, v);
          }
       }
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -399,64 +463,59 @@ __global__ void __launch_bounds__(128, 4) gemm_tc(int64_t rows, const bf16* __re
                    : "memory");
 }
 
-struct FwdFunctor {
-   static constexpr int kBytesPerCol = 8;  // h_old read; z, h_new, cat_next written (BF16)
-   FwdEpi e;
-   __device__ void operator()(int64_t row, int c0, const float* v, int cnt) const
-   {
-      fwd_epilogue(e, row, c0, v, cnt);
-   }
-};
-
-struct BwdFunctor {
-   static constexpr int kBytesPerCol = 4;  // dcat written (FP32)
-   float* dcat;
-   __device__ void operator()(int64_t row, int c0, const float* v, int cnt) const
-   {
-      for (int q = 0; q < cnt; ++q) dcat[row * 2 * HID + c0 + q] = v[q];
-   }
-};
-
-struct StoreFunctor {  // plain FP32 store, for the GEMM check
-   static constexpr int kBytesPerCol = 4;
-   float* out;
-   int ld;
-   __device__ void operator()(int64_t row, int c0, const float* v, int cnt) const
-   {
-      for (int q = 0; q < cnt; ++q) out[row * ld + c0 + q] = v[q];
-   }
-};
-
 // ------------------------------------------------------------------ head --
-// G (lower part incl. diagonal, stored at A's CSR positions; upper = 0)
+// G (lower part incl. diagonal, stored at A's CSR positions; upper = 0).
+// Eight lanes per row, eight features each; the dot products are reduced
+// over the lane group with shuffles.
 __global__ void lp_head(int64_t n, const int32_t* rp, const int32_t* col, const float* at,
                         const float* dsq, const bf16* h, const float* P, float* g)
 {
+   const int lane = threadIdx.x & 31, sub = lane & 7;
+   const unsigned gmask = 0xFFu << (lane & 24);
+   float u[8], v[8];
+#pragma unroll
+   for (int q = 0; q < 8; ++q) {
+      u[q] = P[P_U + sub * 8 + q];
+      v[q] = P[P_V + sub * 8 + q];
+   }
+   const float cc = P[P_C];
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
-   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-      const bf16* hi = h + i * HID;
-      float dv = P[P_C];
-      for (int c = 0; c < HID; ++c) dv += P[P_V + c] * bf2f(hi[c]);
+   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n * 8; t += stride) {
+      const int64_t i = t >> 3;
+      float hi[8];
+      load8(h + i * HID + sub * 8, hi);
+      float dv = 0.f;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) dv += v[q] * hi[q];
+      dv += __shfl_xor_sync(gmask, dv, 1);
+      dv += __shfl_xor_sync(gmask, dv, 2);
+      dv += __shfl_xor_sync(gmask, dv, 4);
       for (int32_t k = rp[i]; k < rp[i + 1]; ++k) {
          const int32_t j = col[k];
          float gv = 0.f;
          if (j == (int32_t)i) {
-            const float sp = fmaxf(dv > 20.f ? dv : log1pf(expf(dv)), 1e-20f);
+            const float s = cc + dv;
+            const float sp = fmaxf(s > 20.f ? s : log1pf(expf(s)), 1e-20f);
             gv = sp / dsq[i];
          }
          else if (j < (int32_t)i && at[k] != 0.f) {
-            const bf16* hj = h + (int64_t)j * HID;
+            float hj[8];
+            load8(h + (int64_t)j * HID + sub * 8, hj);
             float s = 0.f;
-            for (int c = 0; c < HID; ++c) s += P[P_U + c] * bf2f(hi[c]) * bf2f(hj[c]);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) s += u[q] * hi[q] * hj[q];
+            s += __shfl_xor_sync(gmask, s, 1);
+            s += __shfl_xor_sync(gmask, s, 2);
+            s += __shfl_xor_sync(gmask, s, 4);
             gv = at[k] * s / dsq[j];
          }
-         g[k] = gv;
+         if (sub == 0) g[k] = gv;
       }
    }
 }
 
 // ------------------------------------------------------- apply M = G^T G --
-// z = G r (lower rows)
+// z = G r (lower rows), for P columns of n entries (training)
 template <class T>
 __global__ void lp_apply_lower(int64_t n, int64_t ncols, const int32_t* rp, const int32_t* col,
                                const float* g, const T* r, T* z)
@@ -510,13 +569,20 @@ struct ofg_learned {
 
 namespace ofg {
 
-// activations of one forward pass over a matrix
+// Inputs, activations and output of the network on one matrix.  Training
+// keeps every layer's activations (the backward pass needs them); inference
+// keeps two hidden-state buffers and one aggregate buffer.
 struct LearnedGraph {
-   int64_t n = 0;
+   int64_t n = 0, nnz = 0;
+   bool train = false, tp_ready = false;
    DBuf<float> dsq, at, feat, g;
    DBuf<int32_t> tp;
-   DBuf<bf16> h[NLAYER + 1], z[NLAYER + 1], cat[NLAYER];
-   DBuf<double> mean;
+   DBuf<double> mean, partials;
+   DBuf<unsigned> counter;
+   DBuf<bf16> h[NLAYER + 1], z[NLAYER + 1], agg[NLAYER];
+   bf16* hbuf(int l) { return train ? h[l].p : h[l & 1].p; }
+   bf16* aggbuf(int l) { return train ? agg[l].p : agg[0].p; }
+   bf16* zbuf(int l) { return train ? z[l].p : nullptr; }
 };
 
 namespace {
@@ -554,40 +620,56 @@ __global__ void lp_cast_weights(const float* P, bf16* wt, bf16* wb)
 
 }  // namespace
 
-static void graph_prepare(ofg_matrix* A, LearnedGraph& G)
+// (re)computes the graph inputs for A's current values; the transposed
+// positions only when the pattern is new
+static void graph_prepare(ofg_matrix* A, LearnedGraph& G, bool train)
 {
    const int64_t n = A->n;
    ensure_dpos(A);
    OFG_REQUIRE(A->dpos_complete, OFG_ERR_PIVOT, "a row has no diagonal entry");
-   G.n = n;
-   G.dsq.reserve(n);
-   G.at.reserve(A->nnz);
-   G.feat.reserve(n * NFEAT);
-   G.g.reserve(A->nnz);
-   G.tp.reserve(A->nnz);
-   G.mean.reserve(1);
-   for (int l = 0; l <= NLAYER; ++l) {
-      G.h[l].reserve(n * HID);
-      G.z[l].reserve(n * HID);
+   if (G.n != n || G.nnz != A->nnz || G.train != train) {
+      G.tp_ready = false;
+      G.n = n;
+      G.nnz = A->nnz;
+      G.train = train;
+      G.dsq.alloc(n);
+      G.at.alloc(A->nnz);
+      G.feat.alloc(n * NFEAT);
+      G.g.alloc(A->nnz);
+      G.tp.alloc(A->nnz);
+      G.mean.alloc(1);
+      G.partials.alloc(((size_t)grid_for(n, kRedBlock, 8) + 1) * 2);
+      G.counter.alloc(1);
+      G.counter.zero();
+      for (int l = 0; l <= NLAYER; ++l) {
+         G.h[l].release();
+         G.z[l].release();
+         if (l < NLAYER) G.agg[l].release();
+      }
+      const int nh = train ? NLAYER + 1 : 2, na = train ? NLAYER : 1;
+      for (int l = 0; l < nh; ++l) G.h[l].alloc(n * HID);
+      for (int l = 0; l < na; ++l) G.agg[l].alloc(n * HID);
+      if (train)
+         for (int l = 0; l <= NLAYER; ++l) G.z[l].alloc(n * HID);
    }
-   for (int l = 0; l < NLAYER; ++l) G.cat[l].reserve(n * 2 * HID);
    const unsigned gr = grid_for(n, 256);
    lp_scale<<<gr, 256, 0, stream()>>>(n, A->val.p, A->dpos.p, G.dsq.p);
-   lp_features<<<gr, 256, 0, stream()>>>(n, A->row_ptr.p, A->col.p, A->val.p, A->dpos.p, G.dsq.p,
-                                         G.at.p, G.feat.p);
-   DBuf<double> partials(((size_t)grid_for(n, kRedBlock, 8) + 1) * 2);
-   DBuf<unsigned> counter(1);
-   counter.zero();
+   lp_features<<<gr, 256, 0, stream()>>>(n, A->row_ptr.p, A->col.p, A->val.p, G.dsq.p, G.at.p,
+                                         G.feat.p);
    lp_logmean<<<grid_for(n, kRedBlock, 8), kRedBlock, 0, stream()>>>(n, G.feat.p, G.mean.p,
-                                                                     partials.p, counter.p);
+                                                                     G.partials.p, G.counter.p);
    lp_center<<<gr, 256, 0, stream()>>>(n, G.feat.p, G.mean.p);
-   lp_transpose<<<gr, 256, 0, stream()>>>(n, A->row_ptr.p, A->col.p, G.tp.p);
-   count_launch(5);
+   count_launch(4);
+   if (!G.tp_ready) {
+      lp_transpose<<<gr, 256, 0, stream()>>>(n, A->row_ptr.p, A->col.p, G.tp.p);
+      count_launch();
+      G.tp_ready = true;
+   }
    OFG_LAUNCH_CHECK();
 }
 
 template <int K, int N, class Epi>
-static void run_gemm(ofg_learned* L, int64_t rows, const bf16* Am, const bf16* Bt, Epi epi)
+static void run_gemm(ofg_learned* L, int64_t rows, GemmA a, const bf16* Bt, Epi epi)
 {
    if (rows <= 0) return;
    if (L->use_tc) {
@@ -604,35 +686,35 @@ static void run_gemm(ofg_learned* L, int64_t rows, const bf16* Am, const bf16* B
       const int64_t tiles = (rows + 127) / 128;
       const unsigned grid = (unsigned)std::min<int64_t>(tiles, (int64_t)num_sms() * 4);
       int* worked = prof_begin();
-      gemm_tc<K, N, Epi><<<grid, 128, smem, stream()>>>(rows, Am, Bt, epi, L->status.p, worked);
+      gemm_tc<K, N, Epi><<<grid, 128, smem, stream()>>>(rows, a, Bt, epi, L->status.p, worked);
       // algorithmic bytes: the A operand, the weights, and the epilogue's
       // own reads and writes per output column
       prof_end(PROF_NET_GEMM, (double)rows * (K * 2 + N * Epi::kBytesPerCol) + (double)N * K * 2);
    }
    else {
-      gemm_cc<K, N, Epi><<<grid_for(rows * (N / 16), 256), 256, 0, stream()>>>(rows, Am, Bt, epi);
+      gemm_cc<K, N, Epi><<<grid_for(rows * (N / 16), 256), 256, 0, stream()>>>(rows, a, Bt, epi);
    }
    count_launch();
    OFG_LAUNCH_CHECK();
 }
 
-// forward pass: activations of every layer and the factor G
+// forward pass: the hidden states and the factor G
 static void learned_forward(ofg_learned* L, ofg_matrix* A, LearnedGraph& G)
 {
    const int64_t n = A->n;
-   lp_embed<<<grid_for(n * HID, 256), 256, 0, stream()>>>(n, G.feat.p, L->params.p, G.h[0].p,
-                                                            G.z[0].p, G.cat[0].p);
+   lp_embed<<<grid_for(n * HID, 256), 256, 0, stream()>>>(n, G.feat.p, L->params.p, G.hbuf(0),
+                                                            G.zbuf(0));
    count_launch();
    for (int l = 0; l < NLAYER; ++l) {
       lp_aggregate<<<grid_for(n * 8, 256), 256, 0, stream()>>>(n, A->row_ptr.p, A->col.p, G.at.p,
-                                                                G.h[l].p, G.cat[l].p, 2 * HID, HID);
+                                                                G.hbuf(l), G.aggbuf(l));
       count_launch();
-      FwdFunctor f{{L->params.p + P_B + l * HID, G.h[l].p, G.z[l + 1].p, G.h[l + 1].p,
-                    l + 1 < NLAYER ? G.cat[l + 1].p : nullptr}};
-      run_gemm<2 * HID, HID>(L, n, G.cat[l].p, L->wt.p + (size_t)l * 2 * HID * HID, f);
+      FwdFunctor f{L->params.p + P_B + l * HID, G.hbuf(l), G.zbuf(l + 1), G.hbuf(l + 1)};
+      GemmA a{G.hbuf(l), HID, G.aggbuf(l), HID, HID};
+      run_gemm<2 * HID, HID>(L, n, a, L->wt.p + (size_t)l * 2 * HID * HID, f);
    }
-   lp_head<<<grid_for(n, 128), 128, 0, stream()>>>(n, A->row_ptr.p, A->col.p, G.at.p, G.dsq.p,
-                                                    G.h[NLAYER].p, L->params.p, G.g.p);
+   lp_head<<<grid_for(n * 8, 256), 256, 0, stream()>>>(n, A->row_ptr.p, A->col.p, G.at.p, G.dsq.p,
+                                                        G.hbuf(NLAYER), L->params.p, G.g.p);
    count_launch();
    OFG_LAUNCH_CHECK();
 }
@@ -793,16 +875,14 @@ __global__ void lp_head_back(int64_t n, const int32_t* rp, const int32_t* col, c
 }
 
 // per-block partial sums of the head parameter gradients:
-// du_c = sum_lower dS h_ic h_jc; dv_c = sum_i dsd_i h_ic; dc = sum_i dsd_i
+// du_c = sum_lower dS h_ic h_jc; dv_c = sum_i dsd_i h_ic; dc = sum_i dsd_i.
+// Eight threads per row, eight features each; the block's threads are
+// summed in a fixed order (the result does not depend on scheduling).
 constexpr int HEADG = 2 * HID + 1;
 __global__ void __launch_bounds__(256) lp_head_pgrad(int64_t n, const int32_t* rp, const int32_t* col,
                                                      const bf16* h, const float* ds, float* part)
 {
-   // 8 threads per row, 8 features each; registers per thread, then one
-   // shared-memory reduction per block
-   __shared__ float acc[HEADG];
-   for (int q = threadIdx.x; q < HEADG; q += blockDim.x) acc[q] = 0.f;
-   __syncthreads();
+   __shared__ float red[256][17];
    const int sub = threadIdx.x & 7;
    float du[8], dv[8], dc = 0.f;
 #pragma unroll
@@ -810,8 +890,7 @@ __global__ void __launch_bounds__(256) lp_head_pgrad(int64_t n, const int32_t* r
    for (int64_t i = (int64_t)blockIdx.x * (blockDim.x / 8) + (threadIdx.x >> 3); i < n;
         i += (int64_t)gridDim.x * (blockDim.x / 8)) {
       float hi[8];
-#pragma unroll
-      for (int q = 0; q < 8; ++q) hi[q] = bf2f(h[i * HID + sub * 8 + q]);
+      load8(h + i * HID + sub * 8, hi);
       for (int32_t k = rp[i]; k < rp[i + 1]; ++k) {
          const int32_t j = col[k];
          const float s = ds[k];
@@ -822,19 +901,31 @@ __global__ void __launch_bounds__(256) lp_head_pgrad(int64_t n, const int32_t* r
             dc += s;
          }
          else {
+            float hj[8];
+            load8(h + (int64_t)j * HID + sub * 8, hj);
 #pragma unroll
-            for (int q = 0; q < 8; ++q) du[q] += s * hi[q] * bf2f(h[(int64_t)j * HID + sub * 8 + q]);
+            for (int q = 0; q < 8; ++q) du[q] += s * hi[q] * hj[q];
          }
       }
    }
 #pragma unroll
    for (int q = 0; q < 8; ++q) {
-      atomicAdd(&acc[sub * 8 + q], du[q]);
-      atomicAdd(&acc[HID + sub * 8 + q], dv[q]);
+      red[threadIdx.x][q] = du[q];
+      red[threadIdx.x][8 + q] = dv[q];
    }
-   if (sub == 0) atomicAdd(&acc[2 * HID], dc);
+   red[threadIdx.x][16] = sub == 0 ? dc : 0.f;
    __syncthreads();
-   for (int q = threadIdx.x; q < HEADG; q += blockDim.x) part[(int64_t)blockIdx.x * HEADG + q] = acc[q];
+   for (int o = threadIdx.x; o < HEADG; o += blockDim.x) {
+      float s = 0.f;
+      if (o < 2 * HID) {
+         const int oo = o % HID, sb = oo / 8, q = oo % 8 + (o < HID ? 0 : 8);
+         for (int t = sb; t < (int)blockDim.x; t += 8) s += red[t][q];
+      }
+      else {
+         for (int t = 0; t < (int)blockDim.x; t += 8) s += red[t][16];
+      }
+      part[(int64_t)blockIdx.x * HEADG + o] = s;
+   }
 }
 
 // grads[off + q] = sum over blocks of part[b * width + q]   (block order)
@@ -847,7 +938,7 @@ __global__ void lp_sum_parts(const float* part, int nblocks, int width, float* o
    }
 }
 
-// dz = dH * (z > 0); also the BF16 copy for the data GEMM
+// dz = dH * (z > 0); also the BF16 copy for the data product
 __global__ void lp_relu_back(int64_t total, const float* dH, const bf16* z, float* dz, bf16* dz16)
 {
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -875,10 +966,11 @@ __global__ void lp_layer_back(int64_t n, const int32_t* rp, const int32_t* col, 
    }
 }
 
-// per-block partials of X^T dz (rows x KIN and rows x HID; an implicit
-// all-ones column KIN gives the bias gradient): part[b][(KIN+1) x HID]
+// per-block partials of X^T dz with X = [x0 (k0 columns) | x1] and an
+// implicit all-ones column KIN for the bias gradient: part[b][(KIN+1) x HID]
 template <int KIN, class XT>
-__global__ void __launch_bounds__(256) lp_wgrad(int64_t n, const XT* X, const float* dz, float* part)
+__global__ void __launch_bounds__(256) lp_wgrad(int64_t n, const XT* x0, int ld0, int k0,
+                                                const XT* x1, int ld1, const float* dz, float* part)
 {
    constexpr int W = (KIN + 1) * HID;
    float acc[(W + 255) / 256];
@@ -888,7 +980,8 @@ __global__ void __launch_bounds__(256) lp_wgrad(int64_t n, const XT* X, const fl
    __shared__ float zs[HID];
    for (int64_t i = blockIdx.x; i < n; i += gridDim.x) {
       __syncthreads();
-      for (int q = threadIdx.x; q < KIN; q += blockDim.x) xs[q] = to_f(X[i * KIN + q]);
+      for (int q = threadIdx.x; q < KIN; q += blockDim.x)
+         xs[q] = q < k0 ? to_f(x0[i * ld0 + q]) : to_f(x1[i * ld1 + (q - k0)]);
       if (threadIdx.x == 0) xs[KIN] = 1.f;
       for (int q = threadIdx.x; q < HID; q += blockDim.x) zs[q] = dz[i * HID + q];
       __syncthreads();
@@ -954,28 +1047,29 @@ static double learned_backward(ofg_learned* L, ofg_matrix* A, LearnedGraph& G, c
    lp_apply_lower<float><<<gp, 256, 0, stream()>>>(n, P, rp, col, G.g.p, dY.p, dZ.p);
    lp_dG<<<gr, 256, 0, stream()>>>(n, P, rp, col, R, Z.p, dY.p, dZ.p, dg.p);
    if (L->loss_kind != 0) lp_kap_diag<<<gr, 256, 0, stream()>>>(n, A->dpos.p, G.g.p, dg.p);
-   lp_dS<<<gr, 256, 0, stream()>>>(n, A->row_ptr.p, A->col.p, G.at.p, G.dsq.p, G.h[NLAYER].p,
-                                   L->params.p, dg.p, ds.p);
-   lp_head_back<<<grid_for(n * HID, 256), 256, 0, stream()>>>(n, A->row_ptr.p, A->col.p, G.tp.p,
-                                                               G.h[NLAYER].p, L->params.p, ds.p,
-                                                               dH.p);
+   const bf16* hN = G.hbuf(NLAYER);
+   lp_dS<<<gr, 256, 0, stream()>>>(n, rp, col, G.at.p, G.dsq.p, hN, L->params.p, dg.p, ds.p);
+   lp_head_back<<<grid_for(n * HID, 256), 256, 0, stream()>>>(n, rp, col, G.tp.p, hN, L->params.p,
+                                                               ds.p, dH.p);
    const int nb = num_sms() * 2;
    {
       DBuf<float> part((size_t)nb * HEADG);
-      lp_head_pgrad<<<nb, 256, 0, stream()>>>(n, A->row_ptr.p, A->col.p, G.h[NLAYER].p, ds.p, part.p);
+      lp_head_pgrad<<<nb, 256, 0, stream()>>>(n, rp, col, hN, ds.p, part.p);
       lp_sum_parts<<<1, 256, 0, stream()>>>(part.p, nb, HEADG, L->grads.p + P_U);
    }
    count_launch(11);
    // layers, last to first
    for (int l = NLAYER - 1; l >= 0; --l) {
-      lp_relu_back<<<grid_for(n * HID, 256), 256, 0, stream()>>>(n * HID, dH.p, G.z[l + 1].p, dz.p,
+      lp_relu_back<<<grid_for(n * HID, 256), 256, 0, stream()>>>(n * HID, dH.p, G.zbuf(l + 1), dz.p,
                                                                    dz16.p);
       BwdFunctor bf{dcat.p};
-      run_gemm<HID, 2 * HID>(L, n, dz16.p, L->wb.p + (size_t)l * 2 * HID * HID, bf);
+      GemmA a{dz16.p, HID, nullptr, 0, HID};
+      run_gemm<HID, 2 * HID>(L, n, a, L->wb.p + (size_t)l * 2 * HID * HID, bf);
       {
          constexpr int W = (2 * HID + 1) * HID;
          DBuf<float> part((size_t)nb * W), tot(W);
-         lp_wgrad<2 * HID, bf16><<<nb, 256, 0, stream()>>>(n, G.cat[l].p, dz.p, part.p);
+         lp_wgrad<2 * HID, bf16><<<nb, 256, 0, stream()>>>(n, G.hbuf(l), HID, HID, G.aggbuf(l), HID,
+                                                           dz.p, part.p);
          lp_sum_parts<<<32, 256, 0, stream()>>>(part.p, nb, W, tot.p);
          // rows 0..127 -> W_l, row 128 -> b_l
          OFG_CUDA(cudaMemcpyAsync(L->grads.p + P_W + l * 2 * HID * HID, tot.p,
@@ -983,17 +1077,18 @@ static double learned_backward(ofg_learned* L, ofg_matrix* A, LearnedGraph& G, c
          OFG_CUDA(cudaMemcpyAsync(L->grads.p + P_B + l * HID, tot.p + 2 * HID * HID,
                                   sizeof(float) * HID, cudaMemcpyDeviceToDevice, stream()));
       }
-      lp_layer_back<<<grid_for(n * HID, 256), 256, 0, stream()>>>(n, A->row_ptr.p, A->col.p, G.at.p,
-                                                                   dH.p, dcat.p, dprev.p);
+      lp_layer_back<<<grid_for(n * HID, 256), 256, 0, stream()>>>(n, rp, col, G.at.p, dH.p, dcat.p,
+                                                                   dprev.p);
       std::swap(dH, dprev);
       count_launch(4);
    }
    // embedding
-   lp_relu_back<<<grid_for(n * HID, 256), 256, 0, stream()>>>(n * HID, dH.p, G.z[0].p, dz.p, dz16.p);
+   lp_relu_back<<<grid_for(n * HID, 256), 256, 0, stream()>>>(n * HID, dH.p, G.zbuf(0), dz.p, dz16.p);
    {
       constexpr int W = (NFEAT + 1) * HID;
       DBuf<float> part((size_t)nb * W), tot(W);
-      lp_wgrad<NFEAT, float><<<nb, 256, 0, stream()>>>(n, G.feat.p, dz.p, part.p);
+      lp_wgrad<NFEAT, float><<<nb, 256, 0, stream()>>>(n, G.feat.p, NFEAT, NFEAT, G.feat.p, NFEAT,
+                                                       dz.p, part.p);
       lp_sum_parts<<<4, 256, 0, stream()>>>(part.p, nb, W, tot.p);
       OFG_CUDA(cudaMemcpyAsync(L->grads.p + P_WIN, tot.p, sizeof(float) * NFEAT * HID,
                                cudaMemcpyDeviceToDevice, stream()));
@@ -1026,12 +1121,12 @@ static void cast_weights(ofg_learned* L)
 
 }  // namespace ofg
 
-
 // ------------------------------------------------- the preconditioner -----
 // G (lower rows, the diagonal included) and G^T (upper rows) become two
 // matrices of their own on A's row count, so that both products run as
 // SELL-32 SpMVs (FP64 values for the FP64 Krylov loops, FP32 for the mixed
-// one).
+// one).  The network's buffers for the matrix are kept with the
+// preconditioner (the pattern-only parts are computed once).
 namespace ofg {
 namespace {
 
@@ -1058,8 +1153,8 @@ __global__ void lp_to_i32(int64_t n, const int64_t* a, int32_t* b)
       b[i] = (int32_t)a[i];
 }
 
-// pattern (once) and values of G and G^T from the head's output g (stored
-// at A's lower positions) and the transposed positions tp
+// values (and on the first call the columns) of G and G^T from the head's
+// output g (stored at A's lower positions) and the transposed positions tp
 __global__ void lp_tri_fill(int64_t n, const int32_t* rp, const int32_t* col, const int32_t* tp,
                             const float* g, const int32_t* rpL, int32_t* colL, double* valL,
                             const int32_t* rpU, int32_t* colU, double* valU)
@@ -1114,15 +1209,35 @@ ofg_matrix* tri_matrix(int64_t n, const DBuf<int64_t>& len)
    return M;
 }
 
+std::vector<std::pair<const ofg_prec*, LearnedGraph*>> g_graphs;
+
+LearnedGraph* graph_of(const ofg_prec* P)
+{
+   for (auto& e : g_graphs)
+      if (e.first == P) return e.second;
+   g_graphs.push_back({P, new LearnedGraph()});
+   return g_graphs.back().second;
+}
+
 }  // namespace
+
+void learned_release(const ofg_prec* P)
+{
+   for (size_t q = 0; q < g_graphs.size(); ++q)
+      if (g_graphs[q].first == P) {
+         delete g_graphs[q].second;
+         g_graphs.erase(g_graphs.begin() + q);
+         return;
+      }
+}
 
 void learned_setup(ofg_prec* P)
 {
    OFG_REQUIRE(P->net, OFG_ERR_ARG, "learned preconditioner without a network");
    ofg_matrix* A = P->A;
    const int64_t n = A->n;
-   LearnedGraph G;
-   graph_prepare(A, G);
+   LearnedGraph& G = *graph_of(P);
+   graph_prepare(A, G, false);
    learned_forward(P->net, A, G);
    learned_check(P->net);
    const unsigned gr = grid_for(n, 256);
@@ -1253,7 +1368,7 @@ int ofg_learned_train(ofg_learned* L, ofg_matrix* A, const float* R, const float
       const int64_t n = A->n;
       In<float> dR(R, (size_t)npairs * n), dE(E, (size_t)npairs * n);
       LearnedGraph G;
-      graph_prepare(A, G);
+      graph_prepare(A, G, true);
       const int nbatches = npairs / batch;
       for (int s = 0; s < steps; ++s) {
          const int64_t p0 = (int64_t)(s % nbatches) * batch;
@@ -1280,7 +1395,7 @@ int ofg_learned_grad(ofg_learned* L, ofg_matrix* A, const float* R, const float*
       const int64_t n = A->n;
       In<float> dR(R, (size_t)npairs * n), dE(E, (size_t)npairs * n);
       LearnedGraph G;
-      graph_prepare(A, G);
+      graph_prepare(A, G, true);
       learned_forward(L, A, G);
       *loss = learned_backward(L, A, G, dR.d, dE.d, npairs);
       learned_check(L);
@@ -1322,12 +1437,12 @@ int ofg_learned_gemm_check(ofg_learned* L, int layer, int64_t rows, const uint16
       DBuf<float> a(rows * HID), b(rows * HID);
       const int saved = L->use_tc;
       const bf16* w = L->wt.p + (size_t)layer * 2 * HID * HID;
+      const bf16* x = reinterpret_cast<const bf16*>(dX.d);
+      GemmA op{x, 2 * HID, x + HID, 2 * HID, HID};  // the two halves of each row
       L->use_tc = 1;
-      run_gemm<2 * HID, HID>(L, rows, reinterpret_cast<const bf16*>(dX.d), w,
-                             StoreFunctor{a.p, HID});
+      run_gemm<2 * HID, HID>(L, rows, op, w, StoreFunctor{a.p, HID});
       L->use_tc = 0;
-      run_gemm<2 * HID, HID>(L, rows, reinterpret_cast<const bf16*>(dX.d), w,
-                             StoreFunctor{b.p, HID});
+      run_gemm<2 * HID, HID>(L, rows, op, w, StoreFunctor{b.p, HID});
       L->use_tc = saved;
       learned_check(L);
       a.download(out_tc, rows * HID);
