@@ -53,6 +53,7 @@ typedef struct ofg_matrix ofg_matrix;
 typedef struct ofg_mesh ofg_mesh;
 typedef struct ofg_prec ofg_prec;
 typedef struct ofg_learned ofg_learned;
+typedef struct ofg_batch ofg_batch;
 
 /* ---------------------------------------------------------------- runtime */
 const char* ofg_last_error(void);
@@ -278,6 +279,41 @@ int ofg_prec_create_learned(ofg_learned* L, ofg_matrix* A, ofg_prec** out);
 int ofg_fcg_learned(ofg_prec* P, int inner_bits, const double* b, double* x, int max_outer,
                     int max_inner, double inner_tol, double toler, int* outer, int* inner,
                     double* true_res, int* fell_back);
+
+/* ------------------------------------------------------ batched problems --
+ * No counterpart in OFELI (its equivalent is a loop of build() + CG per
+ * problem).  Many independent P1 problems of uneven size (one mesh each, all
+ * of one dimension) are assembled and solved in one persistent launch: per
+ * problem Equation::build() (k per element, f per node, Dirichlet data bc per
+ * node or 0), CG with the diagonal preconditioner in FP64 to
+ * ||r|| / ||b|| <= toler with the FP64 true residual checked at the end, and
+ * insertBC into the nodal solution.  A block owns one problem at a time,
+ * longest problems first; the launch is captured in a CUDA graph. */
+/* Concatenates the meshes' data and builds every pattern; the meshes may be
+ * destroyed afterwards. */
+int ofg_batch_create(int nprob, ofg_mesh* const* meshes, ofg_batch** out);
+int ofg_batch_destroy(ofg_batch* B);
+int ofg_batch_info(const ofg_batch* B, int* nprob, int64_t* nodes, int64_t* elements,
+                   int64_t* rows, int64_t* nnz);
+int ofg_batch_problem_info(const ofg_batch* B, int prob, int64_t* nodes, int64_t* elements,
+                           int64_t* rows, int64_t* nnz);
+/* Inputs concatenated in problem order: kel per element (NULL = 1), f per
+ * node (NULL = 0), bc per node (NULL = 0). */
+int ofg_batch_set_inputs(ofg_batch* B, const double* kel, const double* f, const double* bc);
+/* Assembles and solves every problem (one graph launch). */
+int ofg_batch_solve(ofg_batch* B, int max_it, double toler);
+/* Nodal solutions (concatenated), per-problem iterations (OFELI's CG
+ * convention: negative when max_it ran out) and FP64 true relative residuals;
+ * any argument may be NULL. */
+int ofg_batch_get_results(const ofg_batch* B, double* u, int* iters, double* res);
+/* Assembled values (CSR order of the problem's pattern) and RHS of one problem. */
+int ofg_batch_get_matrix(const ofg_batch* B, int prob, double* values, double* rhs);
+/* Autotuner: times the whole batch once per launch shape (threads per block
+ * x lanes per CSR row; ofg_batch_config_shape) and keeps the fastest;
+ * *chosen = its index, times_ms (may be NULL) receives every shape's time. */
+int ofg_batch_tune(ofg_batch* B, int max_it, double toler, int* chosen, float* times_ms);
+int ofg_batch_set_config(ofg_batch* B, int config, int blocks_per_sm);
+int ofg_batch_config_shape(int config, int* threads, int* lanes_per_row);
 
 #ifdef __cplusplus
 }

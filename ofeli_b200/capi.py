@@ -81,6 +81,17 @@ SIGNATURES = {
     "ofg_learned_gemm_check": (_i32, [_p, _i32, _i64, _p, _p, _p]),
     "ofg_prec_create_learned": (_i32, [_p, _p, _pp]),
     "ofg_fcg_learned": (_i32, [_p, _i32, _p, _p, _i32, _i32, _d, _d, _pi32, _pi32, _pd, _pi32]),
+    "ofg_batch_create": (_i32, [_i32, _p, _pp]),
+    "ofg_batch_destroy": (_i32, [_p]),
+    "ofg_batch_info": (_i32, [_p, _pi32, _pi64, _pi64, _pi64, _pi64]),
+    "ofg_batch_problem_info": (_i32, [_p, _i32, _pi64, _pi64, _pi64, _pi64]),
+    "ofg_batch_set_inputs": (_i32, [_p, _p, _p, _p]),
+    "ofg_batch_solve": (_i32, [_p, _i32, _d]),
+    "ofg_batch_get_results": (_i32, [_p, _p, _p, _p]),
+    "ofg_batch_get_matrix": (_i32, [_p, _i32, _p, _p]),
+    "ofg_batch_tune": (_i32, [_p, _i32, _d, _pi32, _p]),
+    "ofg_batch_set_config": (_i32, [_p, _i32, _i32]),
+    "ofg_batch_config_shape": (_i32, [_i32, _pi32, _pi32]),
 }
 
 _lib = None

@@ -388,6 +388,75 @@ def fcg_learned(P, b, x, inner_bits=32, toler=1e-10, max_outer=200, max_inner=10
     return o.value, i.value, r.value, bool(fb.value)
 
 
+class Batch:
+    """Many independent P1 problems assembled and solved in one persistent
+    launch (ofg_batch_*): per problem build() + CG with the diagonal
+    preconditioner in FP64 + insertBC.  Inputs are concatenated in problem
+    order (k per element, f and bc per node)."""
+
+    def __init__(self, meshes):
+        arr = (ctypes.c_void_p * len(meshes))(*[m._h.value for m in meshes])
+        h = ctypes.c_void_p()
+        _call("ofg_batch_create", len(meshes), ctypes.cast(arr, ctypes.c_void_p), ctypes.byref(h))
+        self._h = h
+        npb, nn, ne, nr, nnz = (ctypes.c_int(), ctypes.c_int64(), ctypes.c_int64(),
+                                ctypes.c_int64(), ctypes.c_int64())
+        _call("ofg_batch_info", h, ctypes.byref(npb), ctypes.byref(nn), ctypes.byref(ne),
+              ctypes.byref(nr), ctypes.byref(nnz))
+        self.nprob, self.nodes, self.elements = npb.value, nn.value, ne.value
+        self.rows, self.nnz = nr.value, nnz.value
+
+    def problem_info(self):
+        """Per problem (nodes, elements, rows, nonzeros) as an (nprob, 4) array."""
+        out = np.zeros((self.nprob, 4), np.int64)
+        v = [ctypes.c_int64() for _ in range(4)]
+        for p in range(self.nprob):
+            _call("ofg_batch_problem_info", self._h, p, *[ctypes.byref(x) for x in v])
+            out[p] = [x.value for x in v]
+        return out
+
+    def set_inputs(self, k=None, f=None, bc=None):
+        k, f, bc = _f64(k, self.elements), _f64(f, self.nodes), _f64(bc, self.nodes)
+        _call("ofg_batch_set_inputs", self._h, _ptr(k), _ptr(f), _ptr(bc))
+
+    def solve(self, max_it=100000, toler=1e-10):
+        _call("ofg_batch_solve", self._h, max_it, toler)
+
+    def results(self):
+        """(nodal solutions, iterations, FP64 true relative residuals)."""
+        u = np.zeros(self.nodes)
+        it = np.zeros(self.nprob, np.int32)
+        res = np.zeros(self.nprob)
+        _call("ofg_batch_get_results", self._h, _ptr(u), _ptr(it), _ptr(res))
+        return u, it, res
+
+    def matrix(self, p, nnz, n):
+        a, b = np.zeros(nnz), np.zeros(n)
+        _call("ofg_batch_get_matrix", self._h, p, _ptr(a), _ptr(b))
+        return a, b
+
+    def tune(self, max_it=100000, toler=1e-10):
+        """Autotuner: (chosen launch shape index, time of every shape in ms)."""
+        c = ctypes.c_int()
+        t = np.zeros(12, np.float32)
+        _call("ofg_batch_tune", self._h, max_it, toler, ctypes.byref(c), _ptr(t))
+        return c.value, t
+
+    def set_config(self, config, blocks_per_sm=0):
+        _call("ofg_batch_set_config", self._h, config, blocks_per_sm)
+
+    @staticmethod
+    def config_shape(config):
+        t, l = ctypes.c_int(), ctypes.c_int()
+        _call("ofg_batch_config_shape", config, ctypes.byref(t), ctypes.byref(l))
+        return t.value, l.value
+
+    def __del__(self):
+        if getattr(self, "_h", None) and capi is not None and capi._lib is not None:
+            capi.lib().ofg_batch_destroy(self._h)
+            self._h = None
+
+
 def residual(A, b, x):
     r = ctypes.c_double()
     _call("ofg_residual", A._h, _ptr(_f64(b, A.n)), _ptr(_f64(x, A.n)), ctypes.byref(r))

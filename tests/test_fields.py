@@ -43,3 +43,13 @@ def test_jitter_stays_within_radius_and_keeps_boundary():
     det = (P[:, 1, 0] - P[:, 0, 0]) * (P[:, 2, 1] - P[:, 0, 1]) - \
           (P[:, 1, 1] - P[:, 0, 1]) * (P[:, 2, 0] - P[:, 0, 0])
     assert (det > 0).all()
+
+
+def test_uneven_batch_sizes():
+    """The batched workload: 1024 problems, node counts log-uniform in
+    [1000, 64000], about 15.4 million nodes in all."""
+    from ofeli_b200 import problems
+    s = problems.uneven_sizes(1234)
+    nodes = (s + 1) ** 2
+    assert len(s) == 1024 and nodes.min() >= 900 and nodes.max() <= 66000
+    assert 15.0e6 < nodes.sum() < 16.0e6
