@@ -31,6 +31,8 @@ sys.path.insert(0, HERE)
 
 METRIC = "FP64-accurate solves/sec (2-D P1 Poisson 2049x2049, true rel. residual <= 1e-10)"
 METRIC_3D = "FP64-accurate solves/sec (3-D P1 variable-k diffusion 129^3, true rel. residual <= 1e-10)"
+METRIC_BATCH = ("FP64-accurate solves/sec (1024 uneven 2-D P1 problems, 1e3..6.4e4 nodes, "
+                "true rel. residual <= 1e-10)")
 UNIT = "solves/s"
 SEED = 1234
 TOL = 1e-10
@@ -47,9 +49,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nx", type=int, default=2048, help="cells per side (nodes = nx+1)")
-    ap.add_argument("--workload", default="poisson2d", choices=["poisson2d", "kuhn3d"],
+    ap.add_argument("--workload", default="poisson2d", choices=["poisson2d", "kuhn3d", "batch2d"],
                     help="poisson2d: the headline 2-D problem; kuhn3d: the 3-D "
-                         "variable-coefficient problem (129^3 Kuhn cube, lognormal k)")
+                         "variable-coefficient problem (129^3 Kuhn cube, lognormal k); batch2d: "
+                         "1024 uneven jittered 2-D problems in one persistent launch")
     ap.add_argument("--m3d", type=int, default=128, help="kuhn3d cells per side")
     ap.add_argument("--inner-bits", type=int, default=32, choices=[32, 16])
     ap.add_argument("--prec", default="jacobi", choices=["jacobi", "learned"],
@@ -517,10 +520,217 @@ def run_ours(args):
     return 0
 
 
+# ------------------------------------------------- batched workload -------
+def batch_bytes(info, iters, nen=3, dim=2):
+    """Algorithmic bytes of one batched step: every problem's assembly
+    (connectivity, coordinates, k, f, A and b written) plus, per CG + DIAG
+    iteration, the minimum fused FP64 traffic 12 nnz + 108 n, plus the
+    true-residual SpMV (12 nnz + 24 n)."""
+    nodes, elems, rows, nnz = (info[:, q].astype(np.float64) for q in range(4))
+    asm = 4 * nen * elems + 8 * dim * nodes + 8 * elems + 8 * nodes + 8 * nnz + 8 * rows
+    it = np.abs(iters).astype(np.float64)
+    return float((asm + it * (12 * nnz + 108 * rows) + 12 * nnz + 24 * rows).sum())
+
+
+def cpu_baseline_batch(sizes, iters, info, sample=16):
+    """The oracle port (1 thread) on a bounded sample of the batch: every
+    (count/sample)-th problem in size order, assembled and solved (CG + DIAG
+    to 1e-10) in full; the whole batch extrapolated by the sample's time per
+    (nonzeros x iterations)."""
+    from oracle import oracle as O
+    from ofeli_b200 import fields
+    order = np.argsort(sizes)
+    pick = order[np.linspace(0, len(order) - 1, sample).astype(int)]
+    t_sample, w_sample = 0.0, 0.0
+    for p in pick:
+        nx = int(sizes[p])
+        s = SEED * 7919 + int(p)
+        xy, elem, code = O.mesh2d(nx, nx)
+        xy = fields.jitter_2d(s, xy, code, nx, nx, radius=0.3)
+        cent = xy.reshape(-1, 2)[elem.reshape(-1, 3)].mean(axis=1)
+        k = fields.lognormal_k(s, cent, 1.0, 0.1, grid=128)
+        f = fields.uniform_pm1(s, code.size)
+        dof, n = O.number_equations(code)
+        rp, ci = O.node_graph(elem, 3, dof, n)
+        t0 = time.perf_counter()
+        a, b = O.assemble(2, xy, elem, dof, code, n, rp, ci, k=k, f=f)
+        x, it = O.cg(rp, ci, a, b, O.DIAG, 100000, TOL)
+        t_sample += time.perf_counter() - t0
+        w_sample += float(rp[-1]) * max(1, abs(it))
+    w_all = float((info[:, 3].astype(np.float64) * np.maximum(1, np.abs(iters))).sum())
+    t_all = t_sample * w_all / w_sample
+    cores = os.cpu_count() or 1
+    return {"value": len(sizes) / t_all, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": "oracle port, 1 thread: %d of the %d problems (evenly spaced in size) "
+                      "assembled and solved with CG + DIAG to 1e-10 in %.2f s; the batch "
+                      "extrapolated by time per (nonzeros x iterations) to %.1f s"
+                      % (sample, len(sizes), t_sample, t_all),
+            "host_cores": cores,
+            "all_cores_ideal": {"value": cores * len(sizes) / t_all, "cores": cores,
+                                "note": "one single-threaded process per core, perfect scaling "
+                                        "assumed (not measured)"}}
+
+
+def run_batch(args):
+    import torch
+    from ofeli_b200 import capi, problems
+    from ofeli_b200 import ofeli as F
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    work_stream = torch.cuda.Stream(device=torch.device("cuda", local))
+    torch.cuda.set_stream(work_stream)
+    capi.call("ofg_set_stream", ctypes.c_void_p(work_stream.cuda_stream))
+    dev = torch.device("cuda", local)
+    meshes, k_host, f_host = problems.uneven_batch(SEED)
+    sizes = problems.uneven_sizes(SEED)
+    B = F.Batch(meshes)
+    info = B.problem_info()
+    k_dev = torch.from_numpy(k_host).to(dev)
+    f_dev = torch.from_numpy(f_host).to(dev)
+    B.set_inputs(k_dev, f_dev)
+    t0 = time.perf_counter()
+    chosen, tune_ms = B.tune(100000, TOL)
+    tune_s = time.perf_counter() - t0
+    shape = F.Batch.config_shape(chosen)
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if not dist:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        B.solve(100000, TOL)
+    torch.cuda.synchronize()
+    launches0 = capi.launch_count()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.4)
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(work_stream)
+    for _ in range(args.steps):
+        B.solve(100000, TOL)
+    e1.record(work_stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    clk = clocks.stop()
+    launches = capi.launch_count() - launches0
+    u_dev, iters, res = B.results()
+    if res.max() > TOL or (iters < 0).any():
+        raise SystemExit("batched solve missed the FP64 target: %.3e" % res.max())
+
+    # end to end: k and f from pinned host memory, u back to pinned host
+    k_pin = torch.from_numpy(k_host).pin_memory()
+    f_pin = torch.from_numpy(f_host).pin_memory()
+    u_pin = torch.zeros(B.nodes, dtype=torch.float64).pin_memory()
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    g0 = torch.cuda.Event(enable_timing=True)
+    g1 = torch.cuda.Event(enable_timing=True)
+    g0.record(work_stream)
+    for _ in range(args.steps):
+        B.set_inputs(k_pin, f_pin)
+        B.solve(100000, TOL)
+        capi.call("ofg_batch_get_results", B._h, F._ptr(u_pin), None, None)
+    g1.record(work_stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(max(g0.elapsed_time(g1), (time.perf_counter() - t0) * 1e3))
+    if not np.array_equal(u_pin.numpy(), u_dev):
+        raise SystemExit("end-to-end result differs from the device-resident one")
+
+    # the plain form: one problem after another through the single-problem
+    # API (assembly + FP64 CG + DIAG per problem)
+    plain = None
+    if not args.no_plain and rank == 0:
+        mats = [F.SpMatrix(m) for m in meshes]
+        eoff = np.concatenate([[0], np.cumsum(info[:, 1])])
+        noff = np.concatenate([[0], np.cumsum(info[:, 0])])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        its = 0
+        for p, (m, A) in enumerate(zip(meshes, mats)):
+            b = torch.zeros(A.n, dtype=torch.float64, device=dev)
+            capi.call("ofg_assemble_p1", m._h, A._h, F._ptr(k_dev[eoff[p]:eoff[p + 1]]),
+                      F._ptr(f_dev[noff[p]:noff[p + 1]]), None, F._ptr(b))
+            x = torch.zeros(A.n, dtype=torch.float64, device=dev)
+            its += abs(F.CG(A, F.DIAG_PREC, b, x, 100000, TOL))
+        torch.cuda.synchronize()
+        t_plain = time.perf_counter() - t0
+        plain = {"solver": "one problem at a time: ofg_assemble_p1 + CG + DIAG (FP64) per problem",
+                 "solve_s": t_plain, "solves_per_s": len(meshes) / t_plain,
+                 "iterations_total": int(its)}
+        del mats
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return 0
+    peak, peak_kind = measured_peaks()
+    nbytes = batch_bytes(info, iters)
+    achieved = nbytes / (ms / args.steps * 1e-3) / 1e9
+    cpu = cpu_baseline_batch(sizes, iters, info) if world == 1 else None
+    line = {
+        "metric": METRIC_BATCH, "value": world * args.steps * B.nprob / (ms / 1e3),
+        "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "%d independent 2-D P1 diffusion problems, nodes log-uniform in "
+                               "[1e3, 6.4e4] (%d nodes, %d unknowns, %d nonzeros in all), "
+                               "jittered meshes, own lognormal k (sigma 1) and f each; assembly "
+                               "+ CG + DIAG to FP64 true rel. residual <= 1e-10 + insertBC, all "
+                               "in one persistent launch (CUDA graph)"
+                               % (B.nprob, B.nodes, B.rows, B.nnz),
+                   "seed": SEED, "inputs_larger_than_l2": True,
+                   "launch_shape": {"threads_per_block": shape[0], "lanes_per_row": shape[1],
+                                    "blocks_per_cluster": shape[2]},
+                   "autotuner_ms": [round(float(t), 2) for t in tune_ms], "tune_s": tune_s,
+                   "iterations": {"min": int(iters.min()), "mean": float(iters.mean()),
+                                  "max": int(iters.max())}},
+        "gpu_launches": launches,
+        "e2e": {"value": world * args.steps * B.nprob / (e2e_ms / 1e3), "unit": UNIT,
+                "h2d_bytes_per_step": 8 * (B.elements + B.nodes),
+                "d2h_bytes_per_step": 8 * B.nodes},
+        "roofline": {"kernel": "batch_kernel (assembly + CG + DIAG, every problem)",
+                     "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                     "bytes_per_launch": nbytes, "avg_launch_us": ms / args.steps * 1e3},
+        "plain": plain,
+        "cpu_baseline": cpu,
+        "clocks": clk,
+    }
+    print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batch2d":
+        return run_batch(args)
     return run_ours(args)
 
 

@@ -308,12 +308,16 @@ int ofg_batch_solve(ofg_batch* B, int max_it, double toler);
 int ofg_batch_get_results(const ofg_batch* B, double* u, int* iters, double* res);
 /* Assembled values (CSR order of the problem's pattern) and RHS of one problem. */
 int ofg_batch_get_matrix(const ofg_batch* B, int prob, double* values, double* rhs);
-/* Autotuner: times the whole batch once per launch shape (threads per block
- * x lanes per CSR row; ofg_batch_config_shape) and keeps the fastest;
- * *chosen = its index, times_ms (may be NULL) receives every shape's time. */
+/* Autotuner: solves once to measure every problem's work (rows x
+ * iterations), then times the whole batch once per launch shape (threads
+ * per block x lanes per CSR row x blocks per cluster, 18 shapes;
+ * ofg_batch_config_shape) and keeps the fastest; *chosen = its index,
+ * times_ms (may be NULL, 18 floats) receives every shape's time.  With
+ * clusters, a problem above one block's fair share of the work is solved by
+ * the whole cluster. */
 int ofg_batch_tune(ofg_batch* B, int max_it, double toler, int* chosen, float* times_ms);
 int ofg_batch_set_config(ofg_batch* B, int config, int blocks_per_sm);
-int ofg_batch_config_shape(int config, int* threads, int* lanes_per_row);
+int ofg_batch_config_shape(int config, int* threads, int* lanes_per_row, int* cluster);
 
 #ifdef __cplusplus
 }

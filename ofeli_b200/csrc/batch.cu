@@ -10,12 +10,19 @@
 // ||b - A x|| / ||b|| (the iteration continues from the true residual if the
 // check fails), and insertBC into the nodal solution.
 //
-// A block owns one problem at a time and takes the next one from a queue in
-// decreasing order of nonzeros (longest first), so all reductions are
-// block-local and nothing waits across blocks.  The launch shape -- threads
-// per block and the lanes that share one CSR row in the SpMV -- is a template
-// choice picked by a measured autotuner (ofg_batch_tune).  The launch (with
-// the queue reset) is captured in a CUDA graph and replayed.
+// Work is taken from a queue, most work first.  Without clusters a block owns
+// one problem at a time, so all reductions are block-local.  With
+// thread-block clusters (4 or 8 blocks) a problem larger than one block's
+// fair share of the total is solved by the whole cluster -- rows, nonzeros,
+// element colours and nodes split among its blocks, cluster barriers
+// between the phases, dot products summed over the blocks in rank order
+// through distributed shared memory -- and smaller problems are taken one
+// per block of the cluster, so that the largest problems no longer set the
+// length of the launch.  The launch shape -- threads per block, lanes per
+// CSR row in the SpMV, blocks per cluster -- is picked by a measured
+// autotuner (ofg_batch_tune) that first measures every problem's work (rows
+// x iterations).  The launch (with the queue reset) is captured in a CUDA
+// graph and replayed.
 #include <algorithm>
 #include <cmath>
 #include <numeric>
@@ -33,10 +40,17 @@ struct BatchProblem {
    int32_t nn, ne, n, ncolors;
 };
 
+// a work item: `count` problems order[first ..] taken one per block of a
+// cluster, or (big) one problem order[first] solved by the whole cluster
+struct BatchItem {
+   int32_t first, count, big, pad;
+};
+
 struct BatchArgs {
-   int nprob;
+   int nprob, nitems;
    const BatchProblem* probs;
    const int32_t* order;
+   const BatchItem* items;
    int* queue;
    // meshes
    const double* coords;
@@ -86,24 +100,97 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double (*sh)[THREADS 
    __syncthreads();
 }
 
-// y = A x over the problem's rows, LPR lanes per row; returns this thread's
-// share of (w, y) (w may be null) and, when b != null, of ||b - y||^2 with
-// b - y stored into rout
+// ---- thread-block clusters: rank, barrier, distributed shared memory loads
+__device__ __forceinline__ unsigned cluster_rank()
+{
+   unsigned r;
+   asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+   return r;
+}
+
+__device__ __forceinline__ void cluster_sync()
+{
+   asm volatile("barrier.cluster.arrive.release.aligned;\n\t"
+                "barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ uint32_t cluster_addr(const void* p, unsigned rank)
+{
+   uint32_t a = (uint32_t)__cvta_generic_to_shared(p), r;
+   asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+   return r;
+}
+
+__device__ __forceinline__ double ld_cluster(const double* p, unsigned rank)
+{
+   double v;
+   asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(cluster_addr(p, rank)) : "memory");
+   return v;
+}
+
+__device__ __forceinline__ int ld_cluster(const int* p, unsigned rank)
+{
+   int v;
+   asm volatile("ld.shared::cluster.s32 %0, [%1];" : "=r"(v) : "r"(cluster_addr(p, rank)) : "memory");
+   return v;
+}
+
+// The blocks working on one problem: one block (size 1: block barriers and
+// block reductions), or the whole cluster (size > 1: each block owns a
+// contiguous share of rows, nonzeros, element colours and nodes; cluster
+// barriers; reductions summed over the blocks in rank order through
+// distributed shared memory, double-buffered exchange slots).
+template <int THREADS>
+struct Team {
+   int rank, size;
+   double (*sh)[THREADS / 32];
+   double (*xr)[4];
+   int parity;
+   __device__ __forceinline__ void bar()
+   {
+      if (size == 1) __syncthreads();
+      else cluster_sync();
+   }
+   template <int NV>
+   __device__ __forceinline__ void sum(double (&v)[NV])
+   {
+      block_sum<NV, THREADS>(v, sh);
+      if (size > 1) {
+         if (threadIdx.x == 0)
+#pragma unroll
+            for (int i = 0; i < NV; ++i) xr[parity][i] = v[i];
+         cluster_sync();
+#pragma unroll
+         for (int i = 0; i < NV; ++i) {
+            double s = 0.0;
+            for (int r = 0; r < size; ++r) s += ld_cluster(&xr[parity][i], (unsigned)r);
+            v[i] = s;
+         }
+         parity ^= 1;
+      }
+   }
+   __device__ __forceinline__ int64_t lo(int64_t n) const { return n * rank / size; }
+   __device__ __forceinline__ int64_t hi(int64_t n) const { return n * (rank + 1) / size; }
+};
+
+// y = A x over rows [r0, r1), LPR lanes per row; adds this thread's share of
+// (w, y) to wy (w may be null) and, when b != null, of ||b - y||^2 to rr
+// with b - y stored into rout
 template <int THREADS, int LPR>
-__device__ __forceinline__ void block_spmv(int n, const int32_t* rp, const int32_t* col,
+__device__ __forceinline__ void block_spmv(int r0, int r1, const int32_t* rp, const int32_t* col,
                                            const double* val, const double* x, double* y,
                                            const double* w, double& wy, const double* b,
                                            double* rout, double& rr)
 {
    const int lane = threadIdx.x % LPR;
-   for (int i0 = 0; i0 < n; i0 += THREADS / LPR) {
+   for (int i0 = r0; i0 < r1; i0 += THREADS / LPR) {
       const int i = i0 + (int)threadIdx.x / LPR;
       double s = 0.0;
-      if (i < n)
+      if (i < r1)
          for (int k = rp[i] + lane; k < rp[i + 1]; k += LPR) s += val[k] * x[col[k]];
 #pragma unroll
       for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, LPR);
-      if (i < n && lane == 0) {
+      if (i < r1 && lane == 0) {
          if (y) y[i] = s;
          if (w) wy += w[i] * s;
          if (b) {
@@ -115,198 +202,292 @@ __device__ __forceinline__ void block_spmv(int n, const int32_t* rp, const int32
    }
 }
 
+// One problem: build(), CG + DIAG with the true-residual check, insertBC.
 template <int NEN, int THREADS, int LPR>
+__device__ void solve_problem(const BatchArgs& a, int pid, Team<THREADS>& T)
+{
+   const int tid = threadIdx.x;
+   const BatchProblem P = a.probs[pid];
+   const int n = P.n;
+   const double* xy = a.coords + P.node_off * (NEN - 1);  // dim = NEN - 1 coordinates
+   const int32_t* code = a.code + P.node_off;
+   const int32_t* dof = a.dof + P.node_off;
+   const int32_t* rp = a.row_ptr + P.rp_off;
+   const int32_t* col = a.col + P.nnz_off;
+   double* val = a.val + P.nnz_off;
+   double* b = a.b + P.row_off;
+   double* x = a.x + P.row_off;
+   double* r = a.r + P.row_off;
+   double* p = a.p + P.row_off;
+   double* q = a.q + P.row_off;
+   double* dinv = a.dinv + P.row_off;
+   const int nnz = rp[n];
+   const int r0 = (int)T.lo(n), r1 = (int)T.hi(n);
+
+   // ---- Equation::build(): zero, then one pass per element colour
+   for (int64_t k = T.lo(nnz) + tid; k < T.hi(nnz); k += THREADS) val[k] = 0.0;
+   for (int i = r0 + tid; i < r1; i += THREADS) b[i] = 0.0;
+   T.bar();
+   for (int c = 0; c < P.ncolors; ++c) {
+      const int64_t beg = a.color_ptr[P.color_base + c];
+      const int64_t cnt = a.color_ptr[P.color_base + c + 1] - beg;
+      for (int64_t t = beg + T.lo(cnt) + tid; t < beg + T.hi(cnt); t += THREADS) {
+         const int64_t e = a.color_elems[P.elem_off + t];
+         const int32_t* ep = a.elem + (P.elem_off + e) * NEN;
+         int32_t en[NEN];
+#pragma unroll
+         for (int i = 0; i < NEN; ++i) en[i] = ep[i];
+         // Laplace2DT3::LHS (times k) + BodyRHS, or DC3DT4::Diffusion(k) +
+         // BodyRHS: the operation order of the single-problem kernels
+         double g[NEN][3], meas;
+         bool ok;
+         if constexpr (NEN == 3) ok = tri3(xy, en, g, meas);
+         else ok = tet4(xy, en, g, meas);
+         if (!ok) {
+            atomicMin(a.bad, (int)(P.elem_off + e));
+            continue;
+         }
+         const double k = a.kel ? a.kel[P.elem_off + e] : 1.0;
+         double Ke[NEN][NEN], Fe[NEN];
+         if constexpr (NEN == 3) {
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+               for (int j = 0; j < 3; ++j) Ke[i][j] = meas * dot3(g[i], g[j]) * k;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) Fe[i] = a.f ? a.f[P.node_off + en[i]] * meas * kThird : 0.0;
+         }
+         else {
+            const double c4 = k * meas;
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+               for (int j = 0; j < 4; ++j) Ke[i][j] = c4 * dot3(g[i], g[j]);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) Fe[i] = a.f ? a.f[P.node_off + en[i]] * 0.25 * meas : 0.0;
+         }
+         if (a.bc) lift_bc<NEN>(en, code, a.bc + P.node_off, Ke, Fe);
+         scatter<NEN>(P.elem_off + e, en, dof, a.emap, Ke, Fe, val, b);
+      }
+      T.bar();
+   }
+
+   // ---- CG with the diagonal preconditioner (FP64)
+   double v[2] = {0.0, 0.0};
+   for (int i = r0 + tid; i < r1; i += THREADS) {
+      const double d = 1.0 / val[a.dpos[P.row_off + i]];
+      const double bi = b[i], zi = d * bi;
+      dinv[i] = d;
+      x[i] = 0.0;
+      r[i] = bi;
+      p[i] = zi;
+      v[0] += bi * bi;
+      v[1] += bi * zi;
+   }
+   T.sum(v);
+   double bnorm = sqrt(v[0]);
+   if (bnorm == 0.0) bnorm = 1.0;
+   double rho = v[1];
+   double res = sqrt(v[0]) / bnorm;
+   int it = 0;
+   bool done = res <= a.tol;
+   while (!done && it < a.max_it) {
+      ++it;
+      double w1[1] = {0.0}, dummy = 0.0;
+      block_spmv<THREADS, LPR>(r0, r1, rp, col, val, p, q, p, w1[0], nullptr, nullptr, dummy);
+      T.sum(w1);
+      const double alpha = rho / w1[0];
+      double u2[2] = {0.0, 0.0};
+      for (int i = r0 + tid; i < r1; i += THREADS) {
+         x[i] += alpha * p[i];
+         const double ri = r[i] - alpha * q[i];
+         r[i] = ri;
+         u2[0] += ri * ri;
+         u2[1] += ri * (dinv[i] * ri);
+      }
+      T.sum(u2);
+      res = sqrt(u2[0]) / bnorm;
+      double rz = u2[1];
+      bool restart = false;
+      if (res <= a.tol) {
+         // FP64 true residual; r <- b - A x either way
+         double w2[1] = {0.0}, d2 = 0.0;
+         block_spmv<THREADS, LPR>(r0, r1, rp, col, val, x, nullptr, nullptr, d2, b, r, w2[0]);
+         T.sum(w2);
+         res = sqrt(w2[0]) / bnorm;
+         if (res <= a.tol) {
+            done = true;
+            break;
+         }
+         restart = true;
+         double u3[1] = {0.0};
+         for (int i = r0 + tid; i < r1; i += THREADS) u3[0] += r[i] * (dinv[i] * r[i]);
+         T.sum(u3);
+         rz = u3[0];
+      }
+      const double beta = restart ? 0.0 : rz / rho;
+      rho = rz;
+      for (int i = r0 + tid; i < r1; i += THREADS) p[i] = dinv[i] * r[i] + beta * p[i];
+      T.bar();
+   }
+   if (!done && it > 0) {
+      // ran out: report the true residual
+      double w2[1] = {0.0}, d2 = 0.0;
+      block_spmv<THREADS, LPR>(r0, r1, rp, col, val, x, nullptr, nullptr, d2, b, q, w2[0]);
+      T.sum(w2);
+      res = sqrt(w2[0]) / bnorm;
+   }
+   T.bar();
+   // ---- insertBC into the nodal solution
+   for (int64_t i = T.lo(P.nn) + tid; i < T.hi(P.nn); i += THREADS) {
+      const int32_t dd = dof[i];
+      a.u[P.node_off + i] = dd ? x[dd - 1] : (a.bc ? a.bc[P.node_off + i] : 0.0);
+   }
+   if (T.rank == 0 && tid == 0) {
+      a.iters[pid] = done ? it : -it;
+      a.res[pid] = res;
+   }
+}
+
+// Persistent kernel: a block (CS == 1) or a cluster of CS blocks takes work
+// items from the queue until it is empty.  An item is either up to CS small
+// problems (one per block of the cluster) or one large problem that the
+// whole cluster solves together.
+template <int NEN, int THREADS, int LPR, int CS>
 __global__ void __launch_bounds__(THREADS) batch_kernel(BatchArgs a)
 {
-   __shared__ int s_slot;
+   __shared__ int s_item;
    __shared__ double sh[3][THREADS / 32];
+   __shared__ double xr[2][4];
    const int tid = threadIdx.x;
+   const unsigned rank = CS > 1 ? cluster_rank() : 0u;
+   Team<THREADS> T{0, 1, sh, xr, 0};
    for (;;) {
-      if (tid == 0) s_slot = atomicAdd(a.queue, 1);
-      __syncthreads();
-      const int slot = s_slot;
-      __syncthreads();
-      if (slot >= a.nprob) break;
-      const int pid = a.order[slot];
-      const BatchProblem P = a.probs[pid];
-      const int n = P.n;
-      const double* xy = a.coords + P.node_off * (NEN - 1);  // dim = NEN - 1 coordinates
-      const int32_t* code = a.code + P.node_off;
-      const int32_t* dof = a.dof + P.node_off;
-      const int32_t* rp = a.row_ptr + P.rp_off;
-      const int32_t* col = a.col + P.nnz_off;
-      double* val = a.val + P.nnz_off;
-      double* b = a.b + P.row_off;
-      double* x = a.x + P.row_off;
-      double* r = a.r + P.row_off;
-      double* p = a.p + P.row_off;
-      double* q = a.q + P.row_off;
-      double* dinv = a.dinv + P.row_off;
-      const int nnz = rp[n];
-
-      // ---- Equation::build(): zero, then one pass per element colour
-      for (int k = tid; k < nnz; k += THREADS) val[k] = 0.0;
-      for (int i = tid; i < n; i += THREADS) b[i] = 0.0;
-      __syncthreads();
-      for (int c = 0; c < P.ncolors; ++c) {
-         const int64_t beg = a.color_ptr[P.color_base + c], end = a.color_ptr[P.color_base + c + 1];
-         for (int64_t t = beg + tid; t < end; t += THREADS) {
-            const int64_t e = a.color_elems[P.elem_off + t];
-            const int32_t* ep = a.elem + (P.elem_off + e) * NEN;
-            int32_t en[NEN];
-#pragma unroll
-            for (int i = 0; i < NEN; ++i) en[i] = ep[i];
-            // Laplace2DT3::LHS (times k) + BodyRHS, or DC3DT4::Diffusion(k) +
-            // BodyRHS: the operation order of the single-problem kernels
-            double g[NEN][3], meas;
-            bool ok;
-            if constexpr (NEN == 3) ok = tri3(xy, en, g, meas);
-            else ok = tet4(xy, en, g, meas);
-            if (!ok) {
-               atomicMin(a.bad, (int)(P.elem_off + e));
-               continue;
-            }
-            const double k = a.kel ? a.kel[P.elem_off + e] : 1.0;
-            double Ke[NEN][NEN], Fe[NEN];
-            if constexpr (NEN == 3) {
-#pragma unroll
-               for (int i = 0; i < 3; ++i)
-#pragma unroll
-                  for (int j = 0; j < 3; ++j) Ke[i][j] = meas * dot3(g[i], g[j]) * k;
-#pragma unroll
-               for (int i = 0; i < 3; ++i) Fe[i] = a.f ? a.f[P.node_off + en[i]] * meas * kThird : 0.0;
-            }
-            else {
-               const double c = k * meas;
-#pragma unroll
-               for (int i = 0; i < 4; ++i)
-#pragma unroll
-                  for (int j = 0; j < 4; ++j) Ke[i][j] = c * dot3(g[i], g[j]);
-#pragma unroll
-               for (int i = 0; i < 4; ++i) Fe[i] = a.f ? a.f[P.node_off + en[i]] * 0.25 * meas : 0.0;
-            }
-            if (a.bc) lift_bc<NEN>(en, code, a.bc + P.node_off, Ke, Fe);
-            scatter<NEN>(P.elem_off + e, en, dof, a.emap, Ke, Fe, val, b);
-         }
+      int item;
+      if constexpr (CS == 1) {
+         if (tid == 0) s_item = atomicAdd(a.queue, 1);
+         __syncthreads();
+         item = s_item;
          __syncthreads();
       }
-
-      // ---- CG with the diagonal preconditioner (FP64)
-      double v[3] = {0.0, 0.0, 0.0};
-      for (int i = tid; i < n; i += THREADS) {
-         const double d = 1.0 / val[a.dpos[P.row_off + i]];
-         const double bi = b[i], zi = d * bi;
-         dinv[i] = d;
-         x[i] = 0.0;
-         r[i] = bi;
-         p[i] = zi;
-         v[0] += bi * bi;
-         v[1] += bi * zi;
+      else {
+         if (rank == 0 && tid == 0) s_item = atomicAdd(a.queue, 1);
+         cluster_sync();
+         item = ld_cluster(&s_item, 0u);
+         cluster_sync();
       }
-      block_sum<3, THREADS>(v, sh);
-      double bnorm = sqrt(v[0]);
-      if (bnorm == 0.0) bnorm = 1.0;
-      double rho = v[1];
-      double res = sqrt(v[0]) / bnorm;
-      int it = 0;
-      bool done = res <= a.tol;
-      while (!done && it < a.max_it) {
-         ++it;
-         double pq = 0.0, dummy = 0.0;
-         block_spmv<THREADS, LPR>(n, rp, col, val, p, q, p, pq, nullptr, nullptr, dummy);
-         double w1[1] = {pq};
-         block_sum<1, THREADS>(w1, sh);
-         const double alpha = rho / w1[0];
-         double u2[3] = {0.0, 0.0, 0.0};
-         for (int i = tid; i < n; i += THREADS) {
-            x[i] += alpha * p[i];
-            const double ri = r[i] - alpha * q[i];
-            r[i] = ri;
-            u2[0] += ri * ri;
-            u2[1] += ri * (dinv[i] * ri);
-         }
-         block_sum<3, THREADS>(u2, sh);
-         res = sqrt(u2[0]) / bnorm;
-         double rz = u2[1];
-         bool restart = false;
-         if (res <= a.tol) {
-            // FP64 true residual; r <- b - A x either way
-            double tr = 0.0, d2 = 0.0;
-            block_spmv<THREADS, LPR>(n, rp, col, val, x, nullptr, nullptr, d2, b, r, tr);
-            double w2[1] = {tr};
-            block_sum<1, THREADS>(w2, sh);
-            res = sqrt(w2[0]) / bnorm;
-            if (res <= a.tol) {
-               done = true;
-               break;
-            }
-            restart = true;
-            double u3[3] = {0.0, 0.0, 0.0};
-            for (int i = tid; i < n; i += THREADS) u3[0] += r[i] * (dinv[i] * r[i]);
-            block_sum<3, THREADS>(u3, sh);
-            rz = u3[0];
-         }
-         const double beta = restart ? 0.0 : rz / rho;
-         rho = rz;
-         for (int i = tid; i < n; i += THREADS) p[i] = dinv[i] * r[i] + beta * p[i];
-         __syncthreads();
+      if (item >= a.nitems) break;
+      const BatchItem w = a.items[item];
+      if (w.big) {
+         T.rank = (int)rank;
+         T.size = CS;
+         solve_problem<NEN, THREADS, LPR>(a, a.order[w.first], T);
       }
-      if (!done && it > 0) {
-         // ran out: report the true residual
-         double tr = 0.0, d2 = 0.0;
-         block_spmv<THREADS, LPR>(n, rp, col, val, x, nullptr, nullptr, d2, b, q, tr);
-         double w2[1] = {tr};
-         block_sum<1, THREADS>(w2, sh);
-         res = sqrt(w2[0]) / bnorm;
-      }
-      // ---- insertBC into the nodal solution
-      for (int i = tid; i < P.nn; i += THREADS) {
-         const int32_t dd = dof[i];
-         a.u[P.node_off + i] = dd ? x[dd - 1] : (a.bc ? a.bc[P.node_off + i] : 0.0);
-      }
-      if (tid == 0) {
-         a.iters[pid] = done ? it : -it;
-         a.res[pid] = res;
+      else if ((int)rank < w.count) {
+         T.rank = 0;
+         T.size = 1;
+         solve_problem<NEN, THREADS, LPR>(a, a.order[w.first + rank], T);
       }
       __syncthreads();
    }
 }
 
 struct Config {
-   int threads, lpr;
+   int threads, lpr, cs;
 };
-constexpr Config kConfigs[] = {{256, 1}, {256, 2}, {256, 4}, {256, 8}, {512, 1}, {512, 2},
-                               {512, 4}, {512, 8}, {1024, 1}, {1024, 2}, {1024, 4}, {1024, 8}};
+constexpr Config kConfigs[] = {
+   {256, 1, 1},  {256, 2, 1},  {512, 1, 1},  {512, 2, 1},  {1024, 1, 1}, {1024, 2, 1},
+   {256, 1, 4},  {256, 2, 4},  {512, 1, 4},  {512, 2, 4},  {1024, 1, 4}, {1024, 2, 4},
+   {256, 1, 8},  {256, 2, 8},  {512, 1, 8},  {512, 2, 8},  {1024, 1, 8}, {1024, 2, 8}};
 constexpr int kNumConfigs = sizeof(kConfigs) / sizeof(kConfigs[0]);
 
-template <int NEN, int T, int L>
-void launch_one(const BatchArgs& a, int blocks_per_sm, int nprob, cudaStream_t st)
+// blocks that run at once for a configuration (whole clusters)
+template <int NEN, int T, int L, int CS>
+int concurrent_blocks(int blocks_per_sm)
 {
-   int occ = 0;
-   OFG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_kernel<NEN, T, L>, T, 0));
-   occ = std::max(1, blocks_per_sm > 0 ? std::min(occ, blocks_per_sm) : occ);
-   const int grid = std::max(1, std::min(nprob, occ * num_sms()));
-   batch_kernel<NEN, T, L><<<grid, T, 0, st>>>(a);
+   if constexpr (CS == 1) {
+      int occ = 0;
+      OFG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_kernel<NEN, T, L, 1>, T, 0));
+      occ = std::max(1, blocks_per_sm > 0 ? std::min(occ, blocks_per_sm) : occ);
+      return occ * num_sms();
+   }
+   else {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(CS * num_sms());
+      cfg.blockDim = dim3(T);
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = CS;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      int nclusters = 0;
+      OFG_CUDA(cudaOccupancyMaxActiveClusters(&nclusters, batch_kernel<NEN, T, L, CS>, &cfg));
+      int blocks = std::max(1, nclusters) * CS;
+      if (blocks_per_sm > 0) blocks = std::min(blocks, std::max(CS, blocks_per_sm * num_sms() / CS * CS));
+      return blocks;
+   }
+}
+
+template <int NEN, int T, int L, int CS>
+void launch_one(const BatchArgs& a, int blocks, cudaStream_t st)
+{
+   if constexpr (CS == 1) {
+      batch_kernel<NEN, T, L, 1><<<std::max(1, blocks), T, 0, st>>>(a);
+   }
+   else {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(std::max(CS, blocks / CS * CS));
+      cfg.blockDim = dim3(T);
+      cfg.stream = st;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = CS;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      OFG_CUDA(cudaLaunchKernelEx(&cfg, batch_kernel<NEN, T, L, CS>, a));
+   }
    count_launch();
 }
 
+// dispatch over the configuration table: concurrency (launch == false) or
+// the launch itself
 template <int NEN>
-void launch_cfg(int c, const BatchArgs& a, int blocks_per_sm, int nprob, cudaStream_t st)
+int for_config(int c, bool launch, const BatchArgs* a, int blocks, int blocks_per_sm,
+               cudaStream_t st)
 {
+#define OFG_BATCH_CASE(idx, T, L, CS)                                        \
+   case idx:                                                                 \
+      if (launch) launch_one<NEN, T, L, CS>(*a, blocks, st);                 \
+      else return concurrent_blocks<NEN, T, L, CS>(blocks_per_sm);           \
+      return 0;
    switch (c) {
-      case 0: launch_one<NEN, 256, 1>(a, blocks_per_sm, nprob, st); break;
-      case 1: launch_one<NEN, 256, 2>(a, blocks_per_sm, nprob, st); break;
-      case 2: launch_one<NEN, 256, 4>(a, blocks_per_sm, nprob, st); break;
-      case 3: launch_one<NEN, 256, 8>(a, blocks_per_sm, nprob, st); break;
-      case 4: launch_one<NEN, 512, 1>(a, blocks_per_sm, nprob, st); break;
-      case 5: launch_one<NEN, 512, 2>(a, blocks_per_sm, nprob, st); break;
-      case 6: launch_one<NEN, 512, 4>(a, blocks_per_sm, nprob, st); break;
-      case 7: launch_one<NEN, 512, 8>(a, blocks_per_sm, nprob, st); break;
-      case 8: launch_one<NEN, 1024, 1>(a, blocks_per_sm, nprob, st); break;
-      case 9: launch_one<NEN, 1024, 2>(a, blocks_per_sm, nprob, st); break;
-      case 10: launch_one<NEN, 1024, 4>(a, blocks_per_sm, nprob, st); break;
-      default: launch_one<NEN, 1024, 8>(a, blocks_per_sm, nprob, st); break;
+      OFG_BATCH_CASE(0, 256, 1, 1)
+      OFG_BATCH_CASE(1, 256, 2, 1)
+      OFG_BATCH_CASE(2, 512, 1, 1)
+      OFG_BATCH_CASE(3, 512, 2, 1)
+      OFG_BATCH_CASE(4, 1024, 1, 1)
+      OFG_BATCH_CASE(5, 1024, 2, 1)
+      OFG_BATCH_CASE(6, 256, 1, 4)
+      OFG_BATCH_CASE(7, 256, 2, 4)
+      OFG_BATCH_CASE(8, 512, 1, 4)
+      OFG_BATCH_CASE(9, 512, 2, 4)
+      OFG_BATCH_CASE(10, 1024, 1, 4)
+      OFG_BATCH_CASE(11, 1024, 2, 4)
+      OFG_BATCH_CASE(12, 256, 1, 8)
+      OFG_BATCH_CASE(13, 256, 2, 8)
+      OFG_BATCH_CASE(14, 512, 1, 8)
+      OFG_BATCH_CASE(15, 512, 2, 8)
+      OFG_BATCH_CASE(16, 1024, 1, 8)
+      default: break;
    }
+   if (launch) launch_one<NEN, 1024, 2, 8>(*a, blocks, st);
+   else return concurrent_blocks<NEN, 1024, 2, 8>(blocks_per_sm);
+   return 0;
+#undef OFG_BATCH_CASE
 }
 
 }  // namespace
@@ -324,8 +505,14 @@ struct ofg_batch {
    ofg::DBuf<int64_t> color_ptr;
    ofg::DBuf<double> val, b, x, r, p, q, dinv, kel, f, bc, u, res;
    bool have_bc = false;
-   int config = 2;  // index into kConfigs
+   int config = 4;  // index into kConfigs
    int blocks_per_sm = 0;
+   // work estimate per problem (rows x iterations once measured) and the
+   // work items built from it for the current configuration
+   std::vector<double> work;
+   ofg::DBuf<ofg::BatchItem> items;
+   int nitems = 0, items_config = -1, blocks = 1;
+   bool work_measured = false;
    cudaGraph_t graph = nullptr;
    cudaGraphExec_t exec = nullptr;
    cudaStream_t capture = nullptr;
@@ -347,8 +534,10 @@ BatchArgs args_of(ofg_batch* B)
 {
    BatchArgs a{};
    a.nprob = B->nprob;
+   a.nitems = B->nitems;
    a.probs = B->d_probs.p;
    a.order = B->order.p;
+   a.items = B->items.p;
    a.queue = B->queue.p;
    a.coords = B->coords.p;
    a.elem = B->elem.p;
@@ -379,14 +568,75 @@ BatchArgs args_of(ofg_batch* B)
    return a;
 }
 
+int concurrency(ofg_batch* B, int config)
+{
+   return B->nen == 3 ? for_config<3>(config, false, nullptr, 0, B->blocks_per_sm, nullptr)
+                      : for_config<4>(config, false, nullptr, 0, B->blocks_per_sm, nullptr);
+}
+
+// Problem order (most work first) and work items for a configuration: with
+// clusters, a problem whose work exceeds one block's fair share of the
+// total gets the whole cluster; the others are grouped CS at a time in
+// order, so a group holds problems of similar size.  Items run in
+// decreasing order of their time per block.
+void build_items(ofg_batch* B, int config)
+{
+   if (B->items_config == config) return;
+   const int np = B->nprob, cs = kConfigs[config].cs;
+   std::vector<int32_t> order(np);
+   std::iota(order.begin(), order.end(), 0);
+   std::stable_sort(order.begin(), order.end(),
+                    [&](int32_t x, int32_t y) { return B->work[x] > B->work[y]; });
+   const double total = std::accumulate(B->work.begin(), B->work.end(), 0.0);
+   const double fair = total / std::max(1, concurrency(B, config));
+   std::vector<BatchItem> items;
+   std::vector<double> cost;
+   for (int i = 0; i < np;) {
+      const double w = B->work[order[i]];
+      if (cs > 1 && w > fair) {
+         items.push_back({i, 1, 1, 0});
+         cost.push_back(w / cs);
+         ++i;
+      }
+      else {
+         const int c = std::min(cs, np - i);
+         items.push_back({i, c, 0, 0});
+         cost.push_back(w);
+         i += c;
+      }
+   }
+   std::vector<int> idx(items.size());
+   std::iota(idx.begin(), idx.end(), 0);
+   std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return cost[x] > cost[y]; });
+   std::vector<BatchItem> sorted;
+   for (int k : idx) sorted.push_back(items[k]);
+   B->order.upload(order.data(), np);
+   B->items.upload(sorted.data(), sorted.size());
+   B->nitems = (int)sorted.size();
+   B->blocks = (int)std::min<int64_t>(concurrency(B, config), (int64_t)B->nitems * cs);
+   B->items_config = config;
+   OFG_CUDA(cudaStreamSynchronize(stream()));
+}
+
 // the queue reset and the persistent launch, as stream work
 void enqueue(ofg_batch* B, int config, cudaStream_t st)
 {
    OFG_CUDA(cudaMemsetAsync(B->queue.p, 0, sizeof(int), st));
    const BatchArgs a = args_of(B);
-   if (B->nen == 3) launch_cfg<3>(config, a, B->blocks_per_sm, B->nprob, st);
-   else launch_cfg<4>(config, a, B->blocks_per_sm, B->nprob, st);
+   if (B->nen == 3) for_config<3>(config, true, &a, B->blocks, B->blocks_per_sm, st);
+   else for_config<4>(config, true, &a, B->blocks, B->blocks_per_sm, st);
    OFG_LAUNCH_CHECK();
+}
+
+// per-problem work from the last solve's iteration counts
+void measure_work(ofg_batch* B)
+{
+   std::vector<int> it(B->nprob);
+   B->iters.download(it.data(), B->nprob);
+   for (int p = 0; p < B->nprob; ++p)
+      B->work[p] = (double)B->probs[p].n * (double)std::max(1, std::abs(it[p]));
+   B->work_measured = true;
+   B->items_config = -1;
 }
 
 // the same work through a CUDA graph, captured (on the batch's own capture
@@ -394,6 +644,10 @@ void enqueue(ofg_batch* B, int config, cudaStream_t st)
 // library stream
 void run_graph(ofg_batch* B)
 {
+   if (B->items_config != B->config) {
+      build_items(B, B->config);
+      B->graph_config = -1;
+   }
    if (B->graph_config != B->config) {
       if (B->exec) cudaGraphExecDestroy(B->exec);
       if (B->graph) cudaGraphDestroy(B->graph);
@@ -513,15 +767,13 @@ int ofg_batch_create(int nprob, ofg_mesh* const* meshes, ofg_batch** out)
          B->color_ptr.upload(cptr.data(), cptr.size());
          OFG_CUDA(cudaStreamSynchronize(stream()));
          for (auto* A : mats) delete A;
-         // longest problems first
-         std::vector<int32_t> order(nprob);
-         std::iota(order.begin(), order.end(), 0);
-         std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
-            const int64_t na = B->probs[a].ne, nb = B->probs[b].ne;
-            return na > nb;
-         });
+         // work estimate until iteration counts are measured: rows x
+         // rows^(1/2) (CG iterations grow like the mesh width in 2-D)
+         B->work.resize(nprob);
+         for (int p = 0; p < nprob; ++p)
+            B->work[p] = (double)B->probs[p].n * std::sqrt((double)std::max(1, B->probs[p].n));
          B->order.alloc(nprob);
-         B->order.upload(order.data(), nprob);
+         B->items.alloc(nprob);
          B->d_probs.alloc(nprob);
          B->d_probs.upload(B->probs.data(), nprob);
          B->queue.alloc(1);
@@ -646,8 +898,10 @@ int ofg_batch_get_matrix(const ofg_batch* B, int prob, double* values, double* r
    });
 }
 
-// Measured autotuner: runs the whole batch once per launch shape (threads
-// per block x lanes per CSR row) on the current inputs, keeps the fastest.
+// Measured autotuner: solves once to measure every problem's work, then runs
+// the whole batch once per launch shape (threads per block x lanes per CSR
+// row x blocks per cluster, with the work items built for that shape) on
+// the current inputs, and keeps the fastest.
 int ofg_batch_tune(ofg_batch* B, int max_it, double toler, int* chosen, float* times_ms)
 {
    return guarded("ofg_batch_tune", [&] {
@@ -659,7 +913,13 @@ int ofg_batch_tune(ofg_batch* B, int max_it, double toler, int* chosen, float* t
       OFG_CUDA(cudaEventCreate(&e1));
       float best = 1e30f;
       int best_c = B->config;
+      // the per-problem work the items are built from: measured iterations
+      build_items(B, B->config);
+      enqueue(B, B->config, stream());
+      OFG_CUDA(cudaStreamSynchronize(stream()));
+      measure_work(B);
       for (int c = 0; c < kNumConfigs; ++c) {
+         build_items(B, c);
          enqueue(B, c, stream());  // warm-up
          OFG_CUDA(cudaEventRecord(e0, stream()));
          enqueue(B, c, stream());
@@ -677,6 +937,7 @@ int ofg_batch_tune(ofg_batch* B, int max_it, double toler, int* chosen, float* t
       cudaEventDestroy(e1);
       check_bad(B);
       B->config = best_c;
+      B->items_config = -1;
       B->graph_config = -1;
       if (chosen) *chosen = best_c;
    });
@@ -689,16 +950,18 @@ int ofg_batch_set_config(ofg_batch* B, int config, int blocks_per_sm)
                   "bad arguments");
       B->config = config;
       B->blocks_per_sm = blocks_per_sm;
+      B->items_config = -1;
       B->graph_config = -1;
    });
 }
 
-int ofg_batch_config_shape(int config, int* threads, int* lanes_per_row)
+int ofg_batch_config_shape(int config, int* threads, int* lanes_per_row, int* cluster)
 {
    return guarded("ofg_batch_config_shape", [&] {
       OFG_REQUIRE(config >= 0 && config < kNumConfigs, OFG_ERR_ARG, "bad configuration");
       if (threads) *threads = kConfigs[config].threads;
       if (lanes_per_row) *lanes_per_row = kConfigs[config].lpr;
+      if (cluster) *cluster = kConfigs[config].cs;
    });
 }
 

@@ -394,6 +394,8 @@ class Batch:
     preconditioner in FP64 + insertBC.  Inputs are concatenated in problem
     order (k per element, f and bc per node)."""
 
+    NCONFIGS = 18
+
     def __init__(self, meshes):
         arr = (ctypes.c_void_p * len(meshes))(*[m._h.value for m in meshes])
         h = ctypes.c_void_p()
@@ -438,7 +440,7 @@ class Batch:
     def tune(self, max_it=100000, toler=1e-10):
         """Autotuner: (chosen launch shape index, time of every shape in ms)."""
         c = ctypes.c_int()
-        t = np.zeros(12, np.float32)
+        t = np.zeros(self.NCONFIGS, np.float32)
         _call("ofg_batch_tune", self._h, max_it, toler, ctypes.byref(c), _ptr(t))
         return c.value, t
 
@@ -447,9 +449,10 @@ class Batch:
 
     @staticmethod
     def config_shape(config):
-        t, l = ctypes.c_int(), ctypes.c_int()
-        _call("ofg_batch_config_shape", config, ctypes.byref(t), ctypes.byref(l))
-        return t.value, l.value
+        """(threads per block, lanes per CSR row, blocks per cluster)."""
+        t, l, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _call("ofg_batch_config_shape", config, ctypes.byref(t), ctypes.byref(l), ctypes.byref(c))
+        return t.value, l.value, c.value
 
     def __del__(self):
         if getattr(self, "_h", None) and capi is not None and capi._lib is not None:

@@ -70,12 +70,12 @@ def test_batch_with_dirichlet_data(cuda):
 
 def test_every_launch_shape_and_the_tuner(cuda):
     B, ref, _ = small_batch([25, 7, 14, 33, 3, 20], seed=11)
-    for c in range(12):
+    for c in range(F.Batch.NCONFIGS):
         B.set_config(c)
         B.solve(100000, TOL)
         check_against_oracle(B, ref, matrices=False)
     chosen, times = B.tune(100000, TOL)
-    assert 0 <= chosen < 12 and (times > 0).all()
+    assert 0 <= chosen < F.Batch.NCONFIGS and (times > 0).all()
     assert times[chosen] == times.min()
     B.solve(100000, TOL)
     check_against_oracle(B, ref, matrices=False)
@@ -115,3 +115,19 @@ def test_inverted_element_is_reported(cuda):
     with pytest.raises(F.OFELIException, match="Jacobian"):
         B.solve(1000, TOL)
 
+
+
+def test_clusters_mix_shared_and_per_block_problems(cuda):
+    """With thread-block clusters, the large problems are solved by a whole
+    cluster and the small ones one per block: both paths against the
+    oracle, for every clustered launch shape (concurrency limited so that
+    the small problems fall below one block's share of the work)."""
+    rng = np.random.default_rng(3)
+    sizes = [44, 37] + list(rng.integers(2, 7, size=300))
+    B, ref, _ = small_batch(sizes, seed=23)
+    for c in range(6, F.Batch.NCONFIGS):
+        B.set_config(c, blocks_per_sm=1)
+        B.solve(100000, TOL)
+        check_against_oracle(B, ref, matrices=False)
+    a, b = B.matrix(0, ref[0]["nnz"], ref[0]["n"])
+    assert rel_err(a, ref[0]["a"]) <= 1e-14 and rel_err(b, ref[0]["b"]) <= 1e-14
