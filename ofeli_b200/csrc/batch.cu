@@ -669,6 +669,7 @@ void run_graph(ofg_batch* B)
       B->graph_config = B->config;
    }
    OFG_CUDA(cudaGraphLaunch(B->exec, stream()));
+   count_launch();  // the graph's kernel (the queue reset is a memset)
 }
 
 void check_bad(ofg_batch* B)

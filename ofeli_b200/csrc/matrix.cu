@@ -377,6 +377,12 @@ void ensure_sell(ofg_matrix* A)
       A->sell_ptr.alloc(A->nslices + 1);
       A->sell_col.alloc(total > 0 ? total : 1);
       A->sell_src.alloc(total > 0 ? total : 1);
+      if (total == 0) {
+         // the one placeholder entry of an empty matrix is padding: the value
+         // copies below read nothing through it
+         OFG_CUDA(cudaMemsetAsync(A->sell_src.p, 0xFF, sizeof(int32_t), stream()));
+         OFG_CUDA(cudaMemsetAsync(A->sell_col.p, 0, sizeof(int32_t), stream()));
+      }
       if (A->nslices) {
          sell_fill<<<(unsigned)((A->nslices * 32 + 255) / 256), 256, 0, stream()>>>(
             A->n, A->nslices, A->row_ptr.p, A->col.p, sp64.p, A->sell_ptr.p, A->sell_col.p,
