@@ -31,6 +31,8 @@ sys.path.insert(0, HERE)
 
 METRIC = "FP64-accurate solves/sec (2-D P1 Poisson 2049x2049, true rel. residual <= 1e-10)"
 METRIC_3D = "FP64-accurate solves/sec (3-D P1 variable-k diffusion 129^3, true rel. residual <= 1e-10)"
+METRIC_TRANSIENT = ("backward-Euler time steps/sec (DC2DT3 convection-diffusion 1025x1025, "
+                    "GMRES(30) to 1e-10 per step, warm start)")
 METRIC_BATCH = ("FP64-accurate solves/sec (1024 uneven 2-D P1 problems, 1e3..6.4e4 nodes, "
                 "true rel. residual <= 1e-10)")
 UNIT = "solves/s"
@@ -49,10 +51,16 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nx", type=int, default=2048, help="cells per side (nodes = nx+1)")
-    ap.add_argument("--workload", default="poisson2d", choices=["poisson2d", "kuhn3d", "batch2d"],
+    ap.add_argument("--workload", default="poisson2d",
+                    choices=["poisson2d", "kuhn3d", "batch2d", "transient2d"],
                     help="poisson2d: the headline 2-D problem; kuhn3d: the 3-D "
                          "variable-coefficient problem (129^3 Kuhn cube, lognormal k); batch2d: "
-                         "1024 uneven jittered 2-D problems in one persistent launch")
+                         "1024 uneven jittered 2-D problems in one persistent launch; "
+                         "transient2d: DC2DT3 backward-Euler steps at 1025^2 (a step = one time "
+                         "step)")
+    ap.add_argument("--tprec", default="DIAG", choices=["ILU", "DIAG"],
+                    help="transient2d: GMRES(30) preconditioner of the timed steps (the plain "
+                         "ILU form is timed beside it)")
     ap.add_argument("--m3d", type=int, default=128, help="kuhn3d cells per side")
     ap.add_argument("--inner-bits", type=int, default=32, choices=[32, 16])
     ap.add_argument("--prec", default="jacobi", choices=["jacobi", "learned"],
@@ -725,12 +733,230 @@ def run_batch(args):
     return 0
 
 
+# ------------------------------------------------- transient workload -----
+T_NX, T_DT, T_EPS, T_M, T_TOL = 1024, 1e-3, 1e-3, 30, 1e-10
+
+
+def transient_fields(xy, code):
+    """u0 = Gaussian bump of width 0.05 at (0.3, 0.5), 0 on the boundary;
+    v = (-(y - 0.5), x - 0.5) at the nodes."""
+    P = xy.reshape(-1, 2)
+    u0 = np.exp(-((P[:, 0] - 0.3) ** 2 + (P[:, 1] - 0.5) ** 2) / (2 * 0.05 ** 2))
+    u0[code > 0] = 0.0
+    v = np.stack([-(P[:, 1] - 0.5), P[:, 0] - 0.5], axis=1).reshape(-1)
+    return u0, v
+
+
+def cpu_baseline_transient(nsteps=2):
+    """OFELI itself (reference sources, -Ofast) when it was built here, else
+    the oracle port: `nsteps` backward-Euler steps at 1025^2 with GMRES(30) +
+    ILU, graph construction once outside the steps."""
+    from oracle import oracle as O
+    xy, elem, code = O.mesh2d(T_NX, T_NX)
+    u0, v = transient_fields(xy, code)
+    flavour = "ofast" if O.have_reference("ofast") else ("o2" if O.have_reference("o2") else None)
+    if flavour:
+        info, _ = O.run_reference(["cd2d", T_NX, T_NX, nsteps, T_DT, T_EPS, "GMRES30", "ILU", T_TOL,
+                                   2000], {"u0": u0, "v": v}, flavour=flavour)
+        t_step = (float(info["t_assembly"]) + float(info["t_prec"]) + float(info["t_solve"])) / nsteps
+        return {"value": 1.0 / t_step, "unit": "steps/s", "cores": 1, "kind": "reference",
+                "sample": "OFELI (reference sources, -%s), 1 thread: %d DC2DT3 backward-Euler steps "
+                          "(build() + Prec + GMRES(30), warm start, %d GMRES iterations in all); "
+                          "graph %.1f s once, outside the steps"
+                          % ("Ofast" if flavour == "ofast" else "O2", nsteps,
+                             int(info["iters_total"]), float(info["t_graph"])),
+                "host_cores": os.cpu_count()}
+    dof, n = O.number_equations(code)
+    rp, ci = O.node_graph(elem, 3, dof, n)
+    u = u0.copy()
+    x = np.zeros(n)
+    t0 = time.perf_counter()
+    its = 0
+    for _ in range(nsteps):
+        a, b = O.assemble_cd2d(xy, elem, dof, code, n, rp, ci, T_EPS, v, T_DT, u)
+        x, it = O.gmres(rp, ci, a, b, O.ILU, T_M, 2000, T_TOL, x0=x)
+        its += abs(it)
+        u = O.insert_bc(code, x)
+    t_step = (time.perf_counter() - t0) / nsteps
+    return {"value": 1.0 / t_step, "unit": "steps/s", "cores": 1, "kind": "port",
+            "sample": "oracle port, 1 thread: %d backward-Euler steps at 1025^2 (assembly + "
+                      "D-ILU + GMRES(30), %d iterations)" % (nsteps, its),
+            "host_cores": os.cpu_count()}
+
+
+def run_transient(args):
+    import torch
+    from ofeli_b200 import capi
+    from ofeli_b200 import ofeli as F
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    work_stream = torch.cuda.Stream(device=torch.device("cuda", local))
+    torch.cuda.set_stream(work_stream)
+    capi.call("ofg_set_stream", ctypes.c_void_p(work_stream.cuda_stream))
+    dev = torch.device("cuda", local)
+    P_ = F._ptr
+    mesh = F.Mesh(0.0, 1.0, 0.0, 1.0, T_NX, T_NX, 1, 1, 1, 1)
+    xy, _, code, _ = mesh.arrays()
+    u0, v = transient_fields(xy, code)
+    A = F.SpMatrix(mesh)
+    n, nn = A.n, mesh.nn
+    prec = F.ILU_PREC if args.tprec == "ILU" else F.DIAG_PREC
+    u_dev = torch.from_numpy(u0).to(dev)
+    v_dev = torch.from_numpy(v).to(dev)
+    b_dev = torch.zeros(n, dtype=torch.float64, device=dev)
+    x_dev = torch.zeros(n, dtype=torch.float64, device=dev)
+    Pc = None
+    its = []
+
+    def step(u_in, u_out):
+        nonlocal Pc
+        capi.call("ofg_assemble_cd2d", mesh._h, A._h, T_EPS, P_(v_dev), T_DT, P_(u_in), None,
+                  P_(b_dev))
+        if Pc is None:
+            Pc = F.Prec(A, prec)
+        it = F.GMRes(A, Pc, b_dev, x_dev, T_M, 2000, T_TOL)  # refactorises: values changed
+        capi.call("ofg_insert_bc", mesh._h, P_(x_dev), None, P_(u_out))
+        its.append(it)
+        return it
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        step(u_dev, u_dev)
+    torch.cuda.synchronize()
+    del its[:]
+    launches0 = capi.launch_count()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.4)
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(work_stream)
+    for _ in range(args.steps):
+        step(u_dev, u_dev)
+    e1.record(work_stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    clk = clocks.stop()
+    launches = capi.launch_count() - launches0
+    if any(i <= 0 for i in its):
+        raise SystemExit("a GMRES solve did not converge: %s" % its)
+    res = F.residual(A, b_dev, x_dev)
+    timed_its = list(its)
+    # kernel families timed with CUDA events over two more steps (every 2nd
+    # launch), kept out of the timed steps
+    capi.profile_enable(2)
+    for _ in range(2):
+        step(u_dev, u_dev)
+    torch.cuda.synchronize()
+    prof = {k: capi.profile_read(k) for k in ("sweep", "spmv64", "assembly")}
+    capi.profile_enable(0)
+
+    # end to end: the state u lives on the host (pinned) and goes up and
+    # comes back every step
+    u_pin = torch.from_numpy(u_dev.cpu().numpy()).pin_memory()
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    g0 = torch.cuda.Event(enable_timing=True)
+    g1 = torch.cuda.Event(enable_timing=True)
+    g0.record(work_stream)
+    for _ in range(args.steps):
+        step(u_pin, u_pin)
+    g1.record(work_stream)
+    torch.cuda.synchronize()
+    e2e_ms = max(g0.elapsed_time(g1), (time.perf_counter() - t0) * 1e3)
+    # the plain form (OFELI's GMRES(30) + ILU) over 10 steps from the same
+    # initial state
+    plain = None
+    if rank == 0 and not args.no_plain and args.tprec != "ILU":
+        prec, Pc = F.ILU_PREC, None
+        u_dev.copy_(torch.from_numpy(u0).to(dev))
+        x_dev.zero_()
+        del its[:]
+        step(u_dev, u_dev)  # factorisation plan and first step, untimed
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(10):
+            step(u_dev, u_dev)
+        torch.cuda.synchronize()
+        t_pl = (time.perf_counter() - t0) / 10
+        plain = {"solver": "GMRES(30) + ILU (OFELI's diagonal ILU), FP64, warm start",
+                 "ms_per_step": t_pl * 1e3, "steps_per_s": 1.0 / t_pl,
+                 "gmres_iterations_per_step": statistics.mean(its[1:]),
+                 "true_rel_residual": F.residual(A, b_dev, x_dev)}
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return 0
+    cpu = cpu_baseline_transient() if world == 1 else None
+    peak, peak_kind = measured_peaks()
+    fam = max(("sweep", "spmv64"), key=lambda k: prof[k][1])
+    cnt, tot_ms, tot_bytes = prof[fam]
+    avg_us = tot_ms / max(cnt, 1) * 1e3
+    achieved = (tot_bytes / max(cnt, 1)) / (avg_us * 1e-6) / 1e9 if cnt else None
+    shares = {k: round(prof[k][1], 3) for k in prof}
+    line = {
+        "metric": METRIC_TRANSIENT, "value": world * args.steps / (ms / 1e3), "unit": "steps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "DC2DT3 on 1025x1025 nodes (%d unknowns, %d nonzeros): capacity + "
+                               "diffusion eps 1e-3 + convection v = (-(y-0.5), x-0.5), u0 Gaussian "
+                               "bump (0.3, 0.5) width 0.05, u = 0 on the boundary, backward Euler "
+                               "dt 1e-3; per step build() + Prec + GMRES(30) warm-started to "
+                               "OFELI's preconditioned residual 1e-10 + insertBC" % (n, A.nnz),
+                   "preconditioner": args.tprec,
+                   "gmres_iterations_per_step": statistics.mean(timed_its),
+                   "last_true_rel_residual": res, "inputs_larger_than_l2": True},
+        "gpu_launches": launches,
+        "e2e": {"value": world * args.steps / (e2e_ms / 1e3), "unit": "steps/s",
+                "h2d_bytes_per_step": 8 * nn, "d2h_bytes_per_step": 8 * nn},
+        "roofline": {"kernel": "solve_sweep (D-ILU triangular sweeps)" if fam == "sweep"
+                     else "spmv_sell_kernel (FP64 SELL-32 SpMV)",
+                     "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if achieved else None, "traffic": None,
+                     "peak_source": peak_kind, "launches_timed": cnt, "avg_launch_us": avg_us,
+                     "bytes_per_launch": tot_bytes / max(cnt, 1),
+                     "family_ms_sampled": shares},
+        "plain": plain,
+        "cpu_baseline": cpu,
+        "clocks": clk,
+    }
+    print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "batch2d":
         return run_batch(args)
+    if args.workload == "transient2d":
+        return run_transient(args)
     return run_ours(args)
 
 

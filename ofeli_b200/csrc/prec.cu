@@ -736,7 +736,10 @@ void launch_solve(ofg_prec* P, SweepPlan& plan, SolveArgs g)
    if (blocks < 1) blocks = 1;
    g.worked = prof_begin();
    solve_sweep<MODE><<<blocks, kWarpsPerBlock * 32, 0, stream()>>>(g);
-   prof_end(PROF_SWEEP, 0.0);
+   // algorithmic bytes: one triangle of the off-diagonal entries (FP64 value
+   // + int32 column), the pivots, the input, the output and the reset
+   const ofg_matrix* A = P->A;
+   prof_end(PROF_SWEEP, 6.0 * (double)(A->nnz - A->n) + 32.0 * (double)A->n);
    count_launch();
    OFG_LAUNCH_CHECK();
 }

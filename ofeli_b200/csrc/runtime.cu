@@ -13,6 +13,7 @@ std::atomic<int64_t> g_launches{0};
 cudaStream_t g_user_stream = nullptr;
 bool g_user_stream_set = false;
 cudaStream_t g_own_stream[64] = {};
+bool g_pool_ready[64] = {};
 int g_sms[64] = {};
 std::mutex g_mu;
 
@@ -27,21 +28,31 @@ int current_device()
 
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 
+// The device's default pool keeps freed blocks, so that the per-call scratch
+// allocations are served without returning memory to the driver at every
+// synchronisation (and mapping it again at the next call).  Done once per
+// device, whichever stream the library runs on.
+static void configure_pool(int d)
+{
+   if (g_pool_ready[d]) return;
+   std::lock_guard<std::mutex> lk(g_mu);
+   if (g_pool_ready[d]) return;
+   cudaMemPool_t pool;
+   OFG_CUDA(cudaDeviceGetDefaultMemPool(&pool, d));
+   uint64_t keep = UINT64_MAX;
+   OFG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+   g_pool_ready[d] = true;
+}
+
 cudaStream_t stream()
 {
-   if (g_user_stream_set) return g_user_stream;
    int d = current_device();
+   configure_pool(d);
+   if (g_user_stream_set) return g_user_stream;
    if (!g_own_stream[d]) {
       std::lock_guard<std::mutex> lk(g_mu);
-      if (!g_own_stream[d]) {
-         // The pool keeps freed blocks so that per-call scratch allocations
-         // are served without returning to the driver.
-         cudaMemPool_t pool;
-         OFG_CUDA(cudaDeviceGetDefaultMemPool(&pool, d));
-         uint64_t keep = UINT64_MAX;
-         OFG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+      if (!g_own_stream[d])
          OFG_CUDA(cudaStreamCreateWithFlags(&g_own_stream[d], cudaStreamNonBlocking));
-      }
    }
    return g_own_stream[d];
 }
