@@ -27,8 +27,13 @@ struct ofg_matrix {
    ofg::DBuf<int32_t> sell_src;  // CSR index of every SELL entry, -1 for padding
    ofg::DBuf<double> sell_val;
    ofg::DBuf<float> sell_val32;
+   ofg::DBuf<uint16_t> sell_valbf;  // BF16 bit patterns of the values
+   // column - row of every SELL entry (0 for padding) when every offset fits
+   // in 16 bits (idx16 = 1; 0 = does not fit; -1 = not built yet)
+   ofg::DBuf<int16_t> sell_d16;
+   int idx16 = -1;
    bool sell_ready = false;
-   uint64_t sell_version = 0, sell32_version = 0;
+   uint64_t sell_version = 0, sell32_version = 0, sellbf_version = 0;
    int max_row = 0;
    double avg_row = 0;
 
@@ -110,6 +115,9 @@ namespace ofg {
 void ensure_dpos(ofg_matrix* A);
 void ensure_sell(ofg_matrix* A);
 void ensure_sell32(ofg_matrix* A);
+void ensure_sell_bf16(ofg_matrix* A);
+// builds the 16-bit column offsets once per pattern; true when they fit
+bool ensure_sell_d16(ofg_matrix* A);
 void spmv_csr(const ofg_matrix* A, const double* x, double* y, bool add);
 void spmv_sell(const ofg_matrix* A, const double* x, double* y, const int* skip = nullptr);
 void matrix_touch(ofg_matrix* A);

@@ -9,6 +9,8 @@
 //     columns), so the matrix streams at full width; x gathers hit L2.
 //   * spmv_csr_vec_kernel: L lanes per row straight on CSR (L = the power of
 //     two covering the mean row length), used where no SELL copy exists.
+#include <cuda_bf16.h>
+
 #include "internal.cuh"
 
 namespace ofg {
@@ -146,6 +148,35 @@ __global__ void sell_values(int64_t total, const int32_t* ssrc, const double* va
    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
       int32_t s = ssrc[i];
       sval[i] = s >= 0 ? (T)val[s] : (T)0;
+   }
+}
+
+__global__ void sell_values_bf16(int64_t total, const int32_t* ssrc, const double* val,
+                                 uint16_t* sval)
+{
+   int64_t stride = (int64_t)gridDim.x * blockDim.x;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+      int32_t s = ssrc[i];
+      const __nv_bfloat16 v = __float2bfloat16(s >= 0 ? (float)val[s] : 0.0f);
+      sval[i] = *reinterpret_cast<const uint16_t*>(&v);
+   }
+}
+
+// column - row of every entry of SELL row r (0 for padding; padding rows of
+// the last slice point at themselves), flagging any offset beyond 16 bits
+__global__ void sell_offsets16(int64_t nslices, const int32_t* sp, const int32_t* scol,
+                               const int32_t* ssrc, int16_t* d16, int* wide)
+{
+   int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   if (r >= nslices * 32) return;
+   const int64_t s = r >> 5;
+   const int lane = (int)(r & 31);
+   const int64_t beg = sp[s], w = (sp[s + 1] - beg) / 32;
+   for (int64_t k = 0; k < w; ++k) {
+      const int64_t idx = beg + k * 32 + lane;
+      const int64_t d = ssrc[idx] >= 0 ? (int64_t)scol[idx] - r : 0;
+      if (d > 32767 || d < -32768) atomicOr(wide, 1);
+      d16[idx] = (int16_t)d;
    }
 }
 
@@ -421,6 +452,45 @@ void ensure_sell32(ofg_matrix* A)
       OFG_LAUNCH_CHECK();
       A->sell32_version = A->version;
    }
+}
+
+void ensure_sell_bf16(ofg_matrix* A)
+{
+   ensure_sell(A);
+   if (A->sellbf_version != A->version || A->sell_valbf.n != A->sell_val.n) {
+      int64_t total = A->sell_val.n;
+      A->sell_valbf.reserve(total);
+      sell_values_bf16<<<grid_for(total, 256), 256, 0, stream()>>>(total, A->sell_src.p, A->val.p,
+                                                                   A->sell_valbf.p);
+      count_launch();
+      OFG_LAUNCH_CHECK();
+      A->sellbf_version = A->version;
+   }
+}
+
+bool ensure_sell_d16(ofg_matrix* A)
+{
+   ensure_sell(A);
+   if (A->idx16 < 0) {
+      const int64_t total = A->sell_val.n;
+      A->sell_d16.alloc(total);
+      DBuf<int> wide(1);
+      wide.zero();
+      if (A->nslices) {
+         sell_offsets16<<<(unsigned)((A->nslices * 32 + 255) / 256), 256, 0, stream()>>>(
+            A->nslices, A->sell_ptr.p, A->sell_col.p, A->sell_src.p, A->sell_d16.p, wide.p);
+         count_launch();
+         OFG_LAUNCH_CHECK();
+      }
+      else {
+         A->sell_d16.zero();
+      }
+      int h = 0;
+      wide.download(&h, 1);
+      A->idx16 = h ? 0 : 1;
+      if (!A->idx16) A->sell_d16.release();
+   }
+   return A->idx16 == 1;
 }
 
 void spmv_csr(const ofg_matrix* A, const double* x, double* y, bool add)

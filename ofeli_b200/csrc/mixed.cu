@@ -119,10 +119,25 @@ __device__ __forceinline__ float4 load_vals(const __nv_bfloat16* p)
    return make_float4(fa.x, fa.y, fb.x, fb.y);
 }
 
+// the columns of four adjacent SELL entries: absolute int32 columns, or
+// 16-bit offsets from the rows r0 .. r0+3 (6 instead of 8 bytes per entry
+// with FP32 values, 4 with BF16 values)
+__device__ __forceinline__ int4 load_cols(const int32_t* p, int64_t)
+{
+   return *reinterpret_cast<const int4*>(p);
+}
+
+__device__ __forceinline__ int4 load_cols(const int16_t* p, int64_t r0)
+{
+   const short4 d = *reinterpret_cast<const short4*>(p);
+   const int r = (int)r0;
+   return make_int4(r + d.x, r + 1 + d.y, r + 2 + d.z, r + 3 + d.w);
+}
+
 // q = A p over four rows per thread, (p, q) -> alpha
-template <class T>
+template <class T, class I>
 __global__ void __launch_bounds__(kRedBlock, 8) mx_spmv(int64_t nquads, const int32_t* __restrict__ sp,
-                                                     const int32_t* __restrict__ scol,
+                                                     const I* __restrict__ scol,
                                                      const T* __restrict__ sval,
                                                      const float* __restrict__ p,
                                                      float* __restrict__ q, MixState* S,
@@ -141,11 +156,11 @@ __global__ void __launch_bounds__(kRedBlock, 8) mx_spmv(int64_t nquads, const in
       const int lane0 = (int)(r0 & 31);
       const int32_t beg = sp[s], w = (sp[s + 1] - beg) >> 5;
       float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-      const int32_t* cp = scol + beg + lane0;
+      const I* cp = scol + beg + lane0;
       const T* vp = sval + beg + lane0;
 #pragma unroll 8
       for (int32_t k = 0; k < w; ++k) {
-         const int4 c = *reinterpret_cast<const int4*>(cp + k * 32);
+         const int4 c = load_cols(cp + k * 32, r0);
          const float4 a = load_vals(vp + k * 32);
          acc.x += a.x * __ldg(p + c.x);
          acc.y += a.y * __ldg(p + c.y);
@@ -242,23 +257,26 @@ __global__ void __launch_bounds__(kRedBlock, 8) mx_direction(int64_t nquads,
 }
 
 // ---- learned preconditioner M = G^T G inside the FP32 iteration --------
-// G (lower rows) and G^T (upper rows) are SELL-32 matrices with FP32 values
-// on the same slices as A; a thread owns four consecutive rows.
+// G (lower rows) and G^T (upper rows) are SELL-32 matrices on the same
+// slices as A, with BF16 values (the preconditioner's own precision; the
+// flexible CG absorbs it) and 16-bit column offsets where they fit; a
+// thread owns four consecutive rows.
+template <class V, class I>
 __device__ __forceinline__ float4 sell_quad(const int32_t* __restrict__ sp,
-                                            const int32_t* __restrict__ scol,
-                                            const float* __restrict__ sval,
+                                            const I* __restrict__ scol,
+                                            const V* __restrict__ sval,
                                             const float* __restrict__ x, int64_t r0)
 {
    const int64_t s = r0 >> 5;
    const int lane0 = (int)(r0 & 31);
    const int32_t beg = sp[s], w = (sp[s + 1] - beg) >> 5;
    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-   const int32_t* cp = scol + beg + lane0;
-   const float* vp = sval + beg + lane0;
+   const I* cp = scol + beg + lane0;
+   const V* vp = sval + beg + lane0;
 #pragma unroll 4
    for (int32_t k = 0; k < w; ++k) {
-      const int4 c = *reinterpret_cast<const int4*>(cp + k * 32);
-      const float4 a = *reinterpret_cast<const float4*>(vp + k * 32);
+      const int4 c = load_cols(cp + k * 32, r0);
+      const float4 a = load_vals(vp + k * 32);
       acc.x += a.x * __ldg(x + c.x);
       acc.y += a.y * __ldg(x + c.y);
       acc.z += a.z * __ldg(x + c.z);
@@ -268,9 +286,10 @@ __device__ __forceinline__ float4 sell_quad(const int32_t* __restrict__ sp,
 }
 
 // t = G r
+template <class V, class I>
 __global__ void __launch_bounds__(kRedBlock, 8) lg_lower(int64_t nquads, const int32_t* __restrict__ sp,
-                                                      const int32_t* __restrict__ scol,
-                                                      const float* __restrict__ sval,
+                                                      const I* __restrict__ scol,
+                                                      const V* __restrict__ sval,
                                                       const float* __restrict__ r, float* t,
                                                       const MixState* S, int* worked)
 {
@@ -286,9 +305,10 @@ __global__ void __launch_bounds__(kRedBlock, 8) lg_lower(int64_t nquads, const i
 // z = G^T t; rho = (r, z); beta of the next direction: flexible
 // (Polak-Ribiere) -alpha (z, q) / rho_old, or rho / rho_old right after a
 // refinement replaced r (fr = 1)
+template <class V, class I>
 __global__ void __launch_bounds__(kRedBlock, 8) lg_upper(int64_t nquads, const int32_t* __restrict__ sp,
-                                                      const int32_t* __restrict__ scol,
-                                                      const float* __restrict__ sval,
+                                                      const I* __restrict__ scol,
+                                                      const V* __restrict__ sval,
                                                       const float* __restrict__ t, float* z,
                                                       const float* __restrict__ r,
                                                       const float* __restrict__ q, MixState* S,
@@ -390,14 +410,20 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
    ensure_sell(A);
    ensure_dpos(A);
    OFG_REQUIRE(A->dpos_complete, OFG_ERR_PIVOT, "a row has no diagonal entry");
+   bool g16 = false;
    if (learned) {
       if (LP->version != A->version) prec_setup(LP);
-      ensure_sell32(LP->gl);
-      ensure_sell32(LP->gu);
+      ensure_sell_bf16(LP->gl);
+      ensure_sell_bf16(LP->gu);
+      g16 = ensure_sell_d16(LP->gl) && ensure_sell_d16(LP->gu);
       OFG_REQUIRE(LP->gl->nslices == A->nslices && LP->gu->nslices == A->nslices, OFG_ERR_ARG,
                   "learned factor does not match the matrix");
    }
    const int64_t npad = A->nslices * 32, nquads = npad / 4;
+   // 16-bit column offsets when every |column - row| fits (banded orderings,
+   // structured meshes): 2 bytes less per entry streamed by every SpMV
+   const bool a16 = ensure_sell_d16(A);
+   const double aidx = a16 ? 2.0 : 4.0;
    DBuf<__nv_bfloat16> v16;
    if (inner_bits == 32) ensure_sell32(A);
    else {
@@ -436,16 +462,32 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
       OFG_LAUNCH_CHECK();
    };
    // z = G^T G r, rho, beta, then the new direction
+   // algorithmic bytes of the two factor products: BF16 value + column
+   // index (2 or 4 bytes) per entry, the gathered input and the output (and
+   // r, q for the reduction of the second)
+   const double gidx = g16 ? 2.0 : 4.0;
    auto learned_direction = [&](int fr, int fresh) {
+      using bf = __nv_bfloat16;
+      const bf* vl = reinterpret_cast<const bf*>(learned ? LP->gl->sell_valbf.p : nullptr);
+      const bf* vu = reinterpret_cast<const bf*>(learned ? LP->gu->sell_valbf.p : nullptr);
       int* worked = prof_begin();
-      launch_pdl(lg_lower, gq, kRedBlock, nquads, LP->gl->sell_ptr.p, LP->gl->sell_col.p,
-                 LP->gl->sell_val32.p, rr.p, tz.p, S.p, worked);
-      prof_end(PROF_LEARNED_APPLY, 8.0 * LP->gl->nnz + 8.0 * n);
+      if (g16)
+         launch_pdl(lg_lower<bf, int16_t>, gq, kRedBlock, nquads, LP->gl->sell_ptr.p,
+                    LP->gl->sell_d16.p, vl, rr.p, tz.p, S.p, worked);
+      else
+         launch_pdl(lg_lower<bf, int32_t>, gq, kRedBlock, nquads, LP->gl->sell_ptr.p,
+                    LP->gl->sell_col.p, vl, rr.p, tz.p, S.p, worked);
+      prof_end(PROF_LEARNED_APPLY, (2.0 + gidx) * LP->gl->nnz + 8.0 * n);
       worked = prof_begin();
-      launch_pdl(lg_upper, gq, kRedBlock, nquads, LP->gu->sell_ptr.p, LP->gu->sell_col.p,
-                 LP->gu->sell_val32.p, tz.p, zz.p, rr.p, q.p, S.p, partials.p, counter.p, fr,
-                 worked);
-      prof_end(PROF_LEARNED_APPLY, 8.0 * LP->gu->nnz + 16.0 * n);
+      if (g16)
+         launch_pdl(lg_upper<bf, int16_t>, gq, kRedBlock, nquads, LP->gu->sell_ptr.p,
+                    LP->gu->sell_d16.p, vu, tz.p, zz.p, rr.p, q.p, S.p, partials.p, counter.p, fr,
+                    worked);
+      else
+         launch_pdl(lg_upper<bf, int32_t>, gq, kRedBlock, nquads, LP->gu->sell_ptr.p,
+                    LP->gu->sell_col.p, vu, tz.p, zz.p, rr.p, q.p, S.p, partials.p, counter.p, fr,
+                    worked);
+      prof_end(PROF_LEARNED_APPLY, (2.0 + gidx) * LP->gu->nnz + 16.0 * n);
       launch_pdl(lg_direction, gq, kRedBlock, nquads, zz.p, p.p, S.p, fresh);
    };
    MixState h{};
@@ -486,14 +528,24 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
             // launch: each one's blocks start while the previous one drains
             // its reduction tail
             int* worked = prof_begin();
-            if (inner_bits == 32)
-               launch_pdl(mx_spmv<float>, gq, kRedBlock, nquads, A->sell_ptr.p, A->sell_col.p,
-                          A->sell_val32.p, p.p, q.p, S.p, partials.p, counter.p, worked);
+            if (inner_bits == 32 && a16)
+               launch_pdl(mx_spmv<float, int16_t>, gq, kRedBlock, nquads, A->sell_ptr.p,
+                          A->sell_d16.p, A->sell_val32.p, p.p, q.p, S.p, partials.p, counter.p,
+                          worked);
+            else if (inner_bits == 32)
+               launch_pdl(mx_spmv<float, int32_t>, gq, kRedBlock, nquads, A->sell_ptr.p,
+                          A->sell_col.p, A->sell_val32.p, p.p, q.p, S.p, partials.p, counter.p,
+                          worked);
+            else if (a16)
+               launch_pdl(mx_spmv<__nv_bfloat16, int16_t>, gq, kRedBlock, nquads, A->sell_ptr.p,
+                          A->sell_d16.p, v16.p, p.p, q.p, S.p, partials.p, counter.p, worked);
             else
-               launch_pdl(mx_spmv<__nv_bfloat16>, gq, kRedBlock, nquads, A->sell_ptr.p,
+               launch_pdl(mx_spmv<__nv_bfloat16, int32_t>, gq, kRedBlock, nquads, A->sell_ptr.p,
                           A->sell_col.p, v16.p, p.p, q.p, S.p, partials.p, counter.p, worked);
+            // algorithmic bytes: value (4 or 2) + column index (4, or 2 as a
+            // 16-bit offset) per entry, p gathered, q written, p read for the dot
             prof_end(inner_bits == 32 ? PROF_SPMV32 : PROF_SPMV16,
-                     (inner_bits == 32 ? 8.0 : 6.0) * A->nnz + 12.0 * n + 4.0);
+                     ((inner_bits == 32 ? 4.0 : 2.0) + aidx) * A->nnz + 12.0 * n + 4.0);
             if (learned) {
                launch_pdl(mx_update<false>, gq, kRedBlock, nquads, d.p, p.p, rr.p, q.p, jac, S.p,
                           partials.p, counter.p, inner_tol, tol, scale, max_inner, mode);

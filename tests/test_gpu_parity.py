@@ -259,3 +259,33 @@ def test_mixed_precision_reaches_fp64_accuracy(p2d65, bits, mode):
     assert res <= 1e-10 and F.residual(A, g["b"], x) <= 1e-10
     err = rel_err(x, xref)
     assert err <= 1e-7, "error vs FP64 solution %.2e" % err
+
+
+@pytest.mark.parametrize("permute", [False, True])
+def test_mixed_precision_column_offset_formats(cuda, permute):
+    """The FP32 SpMV streams 16-bit column offsets when every |column - row|
+    fits in 16 bits and absolute int32 columns otherwise.  A 201x201 Poisson
+    matrix (n = 39 601) in natural order takes the first form; the same
+    matrix under a random symmetric permutation (offsets up to n) the second.
+    Both reach the FP64 target and the oracle's FP64 solution."""
+    xy, elem, code = O.mesh2d(200, 200)
+    dof, n = O.number_equations(code)
+    rp, ci = O.node_graph(elem, 3, dof, n)
+    f = fields.uniform_pm1(41, code.size)
+    a, b = O.assemble(2, xy, elem, dof, code, n, rp, ci, f=f, bc=np.zeros(code.size))
+    if permute:
+        perm = np.random.default_rng(0).permutation(n)  # new index of old row i
+        inv = np.argsort(perm)
+        rows = np.repeat(np.arange(n), np.diff(rp))
+        nr, nc = perm[rows], perm[ci - 1]
+        order = np.lexsort((nc, nr))
+        a, nr, nc = a[order], nr[order], nc[order]
+        rp = np.concatenate([[0], np.cumsum(np.bincount(nr, minlength=n))]).astype(np.int64)
+        ci = (nc + 1).astype(np.int64)
+        b = b[inv]
+    xref, _ = O.cg(rp, ci, a, b, O.DIAG, 40000, 1e-13)
+    A = F.SpMatrix(rp, ci, a)
+    x = np.zeros(n)
+    outer, inner, res = F.solve_mixed(A, b, x, prec=F.DIAG_PREC, toler=1e-10)
+    assert res <= 1e-10 and F.residual(A, b, x) <= 1e-10
+    assert rel_err(x, xref) <= 1e-6
