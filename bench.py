@@ -6,10 +6,15 @@ boundary.
 One step = Equation::build() (element assembly into the CSR matrix and RHS
 from the source term resident in HBM) + the solve to an FP64 true relative
 residual ||b - A x|| / ||b|| <= 1e-10 + insertBC.  The chosen solver is the
-mixed-precision one (FP64 refinement around FP32 Jacobi-PCG); the plain FP64
-CG + D-ILU solve (OFELI's own method) is timed once beside it.
+learned + mixed-precision one: FP64 refinement around a flexible CG in FP32
+whose preconditioner M = G^T G is predicted by the library's network from the
+assembled matrix inside every step (the network is trained once before the
+timed region, on small problems, by the library's own kernels); `--prec
+jacobi` selects the Jacobi inner iteration.  The plain FP64 CG + D-ILU solve
+(OFELI's own method) is timed once beside it.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--workload poisson2d|kuhn3d|batch2d|transient2d]
 
 N > 1 runs N independent replicas (the problem does not shard; no
 collective in the data path), launched one rank per GPU by torchrun.
@@ -58,14 +63,18 @@ def parse():
                          "1024 uneven jittered 2-D problems in one persistent launch; "
                          "transient2d: DC2DT3 backward-Euler steps at 1025^2 (a step = one time "
                          "step)")
+    ap.add_argument("--nprob", type=int, default=1024,
+                    help="batch2d: number of problems (the workload is 1024; smaller counts are "
+                         "for profiling captures)")
     ap.add_argument("--tprec", default="DIAG", choices=["ILU", "DIAG"],
                     help="transient2d: GMRES(30) preconditioner of the timed steps (the plain "
                          "ILU form is timed beside it)")
     ap.add_argument("--m3d", type=int, default=128, help="kuhn3d cells per side")
     ap.add_argument("--inner-bits", type=int, default=32, choices=[32, 16])
-    ap.add_argument("--prec", default="jacobi", choices=["jacobi", "learned"],
-                    help="preconditioner of the FP32 inner iteration (learned: kuhn3d only; "
-                         "the network is trained first, outside the timed region)")
+    ap.add_argument("--prec", default="learned", choices=["jacobi", "learned"],
+                    help="preconditioner of the FP32 inner iteration (learned: the network is "
+                         "trained first on small problems of the workload's dimension, outside "
+                         "the timed region, and runs inside every step)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 CG+D-ILU solve")
     ap.add_argument("--cpu-iters", type=int, default=10, help="CG iterations per CPU sample")
     return ap.parse_args()
@@ -298,10 +307,8 @@ def run_ours(args):
     stream = work_stream
     PL, train_info, fell_back = None, None, []
     if args.prec == "learned":
-        if args.workload != "kuhn3d":
-            raise SystemExit("--prec learned runs on the kuhn3d workload")
         from ofeli_b200 import learned as LN
-        net, train_info = LN.train_default()
+        net, train_info = LN.train_default(dim=3 if args.workload == "kuhn3d" else 2)
         capi.call("ofg_assemble_p1", mesh._h, A._h, P(k_dev), P(f_dev), None, P(b_dev))
         PL = F.Prec(A, F.LEARNED_PREC, net=net)
 
@@ -600,8 +607,8 @@ def run_batch(args):
     torch.cuda.set_stream(work_stream)
     capi.call("ofg_set_stream", ctypes.c_void_p(work_stream.cuda_stream))
     dev = torch.device("cuda", local)
-    meshes, k_host, f_host = problems.uneven_batch(SEED)
-    sizes = problems.uneven_sizes(SEED)
+    meshes, k_host, f_host = problems.uneven_batch(SEED, count=args.nprob)
+    sizes = problems.uneven_sizes(SEED, count=args.nprob)
     B = F.Batch(meshes)
     info = B.problem_info()
     k_dev = torch.from_numpy(k_host).to(dev)

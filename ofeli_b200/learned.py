@@ -26,6 +26,22 @@ def kuhn_problem(M, seed, sigma=1.5, corr_len=0.1, grid=64):
     return eq.getMatrix(), np.array(eq.getRHS()), mesh
 
 
+def square_problem(nx, seed, sigma=None, corr_len=0.1, grid=128):
+    """2-D P1 problem -div(k grad u) = f on the unit square with nx x nx cells
+    (Laplace2DT3), f ~ U[-1, 1] per node, u = 0 on the boundary, k = 1 or
+    log-normal with standard deviation sigma.  Returns (A, b, mesh)."""
+    mesh = F.Mesh(0.0, 1.0, 0.0, 1.0, nx, nx, 1, 1, 1, 1)
+    eq = F.Laplace2DT3(mesh)
+    eq.setSource(fields.uniform_pm1(seed, mesh.nn))
+    eq.setDirichlet(np.zeros(mesh.nn))
+    if sigma:
+        xy, elem, _, _ = mesh.arrays()
+        cent = xy.reshape(-1, 2)[elem.reshape(-1, 3)].mean(axis=1)
+        eq.setElementCoefficient(fields.lognormal_k(seed, cent, sigma, corr_len, grid=grid))
+    eq.build()
+    return eq.getMatrix(), np.array(eq.getRHS()), mesh
+
+
 def train(net, problems, rounds=8, steps=10, batch=16, lr=1e-3, npairs=64):
     """Trains on residual / error pairs of every problem in turn (`steps`
     Adam steps per visit, `rounds` visits each).  problems: (A, b) pairs.
@@ -41,21 +57,27 @@ def train(net, problems, rounds=8, steps=10, batch=16, lr=1e-3, npairs=64):
     return hist
 
 
-def train_default(seed=7, M=20, nproblems=4, rounds=8):
-    """The network used by the benchmark: trained on `nproblems` Kuhn cubes
-    of M^3 cells with log-normal conductivities (sigma 1.5, correlation
-    length 0.1; seeds 100, 101, ...).  Returns (net, info)."""
+def train_default(seed=7, M=20, nproblems=4, rounds=8, dim=3):
+    """The networks used by the benchmark: trained on `nproblems` problems
+    (seeds 100, 101, ...) -- 3-D: Kuhn cubes of M^3 cells with log-normal
+    conductivities (sigma 1.5, correlation length 0.1); 2-D: squares of
+    (6M + 8)^2 cells, alternately k = 1 and log-normal k (sigma 1).  Returns
+    (net, info)."""
     t0 = time.perf_counter()
     net = F.LearnedNet(seed)
     problems = []
     keep = []
     for s in range(nproblems):
-        A, b, mesh = kuhn_problem(M, 100 + s)
+        if dim == 3:
+            A, b, mesh = kuhn_problem(M, 100 + s)
+        else:
+            A, b, mesh = square_problem(6 * M + 8, 100 + s, None if s % 2 == 0 else 1.0)
         problems.append((A, b))
         keep.append(mesh)
     hist = train(net, problems, rounds=rounds)
+    what = ("%d Kuhn cubes %d^3 nodes, lognormal k (sigma 1.5)" % (nproblems, M + 1) if dim == 3
+            else "%d squares %d^2 nodes, k = 1 and lognormal k (sigma 1)" % (nproblems, 6 * M + 9))
     info = {"train_s": time.perf_counter() - t0, "adam_steps": rounds * nproblems * 10,
-            "problems": "%d Kuhn cubes %d^3 nodes, lognormal k (sigma 1.5)" % (nproblems, M + 1),
-            "pairs_per_problem": 64, "loss_first": hist[0], "loss_last": hist[-1],
-            "objective": "Kaporin number of M A on the pairs"}
+            "problems": what, "pairs_per_problem": 64, "loss_first": hist[0],
+            "loss_last": hist[-1], "objective": "Kaporin number of M A on the pairs"}
     return net, info
