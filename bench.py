@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--nprob", type=int, default=1024,
                     help="batch2d: number of problems (the workload is 1024; smaller counts are "
                          "for profiling captures)")
+    ap.add_argument("--batch-bits", type=int, default=32, choices=[32, 64],
+                    help="batch2d: inner CG precision (32: FP32 CG inside FP64 refinement)")
     ap.add_argument("--tprec", default="DIAG", choices=["ILU", "DIAG"],
                     help="transient2d: GMRES(30) preconditioner of the timed steps (the plain "
                          "ILU form is timed beside it)")
@@ -536,15 +538,19 @@ def run_ours(args):
 
 
 # ------------------------------------------------- batched workload -------
-def batch_bytes(info, iters, nen=3, dim=2):
+def batch_bytes(info, iters, nen=3, dim=2, bits=64):
     """Algorithmic bytes of one batched step: every problem's assembly
     (connectivity, coordinates, k, f, A and b written) plus, per CG + DIAG
-    iteration, the minimum fused FP64 traffic 12 nnz + 108 n, plus the
-    true-residual SpMV (12 nnz + 24 n)."""
+    iteration, the minimum fused traffic -- FP64: 12 nnz + 108 n; FP32 inner
+    iteration (FP32 value + 16-bit offset per entry): 6 nnz + 54 n, plus the
+    FP32 value copy (12 nnz) once -- plus one true-residual SpMV in FP64
+    (12 nnz + 24 n)."""
     nodes, elems, rows, nnz = (info[:, q].astype(np.float64) for q in range(4))
     asm = 4 * nen * elems + 8 * dim * nodes + 8 * elems + 8 * nodes + 8 * nnz + 8 * rows
     it = np.abs(iters).astype(np.float64)
-    return float((asm + it * (12 * nnz + 108 * rows) + 12 * nnz + 24 * rows).sum())
+    per_it = 12 * nnz + 108 * rows if bits == 64 else 6 * nnz + 54 * rows
+    extra = 0 if bits == 64 else 12 * nnz
+    return float((asm + extra + it * per_it + 12 * nnz + 24 * rows).sum())
 
 
 def cpu_baseline_batch(sizes, iters, info, sample=16):
@@ -614,6 +620,7 @@ def run_batch(args):
     k_dev = torch.from_numpy(k_host).to(dev)
     f_dev = torch.from_numpy(f_host).to(dev)
     B.set_inputs(k_dev, f_dev)
+    B.set_precision(args.batch_bits)
     t0 = time.perf_counter()
     chosen, tune_ms = B.tune(100000, TOL)
     tune_s = time.perf_counter() - t0
@@ -674,6 +681,27 @@ def run_batch(args):
     if not np.array_equal(u_pin.numpy(), u_dev):
         raise SystemExit("end-to-end result differs from the device-resident one")
 
+    # the other inner precision, same launch shape
+    other = None
+    if rank == 0:
+        ob = 64 if args.batch_bits == 32 else 32
+        B.set_precision(ob)
+        B.solve(100000, TOL)
+        torch.cuda.synchronize()
+        o0 = torch.cuda.Event(enable_timing=True)
+        o1 = torch.cuda.Event(enable_timing=True)
+        o0.record(work_stream)
+        for _ in range(2):
+            B.solve(100000, TOL)
+        o1.record(work_stream)
+        torch.cuda.synchronize()
+        _, it_o, res_o = B.results()
+        other = {"inner_bits": ob, "ms_per_step": o0.elapsed_time(o1) / 2,
+                 "solves_per_s": 2 * B.nprob / (o0.elapsed_time(o1) / 1e3),
+                 "iterations_mean": float(np.abs(it_o).mean()), "worst_true_rel_residual":
+                 float(res_o.max())}
+        B.set_precision(args.batch_bits)
+
     # the plain form: one problem after another through the single-problem
     # API (assembly + FP64 CG + DIAG per problem)
     plain = None
@@ -702,14 +730,16 @@ def run_batch(args):
             dist.destroy_process_group()
         return 0
     peak, peak_kind = measured_peaks()
-    nbytes = batch_bytes(info, iters)
+    nbytes = batch_bytes(info, iters, bits=args.batch_bits)
     achieved = nbytes / (ms / args.steps * 1e-3) / 1e9
     cpu = cpu_baseline_batch(sizes, iters, info) if world == 1 else None
     line = {
         "metric": METRIC_BATCH, "value": world * args.steps * B.nprob / (ms / 1e3),
         "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "vs_baseline": None,
+        "dtype": "f64" if args.batch_bits == 64 else "f64 (assembly, refinement, true residual, "
+                 "dots) / f32 (inner CG)", "data": "synthetic",
         "config": {"workload": "%d independent 2-D P1 diffusion problems, nodes log-uniform in "
                                "[1e3, 6.4e4] (%d nodes, %d unknowns, %d nonzeros in all), "
                                "jittered meshes, own lognormal k (sigma 1) and f each; assembly "
@@ -731,6 +761,7 @@ def run_batch(args):
                      "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
                      "bytes_per_launch": nbytes, "avg_launch_us": ms / args.steps * 1e3},
         "plain": plain,
+        "other_precision": other,
         "cpu_baseline": cpu,
         "clocks": clk,
     }

@@ -317,6 +317,10 @@ int ofg_batch_get_matrix(const ofg_batch* B, int prob, double* values, double* r
  * the whole cluster. */
 int ofg_batch_tune(ofg_batch* B, int max_it, double toler, int* chosen, float* times_ms);
 int ofg_batch_set_config(ofg_batch* B, int config, int blocks_per_sm);
+/* Inner precision: 64 (default) = CG + DIAG in FP64; 32 = CG + DIAG in FP32
+ * (FP32 values, 16-bit column offsets where they fit) inside FP64 iterative
+ * refinement, with the same FP64 true-residual test. */
+int ofg_batch_set_precision(ofg_batch* B, int bits);
 int ofg_batch_config_shape(int config, int* threads, int* lanes_per_row, int* cluster);
 
 #ifdef __cplusplus

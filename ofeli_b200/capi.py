@@ -91,6 +91,7 @@ SIGNATURES = {
     "ofg_batch_get_matrix": (_i32, [_p, _i32, _p, _p]),
     "ofg_batch_tune": (_i32, [_p, _i32, _d, _pi32, _p]),
     "ofg_batch_set_config": (_i32, [_p, _i32, _i32]),
+    "ofg_batch_set_precision": (_i32, [_p, _i32]),
     "ofg_batch_config_shape": (_i32, [_i32, _pi32, _pi32, _pi32]),
 }
 

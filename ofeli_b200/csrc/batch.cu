@@ -76,6 +76,12 @@ struct BatchArgs {
    int* bad;
    int max_it;
    double tol;
+   // mixed precision: FP32 values, 16-bit column offsets (or int32 columns
+   // where an offset does not fit), FP32 inner vectors
+   int mixed, offsets16;
+   float* val32;
+   const int16_t* d16;
+   float *rl, *pl, *ql, *dl, *dinv32;
 };
 
 // sums NV values over the block; every thread receives the totals (fixed
@@ -202,6 +208,144 @@ __device__ __forceinline__ void block_spmv(int r0, int r1, const int32_t* rp, co
    }
 }
 
+// q = A p over rows [r0, r1) with FP32 values and FP32 vectors, columns as
+// 16-bit offsets from the row (d16) or absolute (col); adds this thread's
+// share of (p, q) to pq
+template <int THREADS, int LPR>
+__device__ __forceinline__ void block_spmv32(int r0, int r1, const int32_t* rp, const int16_t* d16,
+                                             const int32_t* col, const float* val, const float* x,
+                                             float* y, double& pq)
+{
+   const int lane = threadIdx.x % LPR;
+   for (int i0 = r0; i0 < r1; i0 += THREADS / LPR) {
+      const int i = i0 + (int)threadIdx.x / LPR;
+      float s = 0.f;
+      if (i < r1) {
+         if (d16)
+            for (int k = rp[i] + lane; k < rp[i + 1]; k += LPR) s += val[k] * x[i + d16[k]];
+         else
+            for (int k = rp[i] + lane; k < rp[i + 1]; k += LPR) s += val[k] * x[col[k]];
+      }
+#pragma unroll
+      for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, LPR);
+      if (i < r1 && lane == 0) {
+         y[i] = s;
+         pq += (double)x[i] * (double)s;
+      }
+   }
+}
+
+// CG + DIAG in FP32 inside FP64 refinement (the reliable-update form of the
+// single-problem mixed solver): one FP32 recurrence; whenever its residual
+// has fallen by 20x since the last refinement, or says the target is
+// reached, x += d in FP64, r = b - A x with the FP64 values, r_lo = (float) r,
+// and the recurrence continues with its direction kept.  Dot products are
+// accumulated in FP64; convergence is declared on the FP64 true residual.
+template <int THREADS, int LPR>
+__device__ void cg_mixed(const BatchArgs& a, const BatchProblem& P, Team<THREADS>& T, int r0,
+                         int r1, int& it_out, double& res_out, bool& done_out)
+{
+   const int tid = threadIdx.x;
+   const int32_t* rp = a.row_ptr + P.rp_off;
+   const int32_t* col = a.col + P.nnz_off;
+   const double* val = a.val + P.nnz_off;
+   const float* v32 = a.val32 + P.nnz_off;
+   const int16_t* d16 = a.offsets16 ? a.d16 + P.nnz_off : nullptr;
+   const double* b = a.b + P.row_off;
+   double* x = a.x + P.row_off;
+   double* r = a.r + P.row_off;
+   float* rl = a.rl + P.row_off;
+   float* pl = a.pl + P.row_off;
+   float* ql = a.ql + P.row_off;
+   float* dl = a.dl + P.row_off;
+   float* m32 = a.dinv32 + P.row_off;
+   double v[3] = {0.0, 0.0, 0.0};
+   for (int i = r0 + tid; i < r1; i += THREADS) {
+      const double bi = b[i];
+      const float ri = (float)bi, mi = (float)(1.0 / val[a.dpos[P.row_off + i]]);
+      const float zi = mi * ri;
+      m32[i] = mi;
+      x[i] = 0.0;
+      r[i] = bi;
+      rl[i] = ri;
+      dl[i] = 0.f;
+      pl[i] = zi;
+      v[0] += bi * bi;
+      v[1] += (double)ri * (double)zi;
+      v[2] += (double)ri * (double)ri;
+   }
+   T.sum(v);
+   double bnorm = sqrt(v[0]);
+   if (bnorm == 0.0) bnorm = 1.0;
+   double rho = v[1], rmark = sqrt(v[2]);
+   double res = sqrt(v[0]) / bnorm;
+   int it = 0;
+   bool done = res <= a.tol;
+   while (!done && it < a.max_it) {
+      ++it;
+      double w1[1] = {0.0};
+      block_spmv32<THREADS, LPR>(r0, r1, rp, d16, col, v32, pl, ql, w1[0]);
+      T.sum(w1);
+      const float alpha = (float)(rho / w1[0]);
+      double u2[2] = {0.0, 0.0};
+      for (int i = r0 + tid; i < r1; i += THREADS) {
+         dl[i] += alpha * pl[i];
+         const float ri = rl[i] - alpha * ql[i];
+         rl[i] = ri;
+         u2[0] += (double)ri * ri;
+         u2[1] += (double)ri * (ri * m32[i]);
+      }
+      T.sum(u2);
+      const double rn = sqrt(u2[0]);
+      double rz = u2[1];
+      if (rn <= 0.05 * rmark || rn <= a.tol * bnorm) {
+         // refinement in FP64
+         for (int i = r0 + tid; i < r1; i += THREADS) {
+            x[i] += (double)dl[i];
+            dl[i] = 0.f;
+         }
+         T.bar();
+         double w2[1] = {0.0}, d2 = 0.0;
+         block_spmv<THREADS, LPR>(r0, r1, rp, col, val, x, nullptr, nullptr, d2, b, r, w2[0]);
+         T.sum(w2);
+         res = sqrt(w2[0]) / bnorm;
+         if (res <= a.tol) {
+            done = true;
+            break;
+         }
+         double u3[2] = {0.0, 0.0};
+         for (int i = r0 + tid; i < r1; i += THREADS) {
+            const float ri = (float)r[i];
+            rl[i] = ri;
+            u3[0] += (double)ri * (ri * m32[i]);
+            u3[1] += (double)ri * ri;
+         }
+         T.sum(u3);
+         rz = u3[0];
+         rmark = sqrt(u3[1]);
+      }
+      const float beta = (float)(rz / rho);
+      rho = rz;
+      for (int i = r0 + tid; i < r1; i += THREADS) pl[i] = m32[i] * rl[i] + beta * pl[i];
+      T.bar();
+   }
+   if (!done && it > 0) {
+      // ran out: fold the correction in and report the true residual
+      for (int i = r0 + tid; i < r1; i += THREADS) {
+         x[i] += (double)dl[i];
+         dl[i] = 0.f;
+      }
+      T.bar();
+      double w2[1] = {0.0}, d2 = 0.0;
+      block_spmv<THREADS, LPR>(r0, r1, rp, col, val, x, nullptr, nullptr, d2, b, r, w2[0]);
+      T.sum(w2);
+      res = sqrt(w2[0]) / bnorm;
+   }
+   it_out = it;
+   res_out = res;
+   done_out = done;
+}
+
 // One problem: build(), CG + DIAG with the true-residual check, insertBC.
 template <int NEN, int THREADS, int LPR>
 __device__ void solve_problem(const BatchArgs& a, int pid, Team<THREADS>& T)
@@ -272,70 +416,79 @@ __device__ void solve_problem(const BatchArgs& a, int pid, Team<THREADS>& T)
       T.bar();
    }
 
-   // ---- CG with the diagonal preconditioner (FP64)
-   double v[2] = {0.0, 0.0};
-   for (int i = r0 + tid; i < r1; i += THREADS) {
-      const double d = 1.0 / val[a.dpos[P.row_off + i]];
-      const double bi = b[i], zi = d * bi;
-      dinv[i] = d;
-      x[i] = 0.0;
-      r[i] = bi;
-      p[i] = zi;
-      v[0] += bi * bi;
-      v[1] += bi * zi;
-   }
-   T.sum(v);
-   double bnorm = sqrt(v[0]);
-   if (bnorm == 0.0) bnorm = 1.0;
-   double rho = v[1];
-   double res = sqrt(v[0]) / bnorm;
    int it = 0;
-   bool done = res <= a.tol;
-   while (!done && it < a.max_it) {
-      ++it;
-      double w1[1] = {0.0}, dummy = 0.0;
-      block_spmv<THREADS, LPR>(r0, r1, rp, col, val, p, q, p, w1[0], nullptr, nullptr, dummy);
-      T.sum(w1);
-      const double alpha = rho / w1[0];
-      double u2[2] = {0.0, 0.0};
+   double res = 0.0;
+   bool done = false;
+   if (a.mixed) {
+      for (int64_t k = T.lo(nnz) + tid; k < T.hi(nnz); k += THREADS) a.val32[P.nnz_off + k] = (float)val[k];
+      T.bar();
+      cg_mixed<THREADS, LPR>(a, P, T, r0, r1, it, res, done);
+   }
+   else {
+      // ---- CG with the diagonal preconditioner (FP64)
+      double v[2] = {0.0, 0.0};
       for (int i = r0 + tid; i < r1; i += THREADS) {
-         x[i] += alpha * p[i];
-         const double ri = r[i] - alpha * q[i];
-         r[i] = ri;
-         u2[0] += ri * ri;
-         u2[1] += ri * (dinv[i] * ri);
+         const double d = 1.0 / val[a.dpos[P.row_off + i]];
+         const double bi = b[i], zi = d * bi;
+         dinv[i] = d;
+         x[i] = 0.0;
+         r[i] = bi;
+         p[i] = zi;
+         v[0] += bi * bi;
+         v[1] += bi * zi;
       }
-      T.sum(u2);
-      res = sqrt(u2[0]) / bnorm;
-      double rz = u2[1];
-      bool restart = false;
-      if (res <= a.tol) {
-         // FP64 true residual; r <- b - A x either way
+      T.sum(v);
+      double bnorm = sqrt(v[0]);
+      if (bnorm == 0.0) bnorm = 1.0;
+      double rho = v[1];
+      res = sqrt(v[0]) / bnorm;
+      done = res <= a.tol;
+      while (!done && it < a.max_it) {
+         ++it;
+         double w1[1] = {0.0}, dummy = 0.0;
+         block_spmv<THREADS, LPR>(r0, r1, rp, col, val, p, q, p, w1[0], nullptr, nullptr, dummy);
+         T.sum(w1);
+         const double alpha = rho / w1[0];
+         double u2[2] = {0.0, 0.0};
+         for (int i = r0 + tid; i < r1; i += THREADS) {
+            x[i] += alpha * p[i];
+            const double ri = r[i] - alpha * q[i];
+            r[i] = ri;
+            u2[0] += ri * ri;
+            u2[1] += ri * (dinv[i] * ri);
+         }
+         T.sum(u2);
+         res = sqrt(u2[0]) / bnorm;
+         double rz = u2[1];
+         bool restart = false;
+         if (res <= a.tol) {
+            // FP64 true residual; r <- b - A x either way
+            double w2[1] = {0.0}, d2 = 0.0;
+            block_spmv<THREADS, LPR>(r0, r1, rp, col, val, x, nullptr, nullptr, d2, b, r, w2[0]);
+            T.sum(w2);
+            res = sqrt(w2[0]) / bnorm;
+            if (res <= a.tol) {
+               done = true;
+               break;
+            }
+            restart = true;
+            double u3[1] = {0.0};
+            for (int i = r0 + tid; i < r1; i += THREADS) u3[0] += r[i] * (dinv[i] * r[i]);
+            T.sum(u3);
+            rz = u3[0];
+         }
+         const double beta = restart ? 0.0 : rz / rho;
+         rho = rz;
+         for (int i = r0 + tid; i < r1; i += THREADS) p[i] = dinv[i] * r[i] + beta * p[i];
+         T.bar();
+      }
+      if (!done && it > 0) {
+         // ran out: report the true residual
          double w2[1] = {0.0}, d2 = 0.0;
-         block_spmv<THREADS, LPR>(r0, r1, rp, col, val, x, nullptr, nullptr, d2, b, r, w2[0]);
+         block_spmv<THREADS, LPR>(r0, r1, rp, col, val, x, nullptr, nullptr, d2, b, q, w2[0]);
          T.sum(w2);
          res = sqrt(w2[0]) / bnorm;
-         if (res <= a.tol) {
-            done = true;
-            break;
-         }
-         restart = true;
-         double u3[1] = {0.0};
-         for (int i = r0 + tid; i < r1; i += THREADS) u3[0] += r[i] * (dinv[i] * r[i]);
-         T.sum(u3);
-         rz = u3[0];
       }
-      const double beta = restart ? 0.0 : rz / rho;
-      rho = rz;
-      for (int i = r0 + tid; i < r1; i += THREADS) p[i] = dinv[i] * r[i] + beta * p[i];
-      T.bar();
-   }
-   if (!done && it > 0) {
-      // ran out: report the true residual
-      double w2[1] = {0.0}, d2 = 0.0;
-      block_spmv<THREADS, LPR>(r0, r1, rp, col, val, x, nullptr, nullptr, d2, b, q, w2[0]);
-      T.sum(w2);
-      res = sqrt(w2[0]) / bnorm;
    }
    T.bar();
    // ---- insertBC into the nodal solution
@@ -389,6 +542,23 @@ __global__ void __launch_bounds__(THREADS) batch_kernel(BatchArgs a)
          solve_problem<NEN, THREADS, LPR>(a, a.order[w.first + rank], T);
       }
       __syncthreads();
+   }
+}
+
+// 16-bit column offsets (column - row, local numbering) of every problem;
+// one block per problem; flags an offset that does not fit
+__global__ void batch_offsets16(int nprob, const BatchProblem* probs, const int32_t* row_ptr,
+                                const int32_t* col, int16_t* d16, int* wide)
+{
+   for (int p = blockIdx.x; p < nprob; p += gridDim.x) {
+      const BatchProblem P = probs[p];
+      const int32_t* rp = row_ptr + P.rp_off;
+      for (int i = threadIdx.x; i < P.n; i += blockDim.x)
+         for (int32_t k = rp[i]; k < rp[i + 1]; ++k) {
+            const int d = col[P.nnz_off + k] - i;
+            if (d > 32767 || d < -32768) atomicOr(wide, 1);
+            d16[P.nnz_off + k] = (int16_t)d;
+         }
    }
 }
 
@@ -519,6 +689,10 @@ struct ofg_batch {
    int graph_config = -1;
    int max_it = 0;
    double tol = 0.0;
+   // mixed precision (bits 32): FP32 value copy, 16-bit offsets, FP32 vectors
+   int bits = 64, offsets16 = 0;
+   ofg::DBuf<float> val32, rl, pl, ql, dl, dinv32;
+   ofg::DBuf<int16_t> d16;
    ~ofg_batch()
    {
       if (exec) cudaGraphExecDestroy(exec);
@@ -565,6 +739,15 @@ BatchArgs args_of(ofg_batch* B)
    a.bad = B->bad.p;
    a.max_it = B->max_it;
    a.tol = B->tol;
+   a.mixed = B->bits == 32;
+   a.offsets16 = B->offsets16;
+   a.val32 = B->val32.p;
+   a.d16 = B->d16.p;
+   a.rl = B->rl.p;
+   a.pl = B->pl.p;
+   a.ql = B->ql.p;
+   a.dl = B->dl.p;
+   a.dinv32 = B->dinv32.p;
    return a;
 }
 
@@ -941,6 +1124,32 @@ int ofg_batch_tune(ofg_batch* B, int max_it, double toler, int* chosen, float* t
       B->items_config = -1;
       B->graph_config = -1;
       if (chosen) *chosen = best_c;
+   });
+}
+
+int ofg_batch_set_precision(ofg_batch* B, int bits)
+{
+   return guarded("ofg_batch_set_precision", [&] {
+      OFG_REQUIRE(B && (bits == 64 || bits == 32), OFG_ERR_ARG, "bits must be 64 or 32");
+      if (bits == 32 && !B->val32.p) {
+         B->val32.alloc(B->nnz);
+         for (auto* v : {&B->rl, &B->pl, &B->ql, &B->dl, &B->dinv32}) v->alloc(B->nrows);
+         B->d16.alloc(B->nnz);
+         DBuf<int> wide(1);
+         wide.zero();
+         batch_offsets16<<<std::min(B->nprob, num_sms() * 4), 256, 0, stream()>>>(
+            B->nprob, B->d_probs.p, B->row_ptr.p, B->col.p, B->d16.p, wide.p);
+         count_launch();
+         OFG_LAUNCH_CHECK();
+         int h = 0;
+         wide.download(&h, 1);
+         B->offsets16 = h ? 0 : 1;
+         if (!B->offsets16) B->d16.release();
+      }
+      if (B->bits != bits) {
+         B->bits = bits;
+         B->graph_config = -1;
+      }
    });
 }
 

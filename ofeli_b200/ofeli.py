@@ -444,6 +444,10 @@ class Batch:
         _call("ofg_batch_tune", self._h, max_it, toler, ctypes.byref(c), _ptr(t))
         return c.value, t
 
+    def set_precision(self, bits):
+        """64: FP64 CG; 32: FP32 CG inside FP64 refinement (same FP64 target)."""
+        _call("ofg_batch_set_precision", self._h, int(bits))
+
     def set_config(self, config, blocks_per_sm=0):
         _call("ofg_batch_set_config", self._h, config, blocks_per_sm)
 

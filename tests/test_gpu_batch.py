@@ -131,3 +131,39 @@ def test_clusters_mix_shared_and_per_block_problems(cuda):
         check_against_oracle(B, ref, matrices=False)
     a, b = B.matrix(0, ref[0]["nnz"], ref[0]["n"])
     assert rel_err(a, ref[0]["a"]) <= 1e-14 and rel_err(b, ref[0]["b"]) <= 1e-14
+
+
+def check_mixed(B, ref):
+    """FP32 inner CG inside FP64 refinement: the same FP64 target, the
+    oracle's FP64 solution up to the conditioning of each problem."""
+    u, it, res = B.results()
+    off = 0
+    for p, r in enumerate(ref):
+        up = u[off:off + r["u"].size]
+        off += r["u"].size
+        assert res[p] <= TOL and it[p] > 0, (p, res[p], it[p])
+        assert it[p] <= 2 * r["it"] + 20, (p, it[p], r["it"])
+        assert rel_err(up, r["u"]) <= 1e-7, p
+
+
+def test_mixed_precision_batch(cuda):
+    B, ref, _ = small_batch([4, 30, 9, 17, 2, 41, 12], seed=29)
+    B.set_precision(32)
+    B.solve(100000, TOL)
+    check_mixed(B, ref)
+    a, b = B.matrix(5, ref[5]["nnz"], ref[5]["n"])
+    assert rel_err(a, ref[5]["a"]) <= 1e-14 and rel_err(b, ref[5]["b"]) <= 1e-14
+    B.set_precision(64)
+    B.solve(100000, TOL)
+    check_against_oracle(B, ref, matrices=False)
+
+
+def test_mixed_precision_batch_with_clusters(cuda):
+    rng = np.random.default_rng(7)
+    sizes = [44, 37] + list(rng.integers(2, 7, size=200))
+    B, ref, _ = small_batch(sizes, seed=31, bc=True)
+    B.set_precision(32)
+    for c in (0, 4, 6, 12, 16):
+        B.set_config(c, blocks_per_sm=1)
+        B.solve(100000, TOL)
+        check_mixed(B, ref)
