@@ -85,10 +85,13 @@ struct BatchArgs {
 };
 
 // sums NV values over the block; every thread receives the totals (fixed
-// order: warps in index order)
+// order: a shuffle tree within each warp, then the same tree over the warp
+// sums in the first warp, whose result is broadcast through shared memory)
 template <int NV, int THREADS>
 __device__ __forceinline__ void block_sum(double (&v)[NV], double (*sh)[THREADS / 32])
 {
+   constexpr int NW = THREADS / 32;
+   __shared__ double tot[NV];
    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
    for (int i = 0; i < NV; ++i) {
@@ -96,14 +99,16 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double (*sh)[THREADS 
       if (lane == 0) sh[i][w] = s;
    }
    __syncthreads();
+   if (w == 0) {
 #pragma unroll
-   for (int i = 0; i < NV; ++i) {
-      double s = 0.0;
-#pragma unroll
-      for (int k = 0; k < THREADS / 32; ++k) s += sh[i][k];
-      v[i] = s;
+      for (int i = 0; i < NV; ++i) {
+         double s = warp_sum(lane < NW ? sh[i][lane] : 0.0);
+         if (lane == 0) tot[i] = s;
+      }
    }
    __syncthreads();
+#pragma unroll
+   for (int i = 0; i < NV; ++i) v[i] = tot[i];
 }
 
 // ---- thread-block clusters: rank, barrier, distributed shared memory loads
