@@ -512,7 +512,7 @@ __device__ void solve_problem(const BatchArgs& a, int pid, Team<THREADS>& T)
 // problems (one per block of the cluster) or one large problem that the
 // whole cluster solves together.
 template <int NEN, int THREADS, int LPR, int CS>
-__global__ void __launch_bounds__(THREADS) batch_kernel(BatchArgs a)
+__global__ void __launch_bounds__(THREADS, 2048 / THREADS) batch_kernel(BatchArgs a)
 {
    __shared__ int s_item;
    __shared__ double sh[3][THREADS / 32];
