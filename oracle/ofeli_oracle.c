@@ -490,6 +490,61 @@ done:
    return ret;
 }
 
+/* BiCGStab(A, P, b, x, max_it, toler), include/solvers/BiCGStab.h:87-161:
+ * the same vector operations in the same order (p = r + beta*(p - omega*v),
+ * x += (alpha*pp + omega*ss)), serial dot products; returns the iteration
+ * count, 2 when (rr, r) vanishes, 3 when omega vanishes, -(max_it+1) when
+ * the loop runs out. */
+int or_bicgstab(int64_t n, const int64_t* row_ptr, const int64_t* col_ind, const double* a,
+                int prec, const double* b, double* x, int max_it, double tol)
+{
+   size_t sz = sizeof(double) * (size_t)(n > 0 ? n : 1);
+   int64_t* id = (int64_t*)malloc(sizeof(int64_t) * (size_t)(n > 0 ? n : 1));
+   double *pivot = (double*)malloc(sz), *p = (double*)malloc(sz), *pp = (double*)malloc(sz),
+          *s = (double*)malloc(sz), *ss = (double*)malloc(sz), *t = (double*)malloc(sz),
+          *v = (double*)malloc(sz), *r = (double*)malloc(sz), *rr = (double*)malloc(sz);
+   int ret;
+   if (or_prec_setup(prec, n, row_ptr, col_ind, a, id, pivot) < 0) { ret = -(1 << 30); goto done; }
+   double rho_1 = 0, rho_2 = 0, alpha = 0, beta = 0, omega = 0, res, nrm = norm2(n, b);
+   or_spmv(n, row_ptr, col_ind, a, x, v);
+   for (int64_t i = 0; i < n; ++i) r[i] = b[i] - v[i];
+   memcpy(rr, r, sz);
+   if (nrm == 0.0) nrm = 1;
+   if ((res = norm2(n, r) / nrm) <= tol) { ret = 0; goto done; }
+   int it;
+   for (it = 1; it <= max_it; it++) {
+      rho_1 = dot(n, rr, r);
+      if (rho_1 == 0.0) { ret = 2; goto done; }
+      if (it == 1)
+         memcpy(p, r, sz);
+      else {
+         beta = (rho_1 / rho_2) * (alpha / omega);
+         for (int64_t i = 0; i < n; ++i) p[i] = r[i] + beta * (p[i] - omega * v[i]);
+      }
+      or_prec_apply(prec, n, row_ptr, col_ind, a, id, pivot, p, pp);
+      or_spmv(n, row_ptr, col_ind, a, pp, v);
+      alpha = rho_1 / dot(n, rr, v);
+      for (int64_t i = 0; i < n; ++i) s[i] = r[i] - alpha * v[i];
+      if ((res = norm2(n, s) / nrm) < tol) {
+         for (int64_t i = 0; i < n; ++i) x[i] += alpha * pp[i];
+         ret = it;
+         goto done;
+      }
+      or_prec_apply(prec, n, row_ptr, col_ind, a, id, pivot, s, ss);
+      or_spmv(n, row_ptr, col_ind, a, ss, t);
+      omega = dot(n, t, s) / dot(n, t, t);
+      for (int64_t i = 0; i < n; ++i) x[i] += alpha * pp[i] + omega * ss[i];
+      for (int64_t i = 0; i < n; ++i) r[i] = s[i] - omega * t[i];
+      rho_2 = rho_1;
+      if ((res = norm2(n, r) / nrm) < tol) { ret = it; goto done; }
+      if (omega == 0.0) { ret = 3; goto done; }
+   }
+   ret = -it;
+done:
+   free(id); free(pivot); free(p); free(pp); free(s); free(ss); free(t); free(v); free(r); free(rr);
+   return ret;
+}
+
 /* GMRes helpers rotate / set_rotation / update, include/solvers/GMRes.h:67-115 */
 static void rotate(double* dx, double* dy, double cs, double sn)
 {

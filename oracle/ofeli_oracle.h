@@ -60,6 +60,8 @@ void or_prec_apply(int type, int64_t n, const int64_t* row_ptr, const int64_t* c
 int or_cg(int64_t n, const int64_t* row_ptr, const int64_t* col_ind, const double* a, int prec,
           const double* b, double* x, int max_it, double tol, double* hist);
 /* a17: GMRes(A,P,b,x,m,max_it,tol), GMRes.h:67-241 */
+int or_bicgstab(int64_t n, const int64_t* row_ptr, const int64_t* col_ind, const double* a,
+                int prec, const double* b, double* x, int max_it, double tol);
 int or_gmres(int64_t n, const int64_t* row_ptr, const int64_t* col_ind, const double* a, int prec,
              const double* b, double* x, int m, int max_it, double tol);
 /* a21: Vect::insertBC, Vect_impl.h:1098-1130 */

@@ -63,6 +63,9 @@ def lib():
         L.or_gmres.argtypes = [_i64, _p, _p, _p, ctypes.c_int, _p, _p, ctypes.c_int,
                                ctypes.c_int, ctypes.c_double]
         L.or_gmres.restype = ctypes.c_int
+        L.or_bicgstab.argtypes = [_i64, _p, _p, _p, ctypes.c_int, _p, _p, ctypes.c_int,
+                                  ctypes.c_double]
+        L.or_bicgstab.restype = ctypes.c_int
         L.or_insert_bc.argtypes = [_i64, _p, _p, _p, _p]
         _lib = L
     return _lib
@@ -158,6 +161,13 @@ def cg(rp, ci, a, b, ptype, max_it, tol, x0=None, history=False):
     it = lib().or_cg(n, _ptr(rp), _ptr(ci), _ptr(a), ptype, _ptr(b), _ptr(x), max_it, tol,
                      _ptr(hist))
     return (x, it, hist) if history else (x, it)
+
+
+def bicgstab(rp, ci, a, b, ptype, max_it, tol, x0=None):
+    n = rp.size - 1
+    x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64)
+    it = lib().or_bicgstab(n, _ptr(rp), _ptr(ci), _ptr(a), ptype, _ptr(b), _ptr(x), max_it, tol)
+    return x, it
 
 
 def gmres(rp, ci, a, b, ptype, m, max_it, tol, x0=None):

@@ -136,6 +136,8 @@ int solve_system(E& eq, SpMatrix<real_t>& A, Vect<real_t>& b, Vect<real_t>& x,
       size_t m = std::stoul(solver.substr(5));
       it = GMRes(A, P, b, x, m, maxit, tol);
    }
+   else if (solver == "BICGSTAB")
+      it = BiCGStab(A, P, b, x, maxit, tol);
    else {
       fprintf(stderr, "unknown solver %s\n", solver.c_str());
       exit(2);

@@ -128,6 +128,29 @@ def case_cd2d():
           "n": info["n"], "nnz": info["nnz"]})
 
 
+def case_bicgstab():
+    """OFELI's BiCGStab: the 65x65 Poisson system of case_p2d_65 with DIAG and
+    ILU, and the 17x17 convection-diffusion steps of case_cd2d with ILU."""
+    nx = 64
+    f = fields.uniform_pm1(1234, (nx + 1) ** 2)
+    arrays, meta = {}, {"nx": nx, "tol": 1e-10, "runs": {}}
+    for prec in ("DIAG", "ILU"):
+        info, out = O.run_reference(["p2d", nx, nx, "BICGSTAB", prec, 1e-10, 20000], {"f": f})
+        arrays["x_p2d_" + prec] = out["x"]
+        meta["runs"]["p2d_" + prec] = {"iters": info["iters"]}
+    nx2, steps, dt, eps = 16, 5, 1e-3, 1e-3
+    xy, elem, code = O.mesh2d(nx2, nx2)
+    P = xy.reshape(-1, 2)
+    u0 = np.exp(-((P[:, 0] - 0.3) ** 2 + (P[:, 1] - 0.5) ** 2) / (2 * 0.05 ** 2))
+    u0[code > 0] = 0.0
+    v = np.stack([-(P[:, 1] - 0.5), P[:, 0] - 0.5], axis=1).reshape(-1)
+    info, out = O.run_reference(["cd2d", nx2, nx2, steps, dt, eps, "BICGSTAB", "ILU", 1e-10, 2000],
+                                {"u0": u0, "v": v})
+    arrays.update(cd2d_u=out["u"], cd2d_iters=out["iters"])
+    meta["cd2d"] = {"nx": nx2, "steps": steps, "dt": dt, "eps": eps}
+    save("bicgstab", arrays, meta)
+
+
 if __name__ == "__main__":
     if not O.have_reference("o2"):
         raise SystemExit("build the reference first: make -C oracle ref")
@@ -136,3 +159,4 @@ if __name__ == "__main__":
     case_p2d_ragged()
     case_p3d()
     case_cd2d()
+    case_bicgstab()

@@ -139,3 +139,38 @@ def test_dilu_is_not_ilu0():
     r = fields.uniform_pm1(3, n)
     z = O.prec_apply(O.ILU, rp, ci, a, idv, piv, r)
     assert np.abs(M @ z - r).max() <= 1e-12 * np.abs(r).max()
+
+
+@pytest.mark.parametrize("prec", ["DIAG", "ILU"])
+def test_bicgstab_p2d_bit_exact(prec):
+    """OFELI's BiCGStab (include/solvers/BiCGStab.h) on the 65x65 system."""
+    g, _ = load_golden("p2d_65")
+    z, info = load_golden("bicgstab")
+    rp, ci, a, b = (g["row_ptr"].astype(np.int64), g["col_ind"].astype(np.int64), g["a"], g["b"])
+    x, it = O.bicgstab(rp, ci, a, b, PREC[prec], 20000, 1e-10)
+    assert it == info["runs"]["p2d_" + prec]["iters"]
+    assert np.array_equal(x, z["x_p2d_" + prec])
+
+
+def test_bicgstab_cd2d_bit_exact():
+    """Five backward-Euler DC2DT3 steps solved by BiCGStab + ILU with the
+    previous step as the initial guess, as OFELI runs them."""
+    z, info = load_golden("bicgstab")
+    c = info["cd2d"]
+    nx, dt, eps = c["nx"], c["dt"], c["eps"]
+    xy, elem, code = O.mesh2d(nx, nx)
+    P = xy.reshape(-1, 2)
+    u = np.exp(-((P[:, 0] - 0.3) ** 2 + (P[:, 1] - 0.5) ** 2) / (2 * 0.05 ** 2))
+    u[code > 0] = 0.0
+    v = np.stack([-(P[:, 1] - 0.5), P[:, 0] - 0.5], axis=1).reshape(-1)
+    dof, n = O.number_equations(code)
+    rp, ci = O.node_graph(elem, 3, dof, n)
+    x = np.zeros(n)
+    its = []
+    for s in range(c["steps"]):
+        a, b = O.assemble_cd2d(xy, elem, dof, code, n, rp, ci, eps, v, dt, u, bc=np.zeros(code.size))
+        x, it = O.bicgstab(rp, ci, a, b, O.ILU, 2000, 1e-10, x0=x)
+        its.append(it)
+        u = O.insert_bc(code, x)
+    assert its == list(z["cd2d_iters"])
+    assert np.array_equal(u, z["cd2d_u"])
