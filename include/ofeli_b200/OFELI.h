@@ -9,7 +9,8 @@
 //   SpMatrix<real_t>                     include/linear_algebra/SpMatrix.h:78-611
 //   Vect<real_t> (std::vector subclass)  include/linear_algebra/Vect.h:138
 //   Prec<real_t>                         include/solvers/Prec.h:73-176
-//   CG, GMRes                            include/solvers/CG.h:99-213, GMRes.h:148-298
+//   CG, GMRes, BiCGStab                  include/solvers/CG.h:99-213, GMRes.h:148-298,
+//                                        BiCGStab.h:87-161
 //   LinearSolver                         include/solvers/LinearSolver.h:68-273
 //   Laplace2DT3, Laplace3DT4/DC3DT4,     src/equations/laplace/Laplace2DT3.cpp,
 //   DC2DT3: build(), run()               src/equations/therm/DC3DT4.cpp, DC2DT3.cpp
@@ -322,6 +323,26 @@ inline int GMRes(const SpMatrix<real_t>& A, int prec, const Vect<real_t>& b, Vec
    return GMRes(A, P, b, x, m, max_it, toler);
 }
 
+// BiCGStab (include/solvers/BiCGStab.h:87-161): iterations; 2 or 3 on a
+// breakdown; -(max_it+1) when the loop runs out.
+inline int BiCGStab(const SpMatrix<real_t>& A, const Prec<real_t>& P, const Vect<real_t>& b,
+                    Vect<real_t>& x, int max_it, real_t toler)
+{
+   (void)A;
+   x.resize(b.size());
+   int it = 0;
+   ofg_check(ofg_bicgstab(P.handle(), b.data(), x.data(), max_it, toler, &it, nullptr),
+             "BiCGStab");
+   return it;
+}
+
+inline int BiCGStab(const SpMatrix<real_t>& A, int prec, const Vect<real_t>& b, Vect<real_t>& x,
+                    int max_it, real_t toler)
+{
+   Prec<real_t> P(A, prec);
+   return BiCGStab(A, P, b, x, max_it, toler);
+}
+
 // -------------------------------------------------------- LinearSolver ----
 class LinearSolver {
  public:
@@ -350,6 +371,8 @@ class LinearSolver {
          size_t m = _b->size() / 5;
          _nb_it = GMRes(*_A, _p, *_b, *_x, m ? m : 1, _max_it, _toler);
       }
+      else if (_s == BICG_STAB_SOLVER)
+         _nb_it = BiCGStab(*_A, _p, *_b, *_x, _max_it, _toler);
       else
          throw OFELIException("LinearSolver: solver outside the GPU path");
       return _nb_it < 0 ? -_nb_it : 0;

@@ -188,6 +188,11 @@ int ofg_cg_history(ofg_prec* P, const double* b, double* x, int max_it, double t
  * (left preconditioned, modified Gram-Schmidt, Givens rotations). */
 int ofg_gmres(ofg_prec* P, const double* b, double* x, int m, int max_it, double toler,
               int* result, double* res);
+/* BiCGStab(A, P, b, x, max_it, toler) -- include/solvers/BiCGStab.h:87-161:
+ * OFELI's return convention (iterations; 2 when (rr, r) vanishes; 3 when
+ * omega vanishes; -(max_it+1) when the loop runs out). */
+int ofg_bicgstab(ofg_prec* P, const double* b, double* x, int max_it, double toler, int* result,
+                 double* res);
 /* Mixed-precision solve: FP64 iterative refinement whose correction is
  * computed by Jacobi-preconditioned CG in FP32 (inner_bits 32) or with BF16
  * matrix values and FP32 vectors (inner_bits 16); FP64 only for b - A x,

@@ -65,6 +65,7 @@ SIGNATURES = {
     "ofg_cg": (_i32, [_p, _p, _p, _i32, _d, _pi32, _pd]),
     "ofg_cg_history": (_i32, [_p, _p, _p, _i32, _d, _pi32, _pd, _p]),
     "ofg_gmres": (_i32, [_p, _p, _p, _i32, _i32, _d, _pi32, _pd]),
+    "ofg_bicgstab": (_i32, [_p, _p, _p, _i32, _d, _pi32, _pd]),
     "ofg_solve_mixed": (_i32, [_p, _i32, _i32, _i32, _p, _p, _i32, _i32, _d, _d, _pi32, _pi32,
                                _pd]),
     "ofg_residual": (_i32, [_p, _p, _p, _pd]),

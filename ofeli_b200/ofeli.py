@@ -269,6 +269,18 @@ def GMRes(A, P, b, x, m, max_it, toler):
     return res.value
 
 
+def BiCGStab(A, P, b, x, max_it, toler):
+    """BiCGStab(A, P|prec, b, x, max_it, toler) -> iterations; 2 or 3 on a
+    breakdown ((rr, r) or omega vanishing); -(max_it+1) when max_it ran out."""
+    P = _as_prec(A, P)
+    b = _f64(b, A.n)
+    res = ctypes.c_int()
+    rr = ctypes.c_double()
+    _call("ofg_bicgstab", P._h, _ptr(b), _ptr(x), max_it, toler, ctypes.byref(res),
+          ctypes.byref(rr))
+    return res.value
+
+
 def solve_mixed(A, b, x, prec=DIAG_PREC, inner_bits=32, toler=1e-10, max_outer=200,
                 max_inner=1000000, inner_tol=0.05, mode=0):
     """FP64 iterative refinement around an FP32 (or BF16-matrix) PCG; mode 0
@@ -512,6 +524,9 @@ class LinearSolver:
         elif self._s == GMRES_SOLVER:
             self._nb_it = GMRes(self._A, self._p, self._b, self._x, max(1, self._A.n // 5),
                                 self._max_it, self._toler)
+        elif self._s == BICG_STAB_SOLVER:
+            self._nb_it = BiCGStab(self._A, self._p, self._b, self._x, self._max_it,
+                                   self._toler)
         else:
             raise OFELIException("solver %d is outside the GPU path" % self._s)
         return -self._nb_it if self._nb_it < 0 else 0
@@ -616,8 +631,13 @@ class DC2DT3:
               _ptr(self.u), _ptr(self._bc), _ptr(self._b))
         return self._A, self._b
 
-    def step(self, prec=ILU_PREC, m=30, max_it=1000, toler=1e-10):
+    def step(self, prec=ILU_PREC, m=30, max_it=1000, toler=1e-10, solver=GMRES_SOLVER):
+        """One time step; the solver is GMRes(m) (default) or BiCGStab
+        (BICG_STAB_SOLVER, OFELI's default for convection)."""
         self.build()
-        it = GMRes(self._A, Prec(self._A, prec), self._b, self.x, m, max_it, toler)
+        if solver == BICG_STAB_SOLVER:
+            it = BiCGStab(self._A, Prec(self._A, prec), self._b, self.x, max_it, toler)
+        else:
+            it = GMRes(self._A, Prec(self._A, prec), self._b, self.x, m, max_it, toler)
         _call("ofg_insert_bc", self.mesh._h, _ptr(self.x), _ptr(self._bc), _ptr(self.u))
         return it

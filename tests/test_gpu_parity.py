@@ -289,3 +289,58 @@ def test_mixed_precision_column_offset_formats(cuda, permute):
     outer, inner, res = F.solve_mixed(A, b, x, prec=F.DIAG_PREC, toler=1e-10)
     assert res <= 1e-10 and F.residual(A, b, x) <= 1e-10
     assert rel_err(x, xref) <= 1e-6
+
+
+@pytest.mark.parametrize("prec", ["DIAG", "ILU"])
+def test_bicgstab_matches_reference(cuda, prec):
+    """BiCGStab on the 65x65 system against OFELI's own run (golden
+    bicgstab.npz): iteration count within the band, same solution."""
+    g, _ = load_golden("p2d_65")
+    z, info = load_golden("bicgstab")
+    A = F.SpMatrix(g["row_ptr"], g["col_ind"], g["a"])
+    x = np.zeros(A.n)
+    it = F.BiCGStab(A, F.Prec(A, PRECS[prec]), g["b"], x, 20000, 1e-10)
+    assert it > 0 and abs(it - info["runs"]["p2d_" + prec]["iters"]) <= IT_TOL
+    # BiCGStab amplifies the different summation order of the parallel dot
+    # products more than CG does: both solutions have residual <= 1e-10 and
+    # agree to 1e-8 (the conditioning bound here is ~2e-7)
+    assert rel_err(x, z["x_p2d_" + prec]) <= 1e-8
+    ls = F.LinearSolver(A, g["b"], np.zeros(A.n))
+    ls.setTolerance(1e-10)
+    ls.setMaxIter(20000)
+    assert ls.solve(F.BICG_STAB_SOLVER, PRECS[prec]) == 0
+    assert abs(ls.getNbIter() - it) <= IT_TOL
+
+
+def test_bicgstab_transient_steps_match_reference(cuda):
+    """Five DC2DT3 backward-Euler steps with BiCGStab + ILU and warm starts,
+    as OFELI runs them (golden bicgstab.npz)."""
+    z, info = load_golden("bicgstab")
+    c = info["cd2d"]
+    nx = c["nx"]
+    mesh = F.Mesh(0.0, 1.0, 0.0, 1.0, nx, nx, 1, 1, 1, 1)
+    xy, _, code, _ = mesh.arrays()
+    P = xy.reshape(-1, 2)
+    u0 = np.exp(-((P[:, 0] - 0.3) ** 2 + (P[:, 1] - 0.5) ** 2) / (2 * 0.05 ** 2))
+    u0[code > 0] = 0.0
+    v = np.stack([-(P[:, 1] - 0.5), P[:, 0] - 0.5], axis=1).reshape(-1)
+    eq = F.DC2DT3(mesh, u0, v, c["eps"], c["dt"])
+    eq.setDirichlet(np.zeros(mesh.nn))
+    its = [eq.step(prec=F.ILU_PREC, max_it=2000, toler=1e-10, solver=F.BICG_STAB_SOLVER)
+           for _ in range(c["steps"])]
+    assert all(abs(a - b) <= IT_TOL for a, b in zip(its, z["cd2d_iters"]))
+    assert rel_err(eq.u, z["cd2d_u"]) <= 1e-8
+
+
+def test_bicgstab_edges(cuda):
+    g, _ = load_golden("p2d_65")
+    A = F.SpMatrix(g["row_ptr"], g["col_ind"], g["a"])
+    x = np.zeros(A.n)
+    assert F.BiCGStab(A, F.Prec(A, F.DIAG_PREC), np.zeros(A.n), x, 100, 1e-10) == 0
+    rp, ci = g["row_ptr"].astype(np.int64), g["col_ind"].astype(np.int64)
+    for pt in (O.IDENT, O.DIAG, O.SSOR):
+        x = np.zeros(A.n)
+        it = F.BiCGStab(A, F.Prec(A, pt), g["b"], x, 5, 1e-10)
+        xo, ito = O.bicgstab(rp, ci, g["a"], g["b"], pt, 5, 1e-10)
+        assert it == ito == -6
+        assert rel_err(x, xo) <= 1e-10
