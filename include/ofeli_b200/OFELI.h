@@ -108,18 +108,67 @@ class Mesh {
                 "Mesh");
       info();
    }
+   // Mesh(file, bc): a P1 mesh from OFELI's XML format (Mesh::get).  The
+   // equations are numbered over the code-0 nodes whatever bc is, as the P1
+   // equations' removeImposedDOF leaves them.
+   explicit Mesh(const std::string& file, bool bc = false)
+   {
+      (void)bc;
+      get(file);
+   }
+   // Mesh::get(file) -- src/mesh/Mesh.cpp:2639-2668
+   void get(const std::string& file)
+   {
+      ofg_mesh_file* f = nullptr;
+      ofg_check(ofg_mesh_file_read(file.c_str(), &f), "Mesh::get");
+      ofg_mesh* h = nullptr;
+      int rc = ofg_mesh_create_from_file(f, &h);
+      if (rc != OFG_OK) {
+         std::string msg = std::string("Mesh::get: ") + ofg_last_error();
+         ofg_mesh_file_destroy(f);
+         throw OFELIException(msg);
+      }
+      if (_h) ofg_mesh_destroy(_h);
+      if (_file) ofg_mesh_file_destroy(_file);
+      _h = h;
+      _file = f;
+      info();
+   }
+   // Mesh::put(file) -- src/mesh/Mesh.cpp:2731-2806
+   void put(const std::string& file) const
+   {
+      if (_file) {
+         ofg_check(ofg_mesh_file_write(_file, file.c_str()), "Mesh::put");
+         return;
+      }
+      ofg_mesh_file* f = nullptr;
+      ofg_check(ofg_mesh_file_from_mesh(_h, &f), "Mesh::put");
+      int rc = ofg_mesh_file_write(f, file.c_str());
+      std::string msg = rc != OFG_OK ? std::string("Mesh::put: ") + ofg_last_error() : "";
+      ofg_mesh_file_destroy(f);
+      if (rc != OFG_OK) throw OFELIException(msg);
+   }
+   // Mesh::save for the ".m" format
+   void save(const std::string& file) const
+   {
+      if (file.size() < 2 || file.compare(file.size() - 2, 2, ".m") != 0)
+         throw OFELIException("Mesh::save: only OFELI's .m format is written");
+      put(file);
+   }
    Mesh(const Mesh&) = delete;
    Mesh& operator=(const Mesh&) = delete;
    Mesh(Mesh&& o) noexcept { *this = std::move(o); }
    Mesh& operator=(Mesh&& o) noexcept
    {
       std::swap(_h, o._h);
+      std::swap(_file, o._file);
       _dim = o._dim; _nn = o._nn; _ne = o._ne; _neq = o._neq;
       return *this;
    }
    ~Mesh()
    {
       if (_h) ofg_mesh_destroy(_h);
+      if (_file) ofg_mesh_file_destroy(_file);
    }
    size_t getDim() const { return (size_t)_dim; }
    size_t getNbNodes() const { return (size_t)_nn; }
@@ -131,6 +180,7 @@ class Mesh {
    explicit Mesh(ofg_mesh* h) : _h(h) { info(); }
    void info() { ofg_check(ofg_mesh_info(_h, &_dim, &_nn, &_ne, &_neq, nullptr), "Mesh"); }
    ofg_mesh* _h = nullptr;
+   ofg_mesh_file* _file = nullptr;   // the file a mesh was read from, kept for put()
    int _dim = 0;
    int64_t _nn = 0, _ne = 0, _neq = 0;
 };

@@ -54,6 +54,7 @@ typedef struct ofg_mesh ofg_mesh;
 typedef struct ofg_prec ofg_prec;
 typedef struct ofg_learned ofg_learned;
 typedef struct ofg_batch ofg_batch;
+typedef struct ofg_mesh_file ofg_mesh_file;
 
 /* ---------------------------------------------------------------- runtime */
 const char* ofg_last_error(void);
@@ -123,7 +124,8 @@ int ofg_mesh_create_rect(double xmin, double xmax, double ymin, double ymax, int
 int ofg_mesh_create_kuhn(int64_t M, ofg_mesh** out);
 /* General P1 mesh (Mesh::Add of nodes and elements, include/mesh/Mesh.h:321-325):
  * dim 2 (triangles, nen 3) or 3 (tetrahedra, nen 4); elem holds 0-based node
- * indices; a node with code > 0 carries an imposed value and no equation. */
+ * indices; a node with a non-zero code carries an imposed value and no
+ * equation. */
 int ofg_mesh_create(int dim, int64_t nn, const double* coords, int64_t ne, const int32_t* elem,
                     const int32_t* code, ofg_mesh** out);
 int ofg_mesh_destroy(ofg_mesh* m);
@@ -158,6 +160,45 @@ int ofg_assemble_cd2d(ofg_mesh* m, ofg_matrix* A, double eps, const double* v, d
 /* Vect::insertBC (include/linear_algebra/Vect_impl.h:1098-1130): nodal
  * vector from the equation-space solution x and bc (may be NULL). */
 int ofg_insert_bc(const ofg_mesh* m, const double* x, const double* bc, double* u);
+
+/* ------------------------------------------------------ mesh files (.m) */
+/* OFELI's XML mesh format, read and written on the host (no GPU needed).
+ * An ofg_mesh_file holds what Mesh::get keeps of a file: nodes (dim
+ * coordinates, nb_dof codes each), elements (OFELI shape code -- LINE 2,
+ * TRIANGLE 3, QUADRILATERAL 4, TETRAHEDRON 5, ... -- node indices 0-based,
+ * one code each) and sides (node indices, nb_dof codes each).
+ *
+ * Mesh::get(file) -- src/mesh/Mesh.cpp:2639-2668 with XMLParser's mesh
+ * reading (src/io/XMLParser.cpp:1174-1217, 2211-2295): coordinates rounded
+ * to float as std::stof does, marks split per DOF by DOFCode
+ * (src/mesh/MeshUtil.cpp:101-116), nothing read after a Material tag.
+ * Converted by a team of host threads (ofg_mesh_file_set_threads). */
+int ofg_mesh_file_read(const char* path, ofg_mesh_file** out);
+/* Mesh::put(file) -- src/mesh/Mesh.cpp:2731-2806, byte for byte. */
+int ofg_mesh_file_write(const ofg_mesh_file* f, const char* path);
+/* A mesh file object from arrays (Mesh::Add of nodes, elements and sides,
+ * include/mesh/Mesh.h:321-330); sides and their codes may be NULL when ns = 0. */
+int ofg_mesh_file_create(int dim, int nb_dof, int64_t nn, const double* coords,
+                         const int32_t* node_code, int el_shape, int el_nodes, int64_t ne,
+                         const int32_t* elem, const int32_t* elem_code, int sd_shape, int sd_nodes,
+                         int64_t ns, const int32_t* sides, const int32_t* side_code,
+                         ofg_mesh_file** out);
+/* The file view of a device mesh (one DOF per node, element code 1), e.g.
+ * to put() a generated mesh; a structured rectangle gets the sides that
+ * OFELI's constructor adds for negative line codes. */
+int ofg_mesh_file_from_mesh(const ofg_mesh* m, ofg_mesh_file** out);
+int ofg_mesh_file_info(const ofg_mesh_file* f, int* dim, int* nb_dof, int64_t* nn, int* el_shape,
+                       int* el_nodes, int64_t* ne, int* sd_shape, int* sd_nodes, int64_t* ns);
+/* Copies any non-NULL array out (sizes from ofg_mesh_file_info). */
+int ofg_mesh_file_get(const ofg_mesh_file* f, double* coords, int32_t* node_code, int32_t* elem,
+                      int32_t* elem_code, int32_t* sides, int32_t* side_code);
+int ofg_mesh_file_destroy(ofg_mesh_file* f);
+/* Host threads used to read and write mesh files (0 = all hardware threads). */
+int ofg_mesh_file_set_threads(int n);
+/* The device mesh of a P1 mesh file (triangles in 2-D, tetrahedra in 3-D,
+ * nb_dof 1), as Mesh(file, true) would number it: equations on the nodes
+ * with code 0 (Mesh::NumberEquations, src/mesh/Mesh.cpp:1483-1510). */
+int ofg_mesh_create_from_file(const ofg_mesh_file* f, ofg_mesh** out);
 
 /* ------------------------------------------------------- preconditioners */
 /* Prec<real_t>(A, type) -- include/solvers/Prec_impl.h:164-195: DIAG

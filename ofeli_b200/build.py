@@ -14,7 +14,8 @@ CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libofeli_gpu.so")
 SOURCES = ["runtime.cu", "matrix.cu", "mesh.cu", "assembly.cu", "prec.cu", "krylov.cu", "mixed.cu",
-           "noalloc.cu", "learned.cu", "batch.cu", "bicgstab.cu"]
+           "noalloc.cu", "learned.cu", "batch.cu", "bicgstab.cu",
+           "meshio.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
          "-Xcompiler", "-fPIC", "-Xcompiler", "-O2", "--expt-relaxed-constexpr"]

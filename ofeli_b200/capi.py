@@ -57,6 +57,16 @@ SIGNATURES = {
     "ofg_assemble_p1": (_i32, [_p, _p, _p, _p, _p, _p]),
     "ofg_assemble_cd2d": (_i32, [_p, _p, _d, _p, _d, _p, _p, _p]),
     "ofg_insert_bc": (_i32, [_p, _p, _p, _p]),
+    "ofg_mesh_file_read": (_i32, [ctypes.c_char_p, _pp]),
+    "ofg_mesh_file_write": (_i32, [_p, ctypes.c_char_p]),
+    "ofg_mesh_file_create": (_i32, [_i32, _i32, _i64, _p, _p, _i32, _i32, _i64, _p, _p, _i32, _i32,
+                                    _i64, _p, _p, _pp]),
+    "ofg_mesh_file_from_mesh": (_i32, [_p, _pp]),
+    "ofg_mesh_file_info": (_i32, [_p, _pi32, _pi32, _pi64, _pi32, _pi32, _pi64, _pi32, _pi32, _pi64]),
+    "ofg_mesh_file_get": (_i32, [_p, _p, _p, _p, _p, _p, _p]),
+    "ofg_mesh_file_destroy": (_i32, [_p]),
+    "ofg_mesh_file_set_threads": (_i32, [_i32]),
+    "ofg_mesh_create_from_file": (_i32, [_p, _pp]),
     "ofg_prec_create": (_i32, [_p, _i32, _pp]),
     "ofg_prec_destroy": (_i32, [_p]),
     "ofg_prec_update": (_i32, [_p]),

@@ -55,6 +55,10 @@ struct ofg_mesh {
    // color_ptr[c+1]); no two elements of one colour share a node
    std::vector<int64_t> color_ptr;
    ofg::DBuf<int32_t> color_elems;
+   // the structured rectangle's cells and line codes (rect_nx < 0 otherwise),
+   // kept for the sides Mesh::put writes
+   int64_t rect_nx = -1, rect_ny = -1;
+   int rect_code[4] = {0, 0, 0, 0};   // cx0, cxN, cy0, cyN
 };
 
 namespace ofg {

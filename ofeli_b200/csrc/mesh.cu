@@ -340,6 +340,8 @@ int ofg_mesh_create_rect(double xmin, double xmax, double ymin, double ymax, int
          count_launch();
          OFG_LAUNCH_CHECK();
          finish_mesh(m);
+         m->rect_nx = nx, m->rect_ny = ny;
+         m->rect_code[0] = cx0, m->rect_code[1] = cxN, m->rect_code[2] = cy0, m->rect_code[3] = cyN;
       }
       catch (...) {
          delete m;

@@ -5,7 +5,9 @@ follow OFELI 5.3.3 (paths within that project):
 
 * ``Mesh(xmin, xmax, ymin, ymax, nx, ny, cx0, cxN, cy0, cyN)``: the structured
   triangulation of src/mesh/Mesh.cpp:547-676; ``Mesh.kuhn(M)`` the unit cube;
-  ``Mesh.from_arrays`` a general P1 mesh (Mesh::Add).
+  ``Mesh.from_arrays`` a general P1 mesh (Mesh::Add); ``Mesh.from_file`` /
+  ``get`` / ``put`` OFELI's XML mesh files (``MeshFile`` holds a file's
+  content on the host).
 * ``SpMatrix(mesh)`` / ``SpMatrix(row_ptr, col_ind[, a])``: CSR with OFELI's
   layout (0-based row_ptr, 1-based col_ind), include/linear_algebra/SpMatrix.h.
 * ``Prec(A, type)``, ``CG(A, P, b, x, max_it, toler)``,
@@ -121,10 +123,128 @@ class Mesh:
     def setCoords(self, coords):
         coords = _f64(coords, self.nn * self.dim)
         _call("ofg_mesh_set_coords", self._h, _ptr(coords))
+        self._coords_changed = True
+
+    @classmethod
+    def from_file(cls, path):
+        """Mesh(file, true): a P1 mesh read from OFELI's XML format, equations
+        on the code-0 nodes.  The file's data (sides, element codes) is kept
+        for put()."""
+        mf = MeshFile(path)
+        m = mf.to_mesh()
+        m._file = mf
+        return m
+
+    def get(self, path):
+        """Mesh::get(file) (src/mesh/Mesh.cpp:2639-2668): replaces this mesh."""
+        m = Mesh.from_file(path)
+        old = getattr(self, "_h", None)
+        self._h, m._h = m._h, old
+        self._file = m._file
+        self._coords_changed = False
+        self._info()
+
+    def put(self, path):
+        """Mesh::put(file) (src/mesh/Mesh.cpp:2731-2806)."""
+        mf = getattr(self, "_file", None)
+        if mf is None or getattr(self, "_coords_changed", False):
+            mf = MeshFile.from_mesh(self)
+        mf.put(path)
+
+    def save(self, path):
+        """Mesh::save for the ".m" format."""
+        if not str(path).endswith(".m"):
+            raise OFELIException("only OFELI's .m format is written")
+        self.put(path)
 
     def __del__(self):
         if getattr(self, "_h", None) and capi is not None and capi._lib is not None:
             capi.lib().ofg_mesh_destroy(self._h)
+            self._h = None
+
+
+# OFELI's element shape codes (include/OFELI_Config.h:274-282)
+POINT, LINE, TRIANGLE, QUADRILATERAL, TETRAHEDRON, HEXAHEDRON, PENTAHEDRON = 1, 2, 3, 4, 5, 6, 7
+
+
+class MeshFile:
+    """The host-side content of an OFELI ``.m`` mesh file, as Mesh::get keeps
+    it: ``coords`` (nn x dim, float-rounded as OFELI's stof does),
+    ``node_code`` (nn x nb_dof), ``elem`` (ne x el_nodes, 0-based),
+    ``elem_code``, ``sides`` (ns x sd_nodes, 0-based), ``side_code``
+    (ns x nb_dof).  Reading and writing need no GPU."""
+
+    def __init__(self, path=None, _handle=None):
+        if _handle is None:
+            h = ctypes.c_void_p()
+            _call("ofg_mesh_file_read", str(path).encode(), ctypes.byref(h))
+            _handle = h
+        self._h = _handle
+        i = [ctypes.c_int() for _ in range(6)]
+        n = [ctypes.c_int64() for _ in range(3)]
+        _call("ofg_mesh_file_info", self._h, ctypes.byref(i[0]), ctypes.byref(i[1]),
+              ctypes.byref(n[0]), ctypes.byref(i[2]), ctypes.byref(i[3]), ctypes.byref(n[1]),
+              ctypes.byref(i[4]), ctypes.byref(i[5]), ctypes.byref(n[2]))
+        self.dim, self.nb_dof = i[0].value, i[1].value
+        self.el_shape, self.el_nodes, self.sd_shape, self.sd_nodes = (i[2].value, i[3].value,
+                                                                      i[4].value, i[5].value)
+        self.nn, self.ne, self.ns = n[0].value, n[1].value, n[2].value
+
+    @classmethod
+    def create(cls, dim, coords, node_code, elem, elem_code, el_shape, nb_dof=1, sides=None,
+               side_code=None, sd_shape=LINE):
+        coords = np.ascontiguousarray(coords, dtype=np.float64).reshape(-1)
+        node_code = np.ascontiguousarray(node_code, dtype=np.int32).reshape(-1)
+        elem = np.ascontiguousarray(elem, dtype=np.int32)
+        elem_code = np.ascontiguousarray(elem_code, dtype=np.int32).reshape(-1)
+        nn, ne = coords.size // dim, elem_code.size
+        el_nodes = elem.size // max(ne, 1)
+        if sides is None:
+            sides = np.zeros(0, np.int32)
+            side_code = np.zeros(0, np.int32)
+        sides = np.ascontiguousarray(sides, dtype=np.int32)
+        side_code = np.ascontiguousarray(side_code, dtype=np.int32).reshape(-1)
+        ns = side_code.size // nb_dof
+        sd_nodes = sides.size // ns if ns else 0
+        h = ctypes.c_void_p()
+        _call("ofg_mesh_file_create", dim, nb_dof, nn, _ptr(coords), _ptr(node_code), el_shape,
+              el_nodes, ne, _ptr(elem), _ptr(elem_code), sd_shape, sd_nodes, ns, _ptr(sides),
+              _ptr(side_code), ctypes.byref(h))
+        return cls(_handle=h)
+
+    @classmethod
+    def from_mesh(cls, mesh):
+        h = ctypes.c_void_p()
+        _call("ofg_mesh_file_from_mesh", mesh._h, ctypes.byref(h))
+        return cls(_handle=h)
+
+    def arrays(self):
+        coords = np.zeros((self.nn, self.dim))
+        node_code = np.zeros((self.nn, self.nb_dof), np.int32)
+        elem = np.zeros((self.ne, self.el_nodes), np.int32)
+        elem_code = np.zeros(self.ne, np.int32)
+        sides = np.zeros((self.ns, self.sd_nodes), np.int32)
+        side_code = np.zeros((self.ns, self.nb_dof), np.int32)
+        _call("ofg_mesh_file_get", self._h, _ptr(coords), _ptr(node_code), _ptr(elem),
+              _ptr(elem_code), _ptr(sides), _ptr(side_code))
+        return dict(coords=coords, node_code=node_code, elem=elem, elem_code=elem_code,
+                    sides=sides, side_code=side_code)
+
+    def put(self, path):
+        _call("ofg_mesh_file_write", self._h, str(path).encode())
+
+    def to_mesh(self):
+        h = ctypes.c_void_p()
+        _call("ofg_mesh_create_from_file", self._h, ctypes.byref(h))
+        return Mesh(_handle=h)
+
+    @staticmethod
+    def set_threads(n):
+        _call("ofg_mesh_file_set_threads", n)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and capi is not None and capi._lib is not None:
+            capi.lib().ofg_mesh_file_destroy(self._h)
             self._h = None
 
 

@@ -8,14 +8,21 @@
 //   ofeli_ref p2d  NX NY   SOLVER PREC TOL MAXIT INDIR OUTDIR
 //   ofeli_ref p3d  M       SOLVER PREC TOL MAXIT INDIR OUTDIR
 //   ofeli_ref cd2d NX NY   NSTEPS DT EPS PREC TOL MAXIT INDIR OUTDIR
-//   SOLVER = CG | GMRES<m> ; PREC = IDENT | DIAG | DILU | ILU | SSOR
+//   ofeli_ref mget FILE INDIR OUTDIR            (Mesh::get, dump, Mesh::put)
+//   ofeli_ref mrect NX NY CX0 CXN CY0 CYN INDIR OUTDIR  (Mesh(rect), dump, put)
+//   ofeli_ref mlap FILE SOLVER PREC TOL MAXIT INDIR OUTDIR
+//   SOLVER = CG | GMRES<m> | BICGSTAB ; PREC = IDENT | DIAG | DILU | ILU | SSOR
 // INDIR holds f.f64 (one value per node), optionally k.f64 (one value per
 // element: scales the element stiffness), xy.f64 (2-D node coordinates that
 // replace the structured ones), u0.f64 / v.f64 (cd2d initial field and the
 // nodal velocity, interleaved vx,vy).
 // OUTDIR receives info.txt (key=value), row_ptr.i64 (0-based), col_ind.i64
 // (1-based, OFELI's own convention), a.f64, b.f64, x.f64 (equation space),
-// u.f64 (nodal, boundary values inserted).
+// u.f64 (nodal, boundary values inserted).  mget writes the mesh as Mesh::get
+// keeps it (coords.f64, node_code.i32, elem.i32 with 1-based node labels,
+// elem_code.i32, side.i32, side_code.i32, shapes and sizes in info.txt) and
+// OUTDIR/put.m from Mesh::put; mlap solves the P1 problem of p2d (2-D) or
+// p3d (3-D) on the mesh read from FILE by Mesh(FILE, true).
 //
 // Reference entry points used (paths within the OFELI project):
 //   Mesh(xmin,xmax,ymin,ymax,nx,ny,c..,TRIANGLE)   src/mesh/Mesh.cpp:547-676
@@ -25,6 +32,7 @@
 //   DC2DT3 Capacity/LCapacity/Diffusion/Convection  src/equations/therm/DC2DT3.cpp:121-207
 //   Equa_Laplace::build, Equa_Therm::build          include/equations/laplace/Equa_Laplace.h:112-133,
 //                                                   include/equations/therm/Equa_Therm.h:162-218
+//   Mesh::get / Mesh::put                           src/mesh/Mesh.cpp:2639-2668, 2731-2806
 //   Prec<real_t>(A,type), CG(A,P,b,x,..), GMRes(A,P,b,x,m,..)
 //                                                   include/solvers/{Prec.h,CG.h:99-157,GMRes.h:148-241}
 #include "OFELI.h"
@@ -552,6 +560,157 @@ int run_cd2d(int argc, char** argv)
    return 0;
 }
 
+// The data a Mesh keeps (coords, codes, 1-based element / side node labels)
+// and Mesh::put of it.
+void dump_mesh(Mesh& ms, const std::string& out, Info& info)
+{
+   size_t nn = ms.getNbNodes(), ne = ms.getNbElements(), ns = ms.getNbSides();
+   size_t dim = ms.getDim();
+   size_t nd = nn ? ms.getPtrNode(1)->getNbDOF() : 0;
+   std::vector<double> xy;
+   std::vector<int> nc;
+   for (size_t i = 1; i <= nn; ++i) {
+      Node* p = ms.getPtrNode(i);
+      for (size_t k = 1; k <= dim; ++k) xy.push_back(p->getCoord(k));
+      for (size_t k = 1; k <= nd; ++k) nc.push_back(p->getCode(k));
+   }
+   std::vector<int> el, ec, sd, sc;
+   size_t enn = ne ? ms.getPtrElement(1)->getNbNodes() : 0;
+   for (size_t i = 1; i <= ne; ++i) {
+      Element* e = ms.getPtrElement(i);
+      for (size_t k = 1; k <= e->getNbNodes(); ++k) el.push_back((int)(*e)(k)->n());
+      ec.push_back(e->getCode());
+   }
+   size_t snn = ns ? ms.getPtrSide(1)->getNbNodes() : 0;
+   for (size_t i = 1; i <= ns; ++i) {
+      Side* s = ms.getPtrSide(i);
+      for (size_t k = 1; k <= s->getNbNodes(); ++k) sd.push_back((int)(*s)(k)->n());
+      for (size_t k = 1; k <= nd; ++k) sc.push_back(s->getCode(k));
+   }
+   write_bin(out + "/coords.f64", xy.data(), xy.size());
+   write_bin(out + "/node_code.i32", nc.data(), nc.size());
+   write_bin(out + "/elem.i32", el.data(), el.size());
+   write_bin(out + "/elem_code.i32", ec.data(), ec.size());
+   write_bin(out + "/side.i32", sd.data(), sd.size());
+   write_bin(out + "/side_code.i32", sc.data(), sc.size());
+   double t1 = now_s();
+   ms.put(out + "/put.m");
+   info.set("t_put", now_s() - t1);
+   info.seti("dim", (long long)dim);
+   info.seti("nb_dof", (long long)nd);
+   info.seti("nodes", (long long)nn);
+   info.seti("elements", (long long)ne);
+   info.seti("sides", (long long)ns);
+   info.seti("el_shape", ne ? (long long)ms.getPtrElement(1)->getShape() : 0);
+   info.seti("el_nodes", (long long)enn);
+   info.seti("sd_shape", ns ? (long long)ms.getPtrSide(1)->getShape() : 0);
+   info.seti("sd_nodes", (long long)snn);
+}
+
+// Mesh::get of an OFELI .m file (INDIR unused).
+int run_mget(int argc, char** argv)
+{
+   if (argc < 5) return 2;
+   std::string file = argv[2], out = argv[4];
+   Info info;
+   double t0 = now_s();
+   Mesh ms;
+   ms.get(file);
+   info.set("t_get", now_s() - t0);
+   dump_mesh(ms, out, info);
+   info.write(out);
+   return 0;
+}
+
+// The structured rectangle mesh of Mesh(0,1,0,1,nx,ny,cx0,cxN,cy0,cyN,
+// TRIANGLE), whose negative line codes give negative node codes and sides.
+int run_mrect(int argc, char** argv)
+{
+   if (argc < 10) return 2;
+   size_t nx = std::stoul(argv[2]), ny = std::stoul(argv[3]);
+   int c[4];
+   for (int i = 0; i < 4; ++i) c[i] = std::stoi(argv[4 + i]);
+   std::string out = argv[9];
+   Info info;
+   Mesh ms(0., 1., 0., 1., nx, ny, c[0], c[1], c[2], c[3], TRIANGLE);
+   dump_mesh(ms, out, info);
+   info.write(out);
+   return 0;
+}
+
+// The p2d / p3d problem on a mesh read from a file: Mesh(FILE, true), then
+// the 2-D Laplace (KLaplace2DT3) or 3-D diffusion (KDC3DT4) equation.
+template <class EQ>
+int solve_on_file_mesh(Mesh& ms, const std::string& solver, Preconditioner prec, const char* pname,
+                       double tol, int maxit, const std::string& in, const std::string& out,
+                       Info& info)
+{
+   size_t nn = ms.getNbNodes(), ne = ms.getNbElements();
+   std::vector<double> fv = read_f64(in + "/f.f64", nn);
+   std::vector<double> kv;
+   if (file_exists(in + "/k.f64")) kv = read_f64(in + "/k.f64", ne);
+   Vect<real_t> u(ms), f(ms), bc(ms);
+   for (size_t i = 0; i < nn; ++i) f[i] = fv[i];
+   bc = 0;
+   if (file_exists(in + "/bc.f64")) {
+      std::vector<double> bv = read_f64(in + "/bc.f64", nn);
+      for (size_t i = 0; i < nn; ++i) bc[i] = bv[i];
+   }
+   EQ eq(ms, u);
+   if (!kv.empty()) eq.k = kv.data();
+   double t1 = now_s();
+   eq.setSolver(CG_SOLVER, prec);
+   double t_graph = now_s() - t1;
+   eq.setSource(f);
+   eq.setDirichlet(bc);
+   Vect<real_t>& b = *eq.rhs();
+   b.clear();
+   eq.sol().setSize(eq.neq());
+   double t2 = now_s();
+   eq.build();
+   double t_asm = now_s() - t2;
+   SpMatrix<real_t>& A = *dynamic_cast<SpMatrix<real_t>*>(eq.mat());
+   double t_prec = 0, t_solve = 0;
+   int it = solve_system(eq, A, b, eq.sol(), solver, prec, maxit, tol, t_prec, t_solve);
+   u.insertBC(ms, eq.sol(), bc);
+   dump_matrix(A, out, info);
+   write_bin(out + "/b.f64", &b[0], b.size());
+   write_bin(out + "/x.f64", &eq.sol()[0], eq.sol().size());
+   write_bin(out + "/u.f64", &u[0], u.size());
+   info.seti("nodes", (long long)nn);
+   info.seti("elements", (long long)ne);
+   info.seti("iters", it);
+   info.set("t_graph", t_graph);
+   info.set("t_assembly", t_asm);
+   info.set("t_prec", t_prec);
+   info.set("t_solve", t_solve);
+   info.set("norm_u", u.getNorm2());
+   info.sets("solver", solver);
+   info.sets("prec", pname);
+   return 0;
+}
+
+int run_mlap(int argc, char** argv)
+{
+   if (argc < 9) return 2;
+   std::string file = argv[2], solver = argv[3];
+   Preconditioner prec = parse_prec(argv[4]);
+   double tol = std::stod(argv[5]);
+   int maxit = std::stoi(argv[6]);
+   std::string in = argv[7], out = argv[8];
+   Info info;
+   double t0 = now_s();
+   Mesh ms(file, true);
+   info.set("t_mesh", now_s() - t0);
+   int rc;
+   if (ms.getDim() == 3)
+      rc = solve_on_file_mesh<KDC3DT4>(ms, solver, prec, argv[4], tol, maxit, in, out, info);
+   else
+      rc = solve_on_file_mesh<KLaplace2DT3>(ms, solver, prec, argv[4], tol, maxit, in, out, info);
+   info.write(out);
+   return rc;
+}
+
 }  // namespace
 
 int main(int argc, char** argv)
@@ -567,6 +726,9 @@ int main(int argc, char** argv)
       if (mode == "p3d") return run_p3d(argc, argv);
       if (mode == "cd2d") return run_cd2d(argc, argv);
       if (mode == "bench2d") return run_bench2d(argc, argv);
+      if (mode == "mget") return run_mget(argc, argv);
+      if (mode == "mrect") return run_mrect(argc, argv);
+      if (mode == "mlap") return run_mlap(argc, argv);
    }
    catch (std::exception& e) {
       fprintf(stderr, "OFELI exception: %s\n", e.what());

@@ -12,6 +12,7 @@ recorded in the file, so the tests regenerate them instead of storing them.
 import json
 import os
 import sys
+import tempfile
 
 import numpy as np
 
@@ -151,6 +152,104 @@ def case_bicgstab():
     save("bicgstab", arrays, meta)
 
 
+# nb_dof 2 with negative and multi-digit marks, the "tria" alias, attributes
+# in either order (one pair written without a blank between them), tabs and a
+# CR, comments outside the blocks, a node no element uses, element code 3
+# only (no material "Generic" under code 1, so Mesh::put writes an empty
+# Material block).
+MESHIO_CODES = (
+    '<?xml version="1.0"?>\n'
+    "<!-- nb_dof 2, negative and multi-digit marks, sides with negative marks -->\n"
+    "<OFELI_File>\n<info><title>codes</title></info>\n"
+    "<Mesh nb_dof=\"2\"   dim=\"2\" >\n"
+    "   <Nodes>\n\t0.0 0.0 11\n   1.0  0.0   -12\r\n   1.0 1.0 3\n 0.0 1.0 -1\n"
+    " 0.5 0.5 0\n 1e-1 2.5E-1 120\n 0.3333333333333333 -7.25e-3 -99\n   </Nodes>\n"
+    "   <!-- four triangles around the centre -->\n"
+    '   <Elements shape="tria" nodes="3">\n 1 2 5 3\n 2 3 5 3\n 3 4 5 3\n 4 1 5 3\n'
+    "   </Elements>\n"
+    "   <Sides nodes=\"2\"shape=\"line\">\n 1 2 -21\n 2 3 10\n 3 4 0\n 4 1 -3\n   </Sides>\n"
+    "</Mesh>\n</OFELI_File>\n")
+
+
+def kuhn_permuted(M, seed):
+    xyz, elem, code = O.mesh3d(M)
+    rng = np.random.default_rng(seed)
+    perm = rng.permutation(code.size)
+    xyz2 = np.empty_like(xyz.reshape(-1, 3))
+    xyz2[perm] = xyz.reshape(-1, 3)
+    code2 = np.empty_like(code)
+    code2[perm] = code
+    return xyz2, perm[elem.reshape(-1, 4)].astype(np.int32), code2
+
+
+def case_meshio():
+    """OFELI's .m mesh files: Mesh::get of three files written here (an
+    annulus with a random numbering, sides and a Material block; a small
+    hand-written nb_dof 2 file; a Kuhn cube with a random numbering), their
+    Mesh::put bytes, Mesh(rect).put with negative line codes, and the P1
+    problems solved on the two P1 meshes by Mesh(file, true)."""
+    from ofeli_b200 import problems
+    from oracle import mesh_oracle as MO
+    xy, elem, code, sides, smark = problems.ring_mesh(6, 24, seed=1)
+    ecode = np.where(np.arange(elem.shape[0]) % 4 == 0, 2, 1).astype(np.int32)
+    ring = dict(dim=2, nb_dof=1, el_shape=3, el_nodes=3, sd_shape=2, sd_nodes=2, coords=xy,
+                node_code=code[:, None], elem=elem, elem_code=ecode, sides=sides,
+                side_code=smark[:, None])
+    text = MO.put(ring).decode().replace(
+        "</Mesh>", "   <Material>\n     1   Generic\n     2   Copper\n   </Material>\n</Mesh>")
+    xyz, tet, tcode = kuhn_permuted(3, seed=2)
+    tetm = dict(dim=3, nb_dof=1, el_shape=5, el_nodes=4, sd_shape=0, sd_nodes=0, coords=xyz,
+                node_code=tcode[:, None], elem=tet, elem_code=np.ones(tet.shape[0], np.int32),
+                sides=np.zeros((0, 1), np.int32), side_code=np.zeros((0, 1), np.int32))
+    files = {"meshio_ring": text, "meshio_codes": MESHIO_CODES,
+             "meshio_tet": MO.put(tetm).decode()}
+    arrays, meta = {}, {"files": {}, "runs": {}}
+    for name, body in files.items():
+        path = os.path.join(HERE, name + ".m")
+        with open(path, "w", newline="") as fh:
+            fh.write(body)
+        info, out = O.run_reference(["mget", path], {})
+        tmp = tempfile.mkdtemp(prefix="mget_")
+        O.run_reference(["mget", path], {}, keep=tmp)
+        put = open(os.path.join(tmp, "out", "put.m"), "rb").read()
+        key = name.split("_", 1)[1]
+        arrays.update({key + "_coords": out["coords"], key + "_node_code": out["node_code"],
+                       key + "_elem": out["elem"] - 1, key + "_elem_code": out["elem_code"],
+                       key + "_side": out["side"] - 1, key + "_side_code": out["side_code"],
+                       key + "_put": np.frombuffer(put, np.uint8)})
+        meta["files"][key] = {k: info[k] for k in ("dim", "nb_dof", "nodes", "elements", "sides",
+                                                   "el_shape", "el_nodes", "sd_shape", "sd_nodes")}
+    # Mesh(0,1,0,1,4,3,-1,2,-3,0): sides on x = 0 and y = 0, code 2 on x = 1
+    tmp = tempfile.mkdtemp(prefix="mrect_")
+    O.run_reference(["mrect", 4, 3, -1, 2, -3, 0], {}, keep=tmp)
+    arrays["rect_put"] = np.fromfile(os.path.join(tmp, "out", "put.m"), np.uint8)
+    # P1 problems on the meshes read back: the annulus with k = 1 (element
+    # code 1) or 3 (code 2), f seed 11, u = 1 on the outer circle; the cube
+    # with f seed 12, u = 0 on the boundary
+    nn = xy.shape[0]
+    ring_bc = np.where(code == 2, 1.0, 0.0)
+    ring_k = np.where(ecode == 2, 3.0, 1.0)
+    ring_f = fields.uniform_pm1(11, nn)
+    tet_f = fields.uniform_pm1(12, xyz.shape[0])
+    for key, path, inputs, runs in [
+            ("ring", "meshio_ring.m", {"f": ring_f, "bc": ring_bc, "k": ring_k},
+             [("CG", "DILU"), ("CG", "DIAG"), ("BICGSTAB", "ILU")]),
+            ("tet", "meshio_tet.m", {"f": tet_f}, [("CG", "DILU")])]:
+        for solver, prec in runs:
+            info, out = O.run_reference(["mlap", os.path.join(HERE, path), solver, prec, 1e-10,
+                                         20000], inputs)
+            if key + "_row_ptr" not in arrays:
+                arrays.update({key + "_row_ptr": out["row_ptr"].astype(np.int32),
+                               key + "_col_ind": out["col_ind"].astype(np.int32),
+                               key + "_a": out["a"], key + "_b": out["b"]})
+            arrays["%s_x_%s_%s" % (key, solver, prec)] = out["x"]
+            arrays["%s_u_%s_%s" % (key, solver, prec)] = out["u"]
+            meta["runs"]["%s_%s_%s" % (key, solver, prec)] = {"iters": info["iters"]}
+    meta["ring"] = {"seed_f": 11, "k": [1.0, 3.0], "bc_outer": 1.0}
+    meta["tet"] = {"seed_f": 12}
+    save("meshio", arrays, meta)
+
+
 if __name__ == "__main__":
     if not O.have_reference("o2"):
         raise SystemExit("build the reference first: make -C oracle ref")
@@ -160,3 +259,4 @@ if __name__ == "__main__":
     case_p3d()
     case_cd2d()
     case_bicgstab()
+    case_meshio()
