@@ -14,7 +14,7 @@ jacobi` selects the Jacobi inner iteration.  The plain FP64 CG + D-ILU solve
 (OFELI's own method) is timed once beside it.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--workload poisson2d|kuhn3d|batch2d|transient2d]
+                    [--workload poisson2d|kuhn3d|batch2d|transient2d|meshfile2d]
 
 N > 1 runs N independent replicas (the problem does not shard; no
 collective in the data path), launched one rank per GPU by torchrun.
@@ -40,6 +40,8 @@ METRIC_TRANSIENT = ("backward-Euler time steps/sec (DC2DT3 convection-diffusion 
                     "GMRES(30) to 1e-10 per step, warm start)")
 METRIC_BATCH = ("FP64-accurate solves/sec (1024 uneven 2-D P1 problems, 1e3..6.4e4 nodes, "
                 "true rel. residual <= 1e-10)")
+METRIC_MESHFILE = ("mesh nodes/sec from an OFELI .m file to the assembled P1 system on the device "
+                   "(Mesh::get + SpMatrix(mesh) + build(), 1.05M-node annulus)")
 UNIT = "solves/s"
 SEED = 1234
 TOL = 1e-10
@@ -57,12 +59,13 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nx", type=int, default=2048, help="cells per side (nodes = nx+1)")
     ap.add_argument("--workload", default="poisson2d",
-                    choices=["poisson2d", "kuhn3d", "batch2d", "transient2d"],
+                    choices=["poisson2d", "kuhn3d", "batch2d", "transient2d", "meshfile2d"],
                     help="poisson2d: the headline 2-D problem; kuhn3d: the 3-D "
                          "variable-coefficient problem (129^3 Kuhn cube, lognormal k); batch2d: "
                          "1024 uneven jittered 2-D problems in one persistent launch; "
                          "transient2d: DC2DT3 backward-Euler steps at 1025^2 (a step = one time "
-                         "step)")
+                         "step); meshfile2d: an OFELI .m mesh file read and turned into the "
+                         "assembled P1 system on the device (a step = one file)")
     ap.add_argument("--nprob", type=int, default=1024,
                     help="batch2d: number of problems (the workload is 1024; smaller counts are "
                          "for profiling captures)")
@@ -217,6 +220,8 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    if args.workload == "meshfile2d":
+        return run_reference_meshfile(args)
     nx = args.nx
     flavour = "ofast" if O.have_reference("ofast") else "o2"
     if not O.have_reference(flavour):
@@ -987,6 +992,258 @@ def run_transient(args):
     return 0
 
 
+# ------------------------------------------------- mesh-file workload -----
+MF_N = 1024          # annulus of MF_N + 1 circles of MF_N nodes, 2 MF_N^2 triangles
+MF_SAMPLE = 512      # the same annulus at 512 for the reference's bounded CPU sample
+
+
+def meshfile_write(nr, seed=SEED):
+    """The annulus (random node numbering, random cell diagonals, jittered
+    interior) written as an OFELI .m file by the library's own Mesh::put.
+    Returns (path, node code, seconds spent in put)."""
+    import tempfile
+    from ofeli_b200 import ofeli as F
+    from ofeli_b200 import problems
+    xy, elem, code, sides, smark = problems.ring_mesh(nr, nr, seed=seed)
+    mf = F.MeshFile.create(2, xy, code, elem, np.ones(elem.shape[0], np.int32), F.TRIANGLE,
+                           sides=sides, side_code=smark)
+    path = os.path.join(tempfile.mkdtemp(prefix="ofeli_meshfile_"), "annulus_%d.m" % nr)
+    t0 = time.perf_counter()
+    mf.put(path)
+    return path, code, time.perf_counter() - t0
+
+
+def meshfile_reference_sample(nsamples=1):
+    """OFELI itself (reference sources, -Ofast, 1 thread) on the 512 annulus:
+    Mesh(file, true) + SpMatrix(mesh) + build(), per sample."""
+    from ofeli_b200 import fields
+    from oracle import oracle as O
+    flavour = "ofast" if O.have_reference("ofast") else ("o2" if O.have_reference("o2") else None)
+    if not flavour:
+        return None
+    path, code, _ = meshfile_write(MF_SAMPLE)
+    nn = code.size
+    f = fields.uniform_pm1(SEED, nn)
+    bc = np.where(code == 2, 1.0, 0.0)
+    times = []
+    for _ in range(nsamples):
+        info, _ = O.run_reference(["mlap", path, "CG", "DIAG", 1e-10, 1], {"f": f, "bc": bc},
+                                  flavour=flavour)
+        times.append(float(info["t_mesh"]) + float(info["t_graph"]) + float(info["t_assembly"]))
+    os.remove(path)
+    return {"nodes": nn, "times": times, "flavour": flavour,
+            "size_mb": None, "last": info}
+
+
+def run_reference_meshfile(args):
+    nsteps = args.warmup + args.steps
+    t0 = time.perf_counter()
+    r = meshfile_reference_sample(nsteps)
+    if r is None:
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref was not built (needs the reference sources)"}))
+        return 0
+    t_step = statistics.mean(r["times"][args.warmup:])
+    value = r["nodes"] / t_step
+    info = r["last"]
+    sample = ("OFELI (reference sources, -%s), 1 thread: Mesh(file, true) %.2f s + SpMatrix(mesh) "
+              "%.2f s + build() %.2f s on the %d-node annulus file (the workload's mesh at "
+              "%d x %d)" % ("Ofast" if r["flavour"] == "ofast" else "O2", float(info["t_mesh"]),
+                            float(info["t_graph"]), float(info["t_assembly"]), r["nodes"],
+                            MF_SAMPLE + 1, MF_SAMPLE))
+    line = {"impl": "reference", "metric": METRIC_MESHFILE, "value": value, "unit": "nodes/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "OFELI .m file of a %d-node annulus, read + graph + P1 "
+                                   "Laplace assembly" % r["nodes"]},
+            "cpu_baseline": {"value": value, "unit": "nodes/s", "cores": 1, "kind": "reference",
+                             "sample": sample, "host_cores": os.cpu_count()},
+            "e2e": {"value": value, "unit": "nodes/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "wall_s": time.perf_counter() - t0}
+    print(json.dumps(line))
+    return 0
+
+
+def run_meshfile(args):
+    import torch
+    from ofeli_b200 import capi, fields
+    from ofeli_b200 import ofeli as F
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    work_stream = torch.cuda.Stream(device=torch.device("cuda", local))
+    torch.cuda.set_stream(work_stream)
+    capi.call("ofg_set_stream", ctypes.c_void_p(work_stream.cuda_stream))
+    dev = torch.device("cuda", local)
+    P_ = F._ptr
+    path, code, t_put = meshfile_write(MF_N, seed=SEED + rank)
+    size = os.path.getsize(path)
+    mf0 = F.MeshFile(path)
+    a0 = mf0.arrays()
+    nn, ne = mf0.nn, mf0.ne
+    f = fields.uniform_pm1(SEED, nn)
+    bc = np.where(a0["node_code"][:, 0] == 2, 1.0, 0.0)
+    m0 = mf0.to_mesh()
+    n = m0.neq
+    del m0, mf0
+    # device-resident inputs of the device leg (the file's values, already parsed)
+    d_xy = torch.from_numpy(np.ascontiguousarray(a0["coords"].ravel())).to(dev)
+    d_el = torch.from_numpy(np.ascontiguousarray(a0["elem"].ravel())).to(dev)
+    d_code = torch.from_numpy(np.ascontiguousarray(a0["node_code"][:, 0])).to(dev)
+    d_f = torch.from_numpy(f).to(dev)
+    d_bc = torch.from_numpy(bc).to(dev)
+    d_b = torch.zeros(n, dtype=torch.float64, device=dev)
+    f_pin = torch.from_numpy(f).pin_memory()
+    bc_pin = torch.from_numpy(bc).pin_memory()
+    b_pin = torch.zeros(n, dtype=torch.float64).pin_memory()
+    nnz = [0]
+
+    def step_device():
+        h = ctypes.c_void_p()
+        capi.call("ofg_mesh_create", 2, nn, P_(d_xy), ne, P_(d_el), P_(d_code), ctypes.byref(h))
+        m = F.Mesh(_handle=h)
+        A = F.SpMatrix(m)
+        capi.call("ofg_assemble_p1", m._h, A._h, None, P_(d_f), P_(d_bc), P_(d_b))
+        nnz[0] = A.nnz
+        del A, m
+
+    def step_e2e():
+        mf = F.MeshFile(path)
+        m = mf.to_mesh()
+        A = F.SpMatrix(m)
+        capi.call("ofg_assemble_p1", m._h, A._h, None, P_(f_pin), P_(bc_pin), P_(b_pin))
+        del A, m, mf
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def timed(fn, k):
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record(work_stream)
+        for _ in range(k):
+            fn()
+        e1.record(work_stream)
+        torch.cuda.synchronize()
+        ms = max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3)
+        barrier()
+        if dist:
+            t = torch.tensor([ms], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    for _ in range(args.warmup):
+        step_device()
+        step_e2e()
+    torch.cuda.synchronize()
+    launches0 = capi.launch_count()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.4)
+    ms = timed(step_device, args.steps)
+    launches = capi.launch_count() - launches0
+    e2e_ms = timed(step_e2e, args.steps)
+    clk = clocks.stop()
+    # the assembled system against the one assembled from the file read in
+    # the e2e leg (same values: both gather in element order)
+    same = bool(torch.equal(d_b.cpu(), b_pin))
+    # phases of one e2e step, each closed by a synchronisation (untimed pass)
+    ph = {}
+    t0 = time.perf_counter()
+    mf = F.MeshFile(path)
+    ph["read_s"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    m = mf.to_mesh()
+    ph["device_mesh_s"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    A = F.SpMatrix(m)
+    torch.cuda.synchronize()
+    ph["pattern_s"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    capi.call("ofg_assemble_p1", m._h, A._h, None, P_(d_f), P_(d_bc), P_(d_b))
+    ph["assembly_s"] = time.perf_counter() - t0
+    # the assembly kernel timed with CUDA events over 20 launches
+    capi.profile_enable(1)
+    for _ in range(20):
+        capi.call("ofg_assemble_p1", m._h, A._h, None, P_(d_f), P_(d_bc), P_(d_b))
+    torch.cuda.synchronize()
+    cnt, tot_ms, tot_bytes = capi.profile_read("assembly")
+    capi.profile_enable(0)
+    del A, m, mf
+    os.remove(path)
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return 0
+    cpu = None
+    if world == 1:
+        r = meshfile_reference_sample(1)
+        if r:
+            info = r["last"]
+            cpu = {"value": r["nodes"] / r["times"][0], "unit": "nodes/s", "cores": 1,
+                   "kind": "reference",
+                   "sample": "OFELI (reference sources, -%s), 1 thread: Mesh(file, true) %.2f s + "
+                             "SpMatrix(mesh) %.2f s + build() %.2f s on the same annulus at "
+                             "%d nodes" % ("Ofast" if r["flavour"] == "ofast" else "O2",
+                                           float(info["t_mesh"]), float(info["t_graph"]),
+                                           float(info["t_assembly"]), r["nodes"]),
+                   "host_cores": os.cpu_count()}
+    peak, peak_kind = measured_peaks()
+    avg_us = tot_ms / max(cnt, 1) * 1e3
+    achieved = (tot_bytes / max(cnt, 1)) / (avg_us * 1e-6) / 1e9 if cnt else None
+    line = {
+        "metric": METRIC_MESHFILE, "value": world * args.steps * nn / (ms / 1e3),
+        "unit": "nodes/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "OFELI .m file (%.0f MB) of an annulus with %d nodes, %d triangles, "
+                               "random node numbering; a step = Mesh::get + device mesh + "
+                               "SpMatrix(mesh) pattern + Laplace2DT3 build() with f ~ U[-1,1] "
+                               "and u = 1 on the outer circle (%d unknowns, %d nonzeros)"
+                               % (size / 1e6, nn, ne, n, nnz[0]),
+                   "value_leg": "mesh arrays already parsed and resident in HBM: device mesh + "
+                                "pattern + assembly",
+                   "e2e_leg": "the file (page cache) through MeshFile read, "
+                              "ofg_mesh_create_from_file, SpMatrix(mesh) and ofg_assemble_p1 "
+                              "with host f, bc and b",
+                   "host_threads": os.cpu_count(), "put_s": t_put,
+                   "phases_one_step": ph, "device_and_file_rhs_equal": same,
+                   "inputs_larger_than_l2": True},
+        "gpu_launches": launches,
+        "e2e": {"value": world * args.steps * nn / (e2e_ms / 1e3), "unit": "nodes/s",
+                "h2d_bytes_per_step": 8 * 2 * nn + 4 * 3 * ne + 4 * nn + 8 * 2 * nn,
+                "d2h_bytes_per_step": 8 * n},
+        "roofline": {"kernel": "assemble_rows<LaplaceT3> (row-gather P1 assembly)",
+                     "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if achieved else None, "traffic": None,
+                     "peak_source": peak_kind, "launches_timed": cnt, "avg_launch_us": avg_us,
+                     "bytes_per_launch": tot_bytes / max(cnt, 1)},
+        "cpu_baseline": cpu,
+        "clocks": clk,
+    }
+    print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -995,6 +1252,8 @@ def main():
         return run_batch(args)
     if args.workload == "transient2d":
         return run_transient(args)
+    if args.workload == "meshfile2d":
+        return run_meshfile(args)
     return run_ours(args)
 
 

@@ -1,17 +1,25 @@
 // assembly.cu -- Equation::build() for P1 elements on the device.
 //
-// One launch per element colour.  A thread owns one element: it computes the
-// element geometry and the local matrix / RHS in registers (FP64, the same
-// formulas as Triang3/Tetra4 and the element classes), lifts imposed values
-// (Equation::updateBC) and scatters through the precomputed element-to-CSR
-// map.  Elements of one colour share no node, so no two threads of a launch
-// touch the same CSR entry or RHS row: the scatter needs no atomics, and the
-// launches of successive colours are ordered by the stream.
+// One thread per mesh node gathers the CSR row of the node's equation and its
+// RHS entry: it zeroes the row, then walks the node's elements in ascending
+// element number (the node-to-element lists are sorted), computes each
+// element's matrix and RHS in registers (FP64, the same formulas as
+// Triang3/Tetra4 and the element classes, imposed values lifted as
+// Equation::updateBC does) and adds the element row into its own CSR row and
+// RHS entry.  Every matrix entry and RHS entry therefore receives its element
+// contributions in OFELI's element-loop order, starting from zero, so the
+// assembled values are the reference's bit for bit on any mesh; a thread
+// writes only its own row, so there are no atomics and no element colouring.
+// Each element is computed once per node (3 or 4 times); the FP64 arithmetic
+// is cheap beside the memory traffic.  An element's Jacobian is checked by
+// the thread of its first node, equation or not, and the lowest bad element
+// is reported as OFELI's element loop would meet it first.
 //
-// Algorithmic bytes per element (2-D / 3-D): connectivity 4*nen, node
-// coordinates 8*dim*nen (gathered; each node is shared by ~6 / ~24
-// elements), k 8, f 8*nen (gathered), the map 4*nen^2, A updates
-// 16*nen^2 (read-modify-write), b updates 16*nen.
+// Algorithmic bytes per launch: node-to-element lists 4*(nn+1) + 4*nen*ne,
+// connectivity 4*nen*ne, coordinates 8*dim*nn, code and equation number
+// 8*nn, the element-to-CSR map 4*nen^2*ne, k 8*ne, the node fields read
+// (f, or u_old and v) 8*nn each, CSR row pointers 4*(n+1), A written 8*nnz,
+// b written 8*n.
 #include "element.cuh"
 
 namespace ofg {
@@ -21,28 +29,19 @@ using namespace elem;
 
 // Laplace2DT3::LHS (times k) + BodyRHS: Ke = area*(g_i.g_j)*k, Fe = f*area/3
 // (src/equations/laplace/Laplace2DT3.cpp:131-143)
-__global__ void __launch_bounds__(256) assemble_t3(int64_t cnt, const int32_t* __restrict__ list,
-                                                   const int32_t* __restrict__ elem,
-                                                   const double* __restrict__ xy,
-                                                   const int32_t* __restrict__ code,
-                                                   const int32_t* __restrict__ dof,
-                                                   const int32_t* __restrict__ emap,
-                                                   const double* __restrict__ kel,
-                                                   const double* __restrict__ f,
-                                                   const double* __restrict__ bc, double* a,
-                                                   double* b, int* bad)
-{
-   int64_t stride = (int64_t)gridDim.x * blockDim.x;
-   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += stride) {
-      int64_t e = list[t];
-      int32_t en[3] = {elem[3 * e], elem[3 * e + 1], elem[3 * e + 2]};
+struct LaplaceT3 {
+   static constexpr int NEN = 3;
+   const double* xy;
+   const int32_t* code;
+   const double* kel;
+   const double* f;
+   const double* bc;
+   __device__ __forceinline__ bool operator()(int64_t e, const int32_t (&en)[3], double (&Ke)[3][3],
+                                              double (&Fe)[3]) const
+   {
       double g[3][3], area;
-      if (!tri3(xy, en, g, area)) {
-         atomicMin(bad, (int)e);
-         continue;
-      }
+      if (!tri3(xy, en, g, area)) return false;
       double k = kel ? kel[e] : 1.0;
-      double Ke[3][3], Fe[3];
 #pragma unroll
       for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -50,34 +49,25 @@ __global__ void __launch_bounds__(256) assemble_t3(int64_t cnt, const int32_t* _
 #pragma unroll
       for (int i = 0; i < 3; ++i) Fe[i] = f ? f[en[i]] * area * kThird : 0.0;
       if (bc) lift_bc<3>(en, code, bc, Ke, Fe);
-      scatter<3>(e, en, dof, emap, Ke, Fe, a, b);
+      return true;
    }
-}
+};
 
 // DC3DT4::Diffusion(k) + BodyRHS: Ke = (k*vol)*(g_i.g_j), Fe = f*vol/4
 // (src/equations/therm/DC3DT4.cpp:128-135, 207-211)
-__global__ void __launch_bounds__(256) assemble_t4(int64_t cnt, const int32_t* __restrict__ list,
-                                                   const int32_t* __restrict__ elem,
-                                                   const double* __restrict__ xyz,
-                                                   const int32_t* __restrict__ code,
-                                                   const int32_t* __restrict__ dof,
-                                                   const int32_t* __restrict__ emap,
-                                                   const double* __restrict__ kel,
-                                                   const double* __restrict__ f,
-                                                   const double* __restrict__ bc, double* a,
-                                                   double* b, int* bad)
-{
-   int64_t stride = (int64_t)gridDim.x * blockDim.x;
-   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += stride) {
-      int64_t e = list[t];
-      int32_t en[4] = {elem[4 * e], elem[4 * e + 1], elem[4 * e + 2], elem[4 * e + 3]};
+struct DiffusionT4 {
+   static constexpr int NEN = 4;
+   const double* xyz;
+   const int32_t* code;
+   const double* kel;
+   const double* f;
+   const double* bc;
+   __device__ __forceinline__ bool operator()(int64_t e, const int32_t (&en)[4], double (&Ke)[4][4],
+                                              double (&Fe)[4]) const
+   {
       double g[4][3], vol;
-      if (!tet4(xyz, en, g, vol)) {
-         atomicMin(bad, (int)e);
-         continue;
-      }
+      if (!tet4(xyz, en, g, vol)) return false;
       double c = (kel ? kel[e] : 1.0) * vol;
-      double Ke[4][4], Fe[4];
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -85,39 +75,32 @@ __global__ void __launch_bounds__(256) assemble_t4(int64_t cnt, const int32_t* _
 #pragma unroll
       for (int i = 0; i < 4; ++i) Fe[i] = f ? f[en[i]] * 0.25 * vol : 0.0;
       if (bc) lift_bc<4>(en, code, bc, Ke, Fe);
-      scatter<4>(e, en, dof, emap, Ke, Fe, a, b);
+      return true;
    }
-}
+};
 
 // DC2DT3 under backward Euler (include/equations/therm/Equa_Therm.h:162-218):
 // eA1 = Capacity + LCapacity (src/equations/therm/DC2DT3.cpp:121-138),
 // eA0 = Diffusion(eps) + Convection (:141-147, 185-207),
 // eMat = eA1/dt + eA0, eRHS = updateBC + (eA1/dt) u_old.
-__global__ void __launch_bounds__(256) assemble_cd2d(int64_t cnt, const int32_t* __restrict__ list,
-                                                     const int32_t* __restrict__ elem,
-                                                     const double* __restrict__ xy,
-                                                     const int32_t* __restrict__ code,
-                                                     const int32_t* __restrict__ dof,
-                                                     const int32_t* __restrict__ emap, double eps,
-                                                     const double* __restrict__ v, double dti,
-                                                     const double* __restrict__ u_old,
-                                                     const double* __restrict__ bc, double* a,
-                                                     double* b, int* bad)
-{
-   int64_t stride = (int64_t)gridDim.x * blockDim.x;
-   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += stride) {
-      int64_t e = list[t];
-      int32_t en[3] = {elem[3 * e], elem[3 * e + 1], elem[3 * e + 2]};
+struct ConvDiffT3 {
+   static constexpr int NEN = 3;
+   const double* xy;
+   const int32_t* code;
+   double eps, dti;
+   const double* v;
+   const double* u_old;
+   const double* bc;
+   __device__ __forceinline__ bool operator()(int64_t, const int32_t (&en)[3], double (&Ke)[3][3],
+                                              double (&Fe)[3]) const
+   {
       double g[3][3], area;
-      if (!tri3(xy, en, g, area)) {
-         atomicMin(bad, (int)e);
-         continue;
-      }
+      if (!tri3(xy, en, g, area)) return false;
       double cc = kSixth * area, dd = 0.5 * cc, cl = kThird * area;
       double v3[3] = {v[2 * en[0]] + v[2 * en[1]] + v[2 * en[2]],
                       v[2 * en[0] + 1] + v[2 * en[1] + 1] + v[2 * en[2] + 1], 0.0};
       double cv = kThird * kThird * area;
-      double Ke[3][3], M1[3][3], Fe[3];
+      double M1[3][3];
 #pragma unroll
       for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -132,16 +115,67 @@ __global__ void __launch_bounds__(256) assemble_cd2d(int64_t cnt, const int32_t*
 #pragma unroll
       for (int i = 0; i < 3; ++i)
          Fe[i] += M1[i][0] * u_old[en[0]] + M1[i][1] * u_old[en[1]] + M1[i][2] * u_old[en[2]];
-      scatter<3>(e, en, dof, emap, Ke, Fe, a, b);
+      return true;
    }
-}
+};
 
-__global__ void insert_bc_kernel(int64_t nn, const int32_t* code, const int32_t* dof,
-                                 const double* x, const double* bc, double* u)
+// One thread per node: the node's CSR row and RHS entry, gathered over its
+// elements in ascending order (see the file comment).
+template <class Elem>
+__global__ void __launch_bounds__(256) assemble_rows(int64_t nn, const int32_t* __restrict__ n2e_ptr,
+                                                     const int32_t* __restrict__ n2e,
+                                                     const int32_t* __restrict__ elem,
+                                                     const int32_t* __restrict__ dof,
+                                                     const int32_t* __restrict__ emap,
+                                                     const int32_t* __restrict__ row_ptr, Elem el,
+                                                     double* __restrict__ a, double* __restrict__ b,
+                                                     int* bad)
 {
+   constexpr int NEN = Elem::NEN;
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
-   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += stride)
-      u[i] = code[i] == 0 ? x[dof[i] - 1] : (bc ? bc[i] : 0.0);
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += stride) {
+      const int32_t r = dof[i];   // 1-based equation, 0 for an imposed node
+      if (r)
+         for (int32_t k = row_ptr[r - 1]; k < row_ptr[r]; ++k) a[k] = 0.0;
+      double bi = 0.0;
+      const int32_t q1 = n2e_ptr[i + 1];
+      for (int32_t q = n2e_ptr[i]; q < q1; ++q) {
+         const int64_t e = n2e[q];
+         int32_t en[NEN];
+#pragma unroll
+         for (int j = 0; j < NEN; ++j) en[j] = elem[NEN * e + j];
+         int li = 0;
+#pragma unroll
+         for (int j = NEN - 1; j > 0; --j)
+            if (en[j] == (int32_t)i) li = j;
+         if (!r && li != 0) continue;   // no row here: only the Jacobian check of led elements
+         double Ke[NEN][NEN], Fe[NEN];
+         if (!el(e, en, Ke, Fe)) {
+            if (li == 0) atomicMin(bad, (int)e);
+            continue;
+         }
+         if (!r) continue;
+         // row li of the element, selected without dynamic register indexing
+         double krow[NEN], frow = 0.0;
+#pragma unroll
+         for (int j = 0; j < NEN; ++j) krow[j] = 0.0;
+#pragma unroll
+         for (int t = 0; t < NEN; ++t)
+            if (t == li) {
+#pragma unroll
+               for (int j = 0; j < NEN; ++j) krow[j] = Ke[t][j];
+               frow = Fe[t];
+            }
+         const int32_t* mp = emap + (e * NEN + li) * NEN;
+#pragma unroll
+         for (int j = 0; j < NEN; ++j) {
+            const int32_t pos = mp[j];
+            if (pos >= 0) a[pos] += krow[j];
+         }
+         bi += frow;
+      }
+      if (r) b[r - 1] = bi;
+   }
 }
 
 void check_jacobian(const DBuf<int>& bad)
@@ -153,30 +187,41 @@ void check_jacobian(const DBuf<int>& bad)
                   "non-positive Jacobian determinant in element " + std::to_string(h + 1));
 }
 
-void prepare(ofg_mesh* m, ofg_matrix* A, double* db)
+// Launches the row-gather kernel for one element kind and checks Jacobians.
+template <class Elem>
+void assemble(ofg_mesh* m, ofg_matrix* A, const Elem& el, double* db, int node_fields)
 {
    OFG_REQUIRE(A->mesh == m, OFG_ERR_ARG, "matrix pattern was not built from this mesh");
-   A->val.zero();
-   if (A->n) OFG_CUDA(cudaMemsetAsync(db, 0, A->n * sizeof(double), stream()));
-}
-
-}  // namespace
-
-// Launches the element kernel once per colour.
-template <class Launch>
-static void for_each_color(ofg_mesh* m, Launch&& launch)
-{
-   for (size_t c = 0; c + 1 < m->color_ptr.size(); ++c) {
-      int64_t beg = m->color_ptr[c], cnt = m->color_ptr[c + 1] - beg;
-      if (!cnt) continue;
+   DBuf<int> bad(1);
+   int big = INT32_MAX;
+   bad.upload(&big, 1);
+   if (m->nn) {
+      const int nen = m->nen;
+      double bytes = 4.0 * (m->nn + 1) + 8.0 * nen * m->ne + 8.0 * m->dim * m->nn + 8.0 * m->nn +
+                     4.0 * nen * nen * m->ne + 8.0 * node_fields * m->nn + 4.0 * (A->n + 1) +
+                     8.0 * A->nnz + 8.0 * A->n;
       int* worked = prof_begin();
       if (worked) OFG_CUDA(cudaMemsetAsync(worked, 1, sizeof(int), stream()));
-      launch(m->color_elems.p + beg, cnt, grid_for(cnt, 256, 16));
-      prof_end(PROF_ASSEMBLY, 0.0);
+      assemble_rows<Elem><<<grid_for(m->nn, 256, 16), 256, 0, stream()>>>(
+          m->nn, m->n2e_ptr.p, m->n2e.p, m->elem.p, m->dof.p, A->emap.p, A->row_ptr.p, el,
+          A->val.p, db, bad.p);
+      prof_end(PROF_ASSEMBLY, bytes);
       count_launch();
       OFG_LAUNCH_CHECK();
    }
+   matrix_touch(A);
+   check_jacobian(bad);
 }
+
+__global__ void insert_bc_kernel(int64_t nn, const int32_t* code, const int32_t* dof,
+                                 const double* x, const double* bc, double* u)
+{
+   int64_t stride = (int64_t)gridDim.x * blockDim.x;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += stride)
+      u[i] = code[i] == 0 ? x[dof[i] - 1] : (bc ? bc[i] : 0.0);
+}
+
+}  // namespace
 
 }  // namespace ofg
 
@@ -191,22 +236,10 @@ int ofg_assemble_p1(ofg_mesh* m, ofg_matrix* A, const double* kel, const double*
       OFG_REQUIRE(m && A && b, OFG_ERR_ARG, "null argument");
       In<double> dk(kel, m->ne), df(f, m->nn), dbc(bc, m->nn);
       InOut<double> db(b, A->n, false);
-      prepare(m, A, db.d);
-      DBuf<int> bad(1);
-      int big = INT32_MAX;
-      bad.upload(&big, 1);
-      for_each_color(m, [&](const int32_t* list, int64_t cnt, unsigned grid) {
-         if (m->dim == 2)
-            assemble_t3<<<grid, 256, 0, stream()>>>(cnt, list, m->elem.p, m->coords.p, m->code.p,
-                                                     m->dof.p, A->emap.p, dk.d, df.d, dbc.d,
-                                                     A->val.p, db.d, bad.p);
-         else
-            assemble_t4<<<grid, 256, 0, stream()>>>(cnt, list, m->elem.p, m->coords.p, m->code.p,
-                                                     m->dof.p, A->emap.p, dk.d, df.d, dbc.d,
-                                                     A->val.p, db.d, bad.p);
-      });
-      matrix_touch(A);
-      check_jacobian(bad);
+      if (m->dim == 2)
+         assemble(m, A, LaplaceT3{m->coords.p, m->code.p, dk.d, df.d, dbc.d}, db.d, f ? 1 : 0);
+      else
+         assemble(m, A, DiffusionT4{m->coords.p, m->code.p, dk.d, df.d, dbc.d}, db.d, f ? 1 : 0);
       db.finish();
    });
 }
@@ -220,18 +253,7 @@ int ofg_assemble_cd2d(ofg_mesh* m, ofg_matrix* A, double eps, const double* v, d
       OFG_REQUIRE(dt > 0, OFG_ERR_ARG, "time step must be positive");
       In<double> dv(v, 2 * m->nn), du(u_old, m->nn), dbc(bc, m->nn);
       InOut<double> db(b, A->n, false);
-      prepare(m, A, db.d);
-      DBuf<int> bad(1);
-      int big = INT32_MAX;
-      bad.upload(&big, 1);
-      double dti = 1. / dt;
-      for_each_color(m, [&](const int32_t* list, int64_t cnt, unsigned grid) {
-         assemble_cd2d<<<grid, 256, 0, stream()>>>(cnt, list, m->elem.p, m->coords.p, m->code.p,
-                                                    m->dof.p, A->emap.p, eps, dv.d, dti, du.d,
-                                                    dbc.d, A->val.p, db.d, bad.p);
-      });
-      matrix_touch(A);
-      check_jacobian(bad);
+      assemble(m, A, ConvDiffT3{m->coords.p, m->code.p, eps, 1. / dt, dv.d, du.d, dbc.d}, db.d, 3);
       db.finish();
    });
 }

@@ -915,6 +915,7 @@ int ofg_batch_create(int nprob, ofg_mesh* const* meshes, ofg_batch** out)
             P.nn = (int32_t)m->nn;
             P.ne = (int32_t)m->ne;
             P.n = (int32_t)mats[p]->n;
+            ensure_colors(m);
             P.ncolors = (int32_t)m->color_ptr.size() - 1;
             B->probs.push_back(P);
             B->nn += m->nn;

@@ -51,8 +51,9 @@ struct ofg_mesh {
    ofg::DBuf<int32_t> dof;    // nn, 1-based equation number or 0
    // node -> element adjacency (elements in ascending order)
    ofg::DBuf<int32_t> n2e_ptr, n2e;
-   // element colouring: elements of colour c are color_elems[color_ptr[c] ..
-   // color_ptr[c+1]); no two elements of one colour share a node
+   // element colouring (the batched solver's assembly; built by
+   // ofg::ensure_colors on first use): elements of colour c are
+   // color_elems[color_ptr[c] .. color_ptr[c+1]); no two share a node
    std::vector<int64_t> color_ptr;
    ofg::DBuf<int32_t> color_elems;
    // the structured rectangle's cells and line codes (rect_nx < 0 otherwise),
@@ -126,6 +127,8 @@ void spmv_csr(const ofg_matrix* A, const double* x, double* y, bool add);
 void spmv_sell(const ofg_matrix* A, const double* x, double* y, const int* skip = nullptr);
 void matrix_touch(ofg_matrix* A);
 void matrix_finish_pattern(ofg_matrix* A);
+// element colouring of a mesh, computed on first use (mesh.cu)
+void ensure_colors(ofg_mesh* m);
 void scan_exclusive_i64(const int64_t* d_in, int64_t* d_out, int64_t n);
 
 // prec.cu

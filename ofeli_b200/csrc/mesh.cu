@@ -268,8 +268,30 @@ void finish_mesh(ofg_mesh* m)
    count_launch();
    OFG_LAUNCH_CHECK();
 
-   // greedy colouring on the host: the colour of an element is the lowest
-   // one not yet used by any element touching one of its nodes
+   OFG_CUDA(cudaStreamSynchronize(stream()));
+}
+
+ofg_mesh* new_mesh(int dim, int64_t nn, int64_t ne)
+{
+   auto m = new ofg_mesh();
+   m->dim = dim;
+   m->nen = dim + 1;
+   m->nn = nn;
+   m->ne = ne;
+   m->coords.alloc(nn * dim > 0 ? nn * dim : 1);
+   m->elem.alloc(ne * m->nen > 0 ? ne * m->nen : 1);
+   m->code.alloc(nn > 0 ? nn : 1);
+   return m;
+}
+
+}  // namespace
+// Element colouring for the batched solver's block-level assembly (computed
+// on first use): greedy on the host, the colour of an element is the lowest
+// one not yet used by any element touching one of its nodes.
+void ensure_colors(ofg_mesh* m)
+{
+   if (!m->color_ptr.empty()) return;
+   const int64_t nn = m->nn, ne = m->ne;
    std::vector<int32_t> el = m->elem.to_host(ne * m->nen);
    std::vector<uint64_t> used(nn, 0);
    std::vector<int32_t> color(ne);
@@ -291,23 +313,9 @@ void finish_mesh(ofg_mesh* m)
    for (int64_t e = 0; e < ne; ++e) order[fillp[color[e]]++] = (int32_t)e;
    m->color_elems.alloc(ne > 0 ? ne : 1);
    if (ne) m->color_elems.upload(order.data(), ne);
-   OFG_CUDA(cudaStreamSynchronize(stream()));
+   OFG_CUDA(cudaStreamSynchronize(stream()));   // `order` is a pageable source
 }
 
-ofg_mesh* new_mesh(int dim, int64_t nn, int64_t ne)
-{
-   auto m = new ofg_mesh();
-   m->dim = dim;
-   m->nen = dim + 1;
-   m->nn = nn;
-   m->ne = ne;
-   m->coords.alloc(nn * dim > 0 ? nn * dim : 1);
-   m->elem.alloc(ne * m->nen > 0 ? ne * m->nen : 1);
-   m->code.alloc(nn > 0 ? nn : 1);
-   return m;
-}
-
-}  // namespace
 }  // namespace ofg
 
 using namespace ofg;
@@ -424,7 +432,7 @@ int ofg_mesh_info(const ofg_mesh* m, int* dim, int64_t* nn, int64_t* ne, int64_t
       if (nn) *nn = m->nn;
       if (ne) *ne = m->ne;
       if (neq) *neq = m->neq;
-      if (ncolors) *ncolors = (int)m->color_ptr.size() - 1;
+      if (ncolors) *ncolors = m->color_ptr.empty() ? 0 : (int)m->color_ptr.size() - 1;
    });
 }
 
