@@ -116,33 +116,26 @@ class Mesh {
       (void)bc;
       get(file);
    }
-   // Mesh::get(file) -- src/mesh/Mesh.cpp:2639-2668
+   // Mesh::get(file) -- src/mesh/Mesh.cpp:2639-2668, tokenised and converted
+   // on the device
    void get(const std::string& file)
    {
-      ofg_mesh_file* f = nullptr;
-      ofg_check(ofg_mesh_file_read(file.c_str(), &f), "Mesh::get");
       ofg_mesh* h = nullptr;
-      int rc = ofg_mesh_create_from_file(f, &h);
-      if (rc != OFG_OK) {
-         std::string msg = std::string("Mesh::get: ") + ofg_last_error();
-         ofg_mesh_file_destroy(f);
-         throw OFELIException(msg);
-      }
+      ofg_check(ofg_mesh_read(file.c_str(), &h), "Mesh::get");
       if (_h) ofg_mesh_destroy(_h);
-      if (_file) ofg_mesh_file_destroy(_file);
       _h = h;
-      _file = f;
+      _path = file;
       info();
    }
-   // Mesh::put(file) -- src/mesh/Mesh.cpp:2731-2806
+   // Mesh::put(file) -- src/mesh/Mesh.cpp:2731-2806; a mesh read from a file
+   // writes that file's content (read again on the host)
    void put(const std::string& file) const
    {
-      if (_file) {
-         ofg_check(ofg_mesh_file_write(_file, file.c_str()), "Mesh::put");
-         return;
-      }
       ofg_mesh_file* f = nullptr;
-      ofg_check(ofg_mesh_file_from_mesh(_h, &f), "Mesh::put");
+      if (!_path.empty())
+         ofg_check(ofg_mesh_file_read(_path.c_str(), &f), "Mesh::put");
+      else
+         ofg_check(ofg_mesh_file_from_mesh(_h, &f), "Mesh::put");
       int rc = ofg_mesh_file_write(f, file.c_str());
       std::string msg = rc != OFG_OK ? std::string("Mesh::put: ") + ofg_last_error() : "";
       ofg_mesh_file_destroy(f);
@@ -161,14 +154,13 @@ class Mesh {
    Mesh& operator=(Mesh&& o) noexcept
    {
       std::swap(_h, o._h);
-      std::swap(_file, o._file);
+      std::swap(_path, o._path);
       _dim = o._dim; _nn = o._nn; _ne = o._ne; _neq = o._neq;
       return *this;
    }
    ~Mesh()
    {
       if (_h) ofg_mesh_destroy(_h);
-      if (_file) ofg_mesh_file_destroy(_file);
    }
    size_t getDim() const { return (size_t)_dim; }
    size_t getNbNodes() const { return (size_t)_nn; }
@@ -180,7 +172,7 @@ class Mesh {
    explicit Mesh(ofg_mesh* h) : _h(h) { info(); }
    void info() { ofg_check(ofg_mesh_info(_h, &_dim, &_nn, &_ne, &_neq, nullptr), "Mesh"); }
    ofg_mesh* _h = nullptr;
-   ofg_mesh_file* _file = nullptr;   // the file a mesh was read from, kept for put()
+   std::string _path;   // the file a mesh was read from (put writes its content)
    int _dim = 0;
    int64_t _nn = 0, _ne = 0, _neq = 0;
 };

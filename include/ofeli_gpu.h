@@ -199,6 +199,13 @@ int ofg_mesh_file_set_threads(int n);
  * nb_dof 1), as Mesh(file, true) would number it: equations on the nodes
  * with code 0 (Mesh::NumberEquations, src/mesh/Mesh.cpp:1483-1510). */
 int ofg_mesh_create_from_file(const ofg_mesh_file* f, ofg_mesh** out);
+/* Mesh(file, true) straight onto the device: the same mesh as
+ * ofg_mesh_file_read + ofg_mesh_create_from_file (same values, same
+ * rejections), with the file's bytes copied to the device once and its
+ * Nodes / Elements / Sides texts tokenised and converted by kernels (rare
+ * coordinate forms are converted on the host).  Keeps a pinned staging
+ * buffer as large as the largest file read. */
+int ofg_mesh_read(const char* path, ofg_mesh** out);
 
 /* ------------------------------------------------------- preconditioners */
 /* Prec<real_t>(A, type) -- include/solvers/Prec_impl.h:164-195: DIAG

@@ -16,6 +16,9 @@ LIB = os.path.join(HERE, "libofeli_gpu.so")
 SOURCES = ["runtime.cu", "matrix.cu", "mesh.cu", "assembly.cu", "prec.cu", "krylov.cu", "mixed.cu",
            "noalloc.cu", "learned.cu", "batch.cu", "bicgstab.cu",
            "meshio.cu"]
+# per-source flags: the element arithmetic is kept free of fused multiply-adds
+# so that assembled values round exactly as OFELI's (separate multiply and add)
+EXTRA = {"assembly.cu": ["--fmad=false"]}
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
          "-Xcompiler", "-fPIC", "-Xcompiler", "-O2", "--expt-relaxed-constexpr"]
@@ -39,7 +42,7 @@ def _compile(src, verbose):
     deps = [os.path.join(CSRC, src)] + _headers()
     if not _needs(obj, deps):
         return obj
-    cmd = [NVCC] + FLAGS + ["-c", os.path.join(CSRC, src), "-o", obj]
+    cmd = [NVCC] + FLAGS + EXTRA.get(src, []) + ["-c", os.path.join(CSRC, src), "-o", obj]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)

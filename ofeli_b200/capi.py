@@ -67,6 +67,7 @@ SIGNATURES = {
     "ofg_mesh_file_destroy": (_i32, [_p]),
     "ofg_mesh_file_set_threads": (_i32, [_i32]),
     "ofg_mesh_create_from_file": (_i32, [_p, _pp]),
+    "ofg_mesh_read": (_i32, [ctypes.c_char_p, _pp]),
     "ofg_prec_create": (_i32, [_p, _i32, _pp]),
     "ofg_prec_destroy": (_i32, [_p]),
     "ofg_prec_update": (_i32, [_p]),

@@ -129,6 +129,11 @@ void matrix_touch(ofg_matrix* A);
 void matrix_finish_pattern(ofg_matrix* A);
 // element colouring of a mesh, computed on first use (mesh.cu)
 void ensure_colors(ofg_mesh* m);
+// a mesh with its coordinate, connectivity and code buffers allocated, and
+// the rest (equation numbers from the codes, node-to-element lists) built
+// once those hold the mesh (mesh.cu)
+ofg_mesh* new_mesh(int dim, int64_t nn, int64_t ne);
+void finish_mesh(ofg_mesh* m);
 void scan_exclusive_i64(const int64_t* d_in, int64_t* d_out, int64_t n);
 
 // prec.cu

@@ -228,6 +228,9 @@ __global__ void build_emap(int64_t ne, int nen, const int32_t* elem, const int32
    }
 }
 
+}  // namespace
+
+// Equation numbers, node-to-element lists (see internal.cuh).
 void finish_mesh(ofg_mesh* m)
 {
    int64_t nn = m->nn, ne = m->ne;
@@ -284,7 +287,6 @@ ofg_mesh* new_mesh(int dim, int64_t nn, int64_t ne)
    return m;
 }
 
-}  // namespace
 // Element colouring for the batched solver's block-level assembly (computed
 // on first use): greedy on the host, the colour of an element is the lowest
 // one not yet used by any element touching one of its nodes.

@@ -54,6 +54,7 @@
 #include <exception>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -275,6 +276,15 @@ struct Reader {
    std::string el_shape = "triangle", sd_shape = "line";
    int el_nodes = 0, sd_nodes = 2;
    bool have_nodes = false, have_elements = false, have_sides = false;
+   // device reading: data blocks are recorded here instead of converted
+   struct Deferred {
+      int kind;   // 0 Nodes, 1 Elements, 2 Sides
+      const char* s;
+      const char* e;
+      int per;    // nodes per element / side
+   };
+   std::vector<Deferred>* defer = nullptr;
+   bool defer_fallback = false;   // a layout the device reader leaves to the host reader
 
    void open(const std::string& name, const std::map<std::string, std::string>& attrs)
    {
@@ -318,8 +328,17 @@ struct Reader {
       OFG_REQUIRE(f->nb_dof >= 1 && f->nb_dof <= kMaxNbDof, OFG_ERR_ARG, "nb_dof must be 1..6");
    }
 
+   static bool data_tag(const std::string& t)
+   {
+      return t == "Nodes" || t == "nodes" || t == "Elements" || t == "elements" || t == "Sides" ||
+             t == "sides";
+   }
+
    void text(const char* s, const char* e)
    {
+      // data blocks check for '>' while they are tokenised
+      if (!(set_mesh && mesh_type && data_tag(tag)) && memchr(s, '>', size_t(e - s)))
+         throw Error(OFG_ERR_ARG, "XML: unexpected character '>' in text");
       if (tag == "Material" && set_mesh) {
          material(s, e);
          return;
@@ -352,8 +371,13 @@ struct Reader {
    {
       check_dims();
       OFG_REQUIRE(!have_nodes, OFG_ERR_ARG, "more than one Nodes text");
+      if (defer && (have_elements || have_sides)) defer_fallback = true;
       OFG_REQUIRE(f->ne == 0 && f->ns == 0, OFG_ERR_ARG, "Nodes must come before Elements and Sides");
       have_nodes = true;
+      if (defer) {
+         defer->push_back({0, s, e, 0});
+         return;
+      }
       const int dim = f->dim, nd = f->nb_dof, rec = dim + 1;
       Block blk(s, e, "Nodes");
       const int64_t n = blk.records(rec, "Nodes");
@@ -378,6 +402,10 @@ struct Reader {
       have_elements = true;
       f->el_shape = shape;
       f->el_nodes = el_nodes;
+      if (defer) {
+         defer->push_back({1, s, e, el_nodes});
+         return;
+      }
       const int k = el_nodes, rec = k + 1;
       const int64_t nn = f->nn;
       Block blk(s, e, "Elements");
@@ -407,6 +435,10 @@ struct Reader {
       have_sides = true;
       f->sd_shape = shape;
       f->sd_nodes = sd_nodes;
+      if (defer) {
+         defer->push_back({2, s, e, sd_nodes});
+         return;
+      }
       const int k = sd_nodes, rec = k + 1, nd = f->nb_dof;
       const int64_t nn = f->nn;
       Block blk(s, e, "Sides");
@@ -431,6 +463,26 @@ inline bool is_label(char c)
 {
    return (c >= 'a' && c <= 'z') || (c >= 'A' && c <= 'Z') || (c >= '0' && c <= '9') || c == '_' ||
           c == '-' || c == ':' || c == '.';
+}
+
+// memchr, with the bytes beyond the first MiB searched by a team of threads
+// (the end of a large data block).
+const char* find_char(const char* p, const char* e, char c)
+{
+   size_t n = size_t(e - p), head = size_t(1) << 20;
+   if (n <= head) return (const char*)memchr(p, c, n);
+   if (const char* q = (const char*)memchr(p, c, head)) return q;
+   const char* s = p + head;
+   size_t rest = size_t(e - s);
+   int T = team_size(rest);
+   std::vector<const char*> hit(T, nullptr);
+   parallel_for(T, [&](int t) {
+      size_t a = rest * size_t(t) / size_t(T), z = rest * size_t(t + 1) / size_t(T);
+      hit[t] = (const char*)memchr(s + a, c, z - a);
+   });
+   for (const char* h : hit)
+      if (h) return h;
+   return nullptr;
 }
 
 // xmlsp's blanks between and inside tags (a CR reads as a newline there).
@@ -472,10 +524,9 @@ void scan_xml(const char* b, const char* e, Reader& rd)
          if (*p != '<') fail("unexpected character outside tag");
       }
       else {
-         const char* lt = (const char*)memchr(p, '<', size_t(e - p));
+         const char* lt = find_char(p, e, '<');
          const char* te = lt ? lt : e;
          if (te > p) {
-            if (memchr(p, '>', size_t(te - p))) fail("unexpected character '>' in text");
             bool blank = true;
             for (const char* q = p; q < te && blank; ++q) blank = tag_space(*q);
             if (!blank) rd.text(p, te);
@@ -717,6 +768,430 @@ void put_file(const ofg_mesh_file* f, const char* path)
 
 }  // namespace
 
+namespace {
+
+using namespace ofg;
+
+// ------------------------------------------------------ device reading --
+// ofg_mesh_read: the file's bytes are read into a pinned staging buffer and
+// copied to the device once; the host walks the XML structure (tags are few)
+// and the Nodes / Elements / Sides texts are tokenised and converted by
+// kernels, straight into the device mesh's buffers.
+//
+// Tokenising: a 256-thread block covers a 4 KiB tile, one 16-byte aligned
+// load per thread; a byte starts a token when it is not blank and the byte
+// before it is (or the block starts there).  Pass 1 counts starts per tile,
+// a scan gives each tile its first token number, pass 2 recounts, scans the
+// threads' counts inside the block and converts every token it starts
+// (record = token / fields, field = token % fields).
+//
+// Coordinates: the token's decimal mantissa (up to 19 significant digits)
+// and exponent are parsed exactly; when the mantissa is below 2^53 and the
+// decimal exponent within +-22, M * 10^e (or M / 10^-e) is one correctly
+// rounded double operation, and rounding that double to float gives strtof's
+// result unless the double lies exactly on a float rounding midpoint.  Every
+// other token (a sign '+', hexadecimal, infinity, NaN, more digits, a wider
+// exponent, a midpoint, a result outside the normal float range) is listed
+// and converted on the host by the same conversion as ofg_mesh_file_read,
+// which also raises the errors std::stof would.  Integers convert exactly on
+// the device.  Errors are flagged by kind; the host reports them.
+
+constexpr int kParseThreads = 256;
+constexpr int kParseChunk = 16;
+constexpr int64_t kParseTile = kParseThreads * kParseChunk;
+enum : unsigned { PF_CHAR = 1, PF_INT = 2, PF_RANGE = 4, PF_LABEL = 8, PF_CODE = 16, PF_FULL = 32 };
+
+__device__ __forceinline__ bool dev_space(unsigned c) { return c == 32u || (c >= 9u && c <= 13u); }
+
+// Start bits of the 16 aligned bytes at a0 (positions outside [beg, end)
+// read as blanks).
+__device__ __forceinline__ unsigned token_starts(const char* buf, int64_t beg, int64_t end,
+                                                 int64_t a0, bool& bad)
+{
+   if (a0 >= end) return 0;
+   const uint4 w = *reinterpret_cast<const uint4*>(buf + a0);
+   const uint32_t word[4] = {w.x, w.y, w.z, w.w};
+   bool prev = (a0 - 1 < beg) ? true : dev_space((unsigned char)buf[a0 - 1]);
+   unsigned bits = 0;
+#pragma unroll
+   for (int i = 0; i < kParseChunk; ++i) {
+      const unsigned c = (word[i >> 2] >> (8 * (i & 3))) & 0xffu;
+      const int64_t q = a0 + i;
+      const bool inside = q >= beg && q < end;
+      const bool sp = !inside || dev_space(c);
+      bad |= inside && (c == '&' || c == '>');
+      if (!sp && prev) bits |= 1u << i;
+      prev = sp;
+   }
+   return bits;
+}
+
+__global__ void __launch_bounds__(kParseThreads) parse_count(const char* buf, int64_t beg, int64_t end,
+                                                             int64_t base, int64_t* tile_count,
+                                                             unsigned* flags)
+{
+   __shared__ int warp_sum[kParseThreads / 32];
+   const int64_t a0 = base + (int64_t)blockIdx.x * kParseTile + (int64_t)threadIdx.x * kParseChunk;
+   bool bad = false;
+   int n = __popc(token_starts(buf, beg, end, a0, bad));
+   if (bad) atomicOr(flags, PF_CHAR);
+#pragma unroll
+   for (int o = 16; o; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
+   if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = n;
+   __syncthreads();
+   if (threadIdx.x == 0) {
+      int t = 0;
+      for (int w = 0; w < kParseThreads / 32; ++w) t += warp_sum[w];
+      tile_count[blockIdx.x] = t;
+   }
+}
+
+// std::stoi of the token [p, q) (see to_int); 0 ok, else a PF_ kind.
+__device__ __forceinline__ unsigned dev_int(const char* buf, int64_t p, int64_t q, int32_t& v)
+{
+   bool neg = false;
+   if (p < q && (buf[p] == '+' || buf[p] == '-')) neg = buf[p++] == '-';
+   const int64_t d = p;
+   uint64_t x = 0;
+   while (p < q && buf[p] >= '0' && buf[p] <= '9') {
+      if (x > 1000000000000ull) return PF_RANGE;
+      x = x * 10 + uint64_t(buf[p] - '0');
+      ++p;
+   }
+   if (p == d) return PF_INT;
+   if (x > (neg ? 2147483648ull : 2147483647ull)) return PF_RANGE;
+   v = neg ? int32_t(-int64_t(x)) : int32_t(x);
+   return 0;
+}
+
+__constant__ double kPow10[23] = {1e0,  1e1,  1e2,  1e3,  1e4,  1e5,  1e6,  1e7,
+                                  1e8,  1e9,  1e10, 1e11, 1e12, 1e13, 1e14, 1e15,
+                                  1e16, 1e17, 1e18, 1e19, 1e20, 1e21, 1e22};
+
+// std::stof of the token [p, q) when the fast path above decides it; false
+// sends the token to the host.
+__device__ __forceinline__ bool dev_coord(const char* buf, int64_t p, int64_t q, double& v)
+{
+   bool neg = false;
+   if (p < q && buf[p] == '-') neg = true, ++p;
+   if (p + 1 < q && buf[p] == '0' && (buf[p + 1] == 'x' || buf[p + 1] == 'X')) return false;
+   uint64_t M = 0;
+   int nd = 0, dexp = 0;
+   bool any = false, lost = false;
+   while (p < q && buf[p] >= '0' && buf[p] <= '9') {
+      const int dg = buf[p++] - '0';
+      any = true;
+      if (M == 0 && dg == 0) continue;
+      if (nd < 19) M = M * 10 + uint64_t(dg), ++nd;
+      else ++dexp, lost |= dg != 0;
+   }
+   if (p < q && buf[p] == '.') {
+      ++p;
+      while (p < q && buf[p] >= '0' && buf[p] <= '9') {
+         const int dg = buf[p++] - '0';
+         any = true;
+         if (M == 0 && dg == 0) {
+            --dexp;
+            continue;
+         }
+         if (nd < 19) M = M * 10 + uint64_t(dg), ++nd, --dexp;
+         else lost |= dg != 0;
+      }
+   }
+   if (!any || lost) return false;
+   if (p < q && (buf[p] == 'e' || buf[p] == 'E')) {
+      int64_t j = p + 1;
+      bool eneg = false;
+      if (j < q && (buf[j] == '+' || buf[j] == '-')) eneg = buf[j++] == '-';
+      if (j < q && buf[j] >= '0' && buf[j] <= '9') {
+         int x = 0;
+         while (j < q && buf[j] >= '0' && buf[j] <= '9') {
+            if (x < 100000) x = x * 10 + (buf[j] - '0');
+            ++j;
+         }
+         dexp += eneg ? -x : x;
+      }
+   }
+   if (M == 0) {
+      v = neg ? -0.0 : 0.0;
+      return true;
+   }
+   if (M > (uint64_t(1) << 53) || dexp < -22 || dexp > 22) return false;
+   double d = dexp >= 0 ? __dmul_rn(double(M), kPow10[dexp]) : __ddiv_rn(double(M), kPow10[-dexp]);
+   if (!(d >= 1.1754943508222875e-38 && d <= 3.4028234663852886e38)) return false;
+   const float f = __double2float_rn(d);
+   const double fd = double(f);
+   if (fd != d) {
+      const int nb = __float_as_int(f) + (d > fd ? 1 : -1);   // the float neighbour on d's side
+      const double mid = 0.5 * (fd + double(__int_as_float(nb)));
+      if (mid == d) return false;
+   }
+   v = neg ? -fd : fd;
+   return true;
+}
+
+struct ParseOut {
+   int kind;              // 0 Nodes, 1 Elements, 2 Sides
+   int fields;            // tokens per record
+   int dim;               // Nodes: coordinates per record
+   int64_t nn;            // Elements / Sides: node labels must be in 1..nn
+   double* coords;        // Nodes
+   int32_t* code;         // Nodes (nb_dof 1: DOFCode gives |mark|)
+   int32_t* elem;         // Elements (0-based)
+   int64_t* fb_pos;       // coordinate tokens left to the host
+   int64_t* fb_out;
+   int fb_cap;
+   int* fb_count;
+};
+
+__global__ void __launch_bounds__(kParseThreads) parse_convert(const char* buf, int64_t beg, int64_t end,
+                                                               int64_t base, const int64_t* tile_off,
+                                                               ParseOut o, unsigned* flags)
+{
+   __shared__ int warp_sum[kParseThreads / 32];
+   const int64_t a0 = base + (int64_t)blockIdx.x * kParseTile + (int64_t)threadIdx.x * kParseChunk;
+   bool bad = false;
+   unsigned bits = token_starts(buf, beg, end, a0, bad);
+   const int n = __popc(bits);
+   // exclusive scan of the threads' counts
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   int incl = n;
+#pragma unroll
+   for (int k = 1; k < 32; k <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, k);
+      if (lane >= k) incl += y;
+   }
+   if (lane == 31) warp_sum[warp] = incl;
+   __syncthreads();
+   int before = 0;
+   for (int w = 0; w < warp; ++w) before += warp_sum[w];
+   int64_t g = tile_off[blockIdx.x] + before + incl - n;
+   unsigned err = 0;
+   while (bits) {
+      const int i = __ffs(bits) - 1;
+      bits &= bits - 1;
+      const int64_t p = a0 + i;
+      int64_t q = p;
+      while (q < end && !dev_space((unsigned char)buf[q])) ++q;
+      const int64_t r = g / o.fields;
+      const int fld = int(g - r * o.fields);
+      ++g;
+      if (o.kind == 0 && fld < o.dim) {
+         double x;
+         if (dev_coord(buf, p, q, x))
+            o.coords[r * o.dim + fld] = x;
+         else {
+            const int slot = atomicAdd(o.fb_count, 1);
+            if (slot < o.fb_cap) {
+               o.fb_pos[slot] = p;
+               o.fb_out[slot] = r * o.dim + fld;
+            }
+            else
+               err |= PF_FULL;
+         }
+         continue;
+      }
+      int32_t v = 0;
+      const unsigned st = dev_int(buf, p, q, v);
+      if (st) {
+         err |= st;
+         continue;
+      }
+      if (o.kind == 0) {   // node mark, nb_dof 1
+         if (v == INT32_MIN) err |= PF_CODE;
+         else o.code[r] = v < 0 ? -v : v;
+      }
+      else if (fld < o.fields - 1) {   // a node label
+         if (v < 1 || v > o.nn) err |= PF_LABEL;
+         else if (o.kind == 1) o.elem[r * (o.fields - 1) + fld] = v - 1;
+      }
+      else if (o.kind == 2 && v == INT32_MIN)
+         err |= PF_CODE;
+   }
+   if (bad) err |= PF_CHAR;
+   if (err) atomicOr(flags, err);
+}
+
+__global__ void scatter_values(int n, const int64_t* idx, const double* val, double* out)
+{
+   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+   if (i < n) out[idx[i]] = val[i];
+}
+
+// The pinned staging buffer, kept between reads (grown on demand).
+std::mutex g_pin_mu;
+char* g_pin = nullptr;
+size_t g_pin_cap = 0;
+
+char* pinned_staging(size_t n)
+{
+   if (n > g_pin_cap) {
+      if (g_pin) OFG_CUDA(cudaFreeHost(g_pin));
+      g_pin = nullptr;
+      g_pin_cap = 0;
+      OFG_CUDA(cudaHostAlloc((void**)&g_pin, n, cudaHostAllocDefault));
+      g_pin_cap = n;
+   }
+   return g_pin;
+}
+
+// The file into the staging buffer (parallel reads), NUL-terminated.
+size_t read_pinned(const char* path, char*& buf)
+{
+   int fd = ::open(path, O_RDONLY);
+   if (fd < 0) throw Error(OFG_ERR_ARG, std::string("cannot open ") + path);
+   struct stat st;
+   if (fstat(fd, &st) != 0) {
+      ::close(fd);
+      throw Error(OFG_ERR_ARG, std::string("cannot stat ") + path);
+   }
+   const size_t size = size_t(st.st_size);
+   try {
+      buf = pinned_staging(size + 1);
+      int T = team_size(size >> 2);
+      parallel_for(T, [&](int t) {
+         size_t a = size * size_t(t) / size_t(T), z = size * size_t(t + 1) / size_t(T);
+         while (a < z) {
+            ssize_t r = ::pread(fd, buf + a, z - a, off_t(a));
+            if (r <= 0) throw Error(OFG_ERR_ARG, std::string("read error on ") + path);
+            a += size_t(r);
+         }
+      });
+   }
+   catch (...) {
+      ::close(fd);
+      throw;
+   }
+   ::close(fd);
+   buf[size] = 0;
+   return size;
+}
+
+// Tokens of one block: tile counts and their exclusive scan; returns the total.
+int64_t count_tokens(const char* dbuf, int64_t beg, int64_t end, int64_t& base, int64_t& tiles,
+                     DBuf<int64_t>& off, unsigned* dflags)
+{
+   base = beg & ~int64_t(15);
+   tiles = (end - base + kParseTile - 1) / kParseTile;
+   DBuf<int64_t> cnt(tiles + 1);
+   off.alloc(tiles + 1);
+   OFG_CUDA(cudaMemsetAsync(cnt.p + tiles, 0, sizeof(int64_t), stream()));
+   parse_count<<<(unsigned)tiles, kParseThreads, 0, stream()>>>(dbuf, beg, end, base, cnt.p, dflags);
+   count_launch();
+   OFG_LAUNCH_CHECK();
+   scan_exclusive_i64(cnt.p, off.p, tiles + 1);
+   int64_t total = 0;
+   OFG_CUDA(cudaMemcpyAsync(&total, off.p + tiles, sizeof(int64_t), cudaMemcpyDeviceToHost, stream()));
+   OFG_CUDA(cudaStreamSynchronize(stream()));
+   return total;
+}
+
+void raise_parse_flags(unsigned fl)
+{
+   if (fl & PF_CHAR) throw Error(OFG_ERR_ARG, "unexpected '&' or '>' in mesh data");
+   if (fl & PF_INT) throw Error(OFG_ERR_ARG, "invalid integer token in mesh data");
+   if (fl & PF_RANGE) throw Error(OFG_ERR_ARG, "integer out of int range in mesh data");
+   if (fl & PF_CODE) throw Error(OFG_ERR_ARG, "code out of range");
+   if (fl & PF_LABEL) throw Error(OFG_ERR_ARG, "element or side names a node that does not exist");
+}
+
+// Mesh(file, true) on the device; false when the layout is left to the host
+// reader (blocks out of order, too many coordinates for the device path).
+bool read_device(const char* path, ofg_mesh** out)
+{
+   std::lock_guard<std::mutex> lock(g_pin_mu);
+   char* hb = nullptr;
+   const size_t size = read_pinned(path, hb);
+   DBuf<char> db(((size + 15) & ~size_t(15)) + 32);
+   if (size) OFG_CUDA(cudaMemcpyAsync(db.p, hb, size, cudaMemcpyHostToDevice, stream()));
+   ofg_mesh_file meta;
+   Reader rd{&meta};
+   std::vector<Reader::Deferred> blocks;
+   rd.defer = &blocks;
+   scan_xml(hb, hb + size, rd);
+   if (rd.defer_fallback) return false;
+   OFG_REQUIRE((meta.dim == 2 && meta.el_shape == SH_TRIANGLE && meta.el_nodes == 3) ||
+                   (meta.dim == 3 && meta.el_shape == SH_TETRA && meta.el_nodes == 4),
+               OFG_ERR_ARG, "the P1 path takes triangles in 2-D or tetrahedra in 3-D");
+   OFG_REQUIRE(meta.nb_dof == 1, OFG_ERR_ARG, "the P1 path takes meshes with one DOF per node");
+   DBuf<unsigned> dflags(1);
+   dflags.zero();
+   struct Counted {
+      const Reader::Deferred* d;
+      int64_t beg, end, base, tiles, ntok;
+      DBuf<int64_t> off;
+   };
+   std::vector<Counted> cb(blocks.size());
+   int64_t nn = 0, ne = 0;
+   for (size_t i = 0; i < blocks.size(); ++i) {
+      Counted& c = cb[i];
+      c.d = &blocks[i];
+      c.beg = blocks[i].s - hb;
+      c.end = blocks[i].e - hb;
+      c.ntok = count_tokens(db.p, c.beg, c.end, c.base, c.tiles, c.off, dflags.p);
+      const int fields = c.d->kind == 0 ? meta.dim + 1 : c.d->per + 1;
+      const char* what = c.d->kind == 0 ? "Nodes" : c.d->kind == 1 ? "Elements" : "Sides";
+      if (c.ntok % fields) throw Error(OFG_ERR_ARG, std::string(what) + " block ends inside a record");
+      if (c.d->kind == 0) nn = c.ntok / fields;
+      if (c.d->kind == 1) ne = c.ntok / fields;
+   }
+   OFG_REQUIRE(nn > 0 && ne > 0, OFG_ERR_ARG, "bad mesh arguments");
+   OFG_REQUIRE(ne * (meta.dim + 1) < (int64_t(1) << 31) && nn < (int64_t(1) << 31), OFG_ERR_SIZE,
+               "mesh too large");
+   std::unique_ptr<ofg_mesh> m(new_mesh(meta.dim, nn, ne));
+   const int fb_cap = int(std::min<int64_t>(nn * meta.dim, 1 << 20));
+   DBuf<int64_t> fb_pos(fb_cap), fb_out(fb_cap);
+   DBuf<int> fb_count(1);
+   fb_count.zero();
+   for (Counted& c : cb) {
+      if (c.tiles == 0) continue;
+      ParseOut o{};
+      o.kind = c.d->kind;
+      o.fields = c.d->kind == 0 ? meta.dim + 1 : c.d->per + 1;
+      o.dim = meta.dim;
+      o.nn = nn;
+      o.coords = m->coords.p;
+      o.code = m->code.p;
+      o.elem = m->elem.p;
+      o.fb_pos = fb_pos.p;
+      o.fb_out = fb_out.p;
+      o.fb_cap = fb_cap;
+      o.fb_count = fb_count.p;
+      parse_convert<<<(unsigned)c.tiles, kParseThreads, 0, stream()>>>(db.p, c.beg, c.end, c.base,
+                                                                       c.off.p, o, dflags.p);
+      count_launch();
+      OFG_LAUNCH_CHECK();
+   }
+   unsigned fl = 0;
+   int nfb = 0;
+   OFG_CUDA(cudaMemcpyAsync(&fl, dflags.p, sizeof(unsigned), cudaMemcpyDeviceToHost, stream()));
+   OFG_CUDA(cudaMemcpyAsync(&nfb, fb_count.p, sizeof(int), cudaMemcpyDeviceToHost, stream()));
+   OFG_CUDA(cudaStreamSynchronize(stream()));
+   raise_parse_flags(fl);
+   if (fl & PF_FULL) return false;
+   if (nfb > 0) {
+      std::vector<int64_t> pos = fb_pos.to_host(nfb);
+      std::vector<double> val(nfb);
+      for (int i = 0; i < nfb; ++i) {
+         const char* p = hb + pos[i];
+         const char* q = p;
+         while (q < hb + size && !is_space(*q)) ++q;
+         val[i] = to_coord(p, q);
+      }
+      DBuf<double> dval(nfb);
+      dval.upload(val.data(), nfb);
+      scatter_values<<<(nfb + 255) / 256, 256, 0, stream()>>>(nfb, fb_out.p, dval.p, m->coords.p);
+      count_launch();
+      OFG_LAUNCH_CHECK();
+      OFG_CUDA(cudaStreamSynchronize(stream()));   // val is a pageable source
+   }
+   finish_mesh(m.get());
+   *out = m.release();
+   return true;
+}
+
+}  // namespace
+
 extern "C" {
 
 int ofg_mesh_file_set_threads(int n)
@@ -867,6 +1342,21 @@ int ofg_mesh_file_write(const ofg_mesh_file* f, const char* path)
 int ofg_mesh_file_destroy(ofg_mesh_file* f)
 {
    return guarded("ofg_mesh_file_destroy", [&] { delete f; });
+}
+
+int ofg_mesh_read(const char* path, ofg_mesh** out)
+{
+   return guarded("ofg_mesh_read", [&] {
+      OFG_REQUIRE(path && out, OFG_ERR_ARG, "null argument");
+      if (read_device(path, out)) return;
+      // layouts left to the host reader: read, then hand over
+      ofg_mesh_file* f = nullptr;
+      int rc = ofg_mesh_file_read(path, &f);
+      if (rc != OFG_OK) throw Error(rc, ofg_last_error());
+      std::unique_ptr<ofg_mesh_file> keep(f);
+      rc = ofg_mesh_create_from_file(f, out);
+      if (rc != OFG_OK) throw Error(rc, ofg_last_error());
+   });
 }
 
 int ofg_mesh_create_from_file(const ofg_mesh_file* f, ofg_mesh** out)

@@ -128,11 +128,13 @@ class Mesh:
     @classmethod
     def from_file(cls, path):
         """Mesh(file, true): a P1 mesh read from OFELI's XML format, equations
-        on the code-0 nodes.  The file's data (sides, element codes) is kept
-        for put()."""
-        mf = MeshFile(path)
-        m = mf.to_mesh()
-        m._file = mf
+        on the code-0 nodes, tokenised and converted on the device
+        (ofg_mesh_read).  put() writes the file's own content (sides,
+        element codes), read again from `path` on the host when asked."""
+        h = ctypes.c_void_p()
+        _call("ofg_mesh_read", str(path).encode(), ctypes.byref(h))
+        m = cls(_handle=h)
+        m._path = str(path)
         return m
 
     def get(self, path):
@@ -140,13 +142,16 @@ class Mesh:
         m = Mesh.from_file(path)
         old = getattr(self, "_h", None)
         self._h, m._h = m._h, old
-        self._file = m._file
+        self._path, self._file = m._path, None
         self._coords_changed = False
         self._info()
 
     def put(self, path):
         """Mesh::put(file) (src/mesh/Mesh.cpp:2731-2806)."""
         mf = getattr(self, "_file", None)
+        if mf is None and getattr(self, "_path", None) and not getattr(self, "_coords_changed",
+                                                                      False):
+            mf = self._file = MeshFile(self._path)
         if mf is None or getattr(self, "_coords_changed", False):
             mf = MeshFile.from_mesh(self)
         mf.put(path)
