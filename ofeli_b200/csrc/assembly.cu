@@ -10,15 +10,17 @@
 // contributions in OFELI's element-loop order, starting from zero, so the
 // assembled values are the reference's bit for bit on any mesh; a thread
 // writes only its own row, so there are no atomics and no element colouring.
-// Each element is computed once per node (3 or 4 times); the FP64 arithmetic
-// is cheap beside the memory traffic.  An element's Jacobian is checked by
+// Each node computes only its own row of an element (geometry is recomputed
+// by each of the element's 3 or 4 nodes; the FP64 arithmetic is cheap beside
+// the gathers).  An element's Jacobian is checked by
 // the thread of its first node, equation or not, and the lowest bad element
 // is reported as OFELI's element loop would meet it first.
 //
 // Algorithmic bytes per launch: node-to-element lists 4*(nn+1) + 4*nen*ne,
 // connectivity 4*nen*ne, coordinates 8*dim*nn, code and equation number
-// 8*nn, the element-to-CSR map 4*nen^2*ne, k 8*ne, the node fields read
-// (f, or u_old and v) 8*nn each, CSR row pointers 4*(n+1), A written 8*nnz,
+// 8*nn, the element-to-CSR map 4*nen^2*ne, the node fields read
+// (f, or u_old and v) 8*nn each, k 8*ne when given, CSR row pointers
+// 4*(n+1), A written 8*nnz,
 // b written 8*n.
 #include "element.cuh"
 
@@ -26,6 +28,35 @@ namespace ofg {
 namespace {
 
 using namespace elem;
+
+// Each element kind computes row li of its element matrix and RHS -- the row
+// of the thread's own node i = en[li] -- with the arithmetic of the full
+// element computation (the same products and sums in the same order), and
+// lifts imposed values as Equation::updateBC does
+// (include/equations/Equation_impl.h:160-176): a column j whose DOF is
+// imposed (CSR position -1 in the element map) with code > 0 subtracts
+// Ke(li, j) * bc(en[j]).  Only the node's own source value and the imposed
+// columns' codes and values are loaded.
+
+template <int NEN>
+__device__ __forceinline__ void lift_row(const int32_t (&en)[NEN], const int32_t (&pos)[NEN],
+                                         const int32_t* code, const double* bc,
+                                         const double (&krow)[NEN], double& frow)
+{
+#pragma unroll
+   for (int j = 0; j < NEN; ++j)
+      if (pos[j] < 0 && code[en[j]] > 0) frow -= krow[j] * bc[en[j]];
+}
+
+// g[li] without dynamic register indexing
+template <int NEN>
+__device__ __forceinline__ void gradient_of(const double (&g)[NEN][3], int li, double (&gl)[3])
+{
+   gl[0] = g[0][0], gl[1] = g[0][1], gl[2] = g[0][2];
+#pragma unroll
+   for (int t = 1; t < NEN; ++t)
+      if (t == li) gl[0] = g[t][0], gl[1] = g[t][1], gl[2] = g[t][2];
+}
 
 // Laplace2DT3::LHS (times k) + BodyRHS: Ke = area*(g_i.g_j)*k, Fe = f*area/3
 // (src/equations/laplace/Laplace2DT3.cpp:131-143)
@@ -36,19 +67,23 @@ struct LaplaceT3 {
    const double* kel;
    const double* f;
    const double* bc;
-   __device__ __forceinline__ bool operator()(int64_t e, const int32_t (&en)[3], double (&Ke)[3][3],
-                                              double (&Fe)[3]) const
+   __device__ __forceinline__ bool geometry_ok(const int32_t (&en)[3]) const
    {
       double g[3][3], area;
+      return tri3(xy, en, g, area);
+   }
+   __device__ __forceinline__ bool row(int64_t e, const int32_t (&en)[3], int li, int64_t node,
+                                       const int32_t (&pos)[3], double (&krow)[3],
+                                       double& frow) const
+   {
+      double g[3][3], area, gl[3];
       if (!tri3(xy, en, g, area)) return false;
-      double k = kel ? kel[e] : 1.0;
+      gradient_of<3>(g, li, gl);
+      const double k = kel ? kel[e] : 1.0;
 #pragma unroll
-      for (int i = 0; i < 3; ++i)
-#pragma unroll
-         for (int j = 0; j < 3; ++j) Ke[i][j] = area * dot3(g[i], g[j]) * k;
-#pragma unroll
-      for (int i = 0; i < 3; ++i) Fe[i] = f ? f[en[i]] * area * kThird : 0.0;
-      if (bc) lift_bc<3>(en, code, bc, Ke, Fe);
+      for (int j = 0; j < 3; ++j) krow[j] = area * dot3(gl, g[j]) * k;
+      frow = f ? f[node] * area * kThird : 0.0;
+      if (bc) lift_row<3>(en, pos, code, bc, krow, frow);
       return true;
    }
 };
@@ -62,19 +97,23 @@ struct DiffusionT4 {
    const double* kel;
    const double* f;
    const double* bc;
-   __device__ __forceinline__ bool operator()(int64_t e, const int32_t (&en)[4], double (&Ke)[4][4],
-                                              double (&Fe)[4]) const
+   __device__ __forceinline__ bool geometry_ok(const int32_t (&en)[4]) const
    {
       double g[4][3], vol;
+      return tet4(xyz, en, g, vol);
+   }
+   __device__ __forceinline__ bool row(int64_t e, const int32_t (&en)[4], int li, int64_t node,
+                                       const int32_t (&pos)[4], double (&krow)[4],
+                                       double& frow) const
+   {
+      double g[4][3], vol, gl[3];
       if (!tet4(xyz, en, g, vol)) return false;
-      double c = (kel ? kel[e] : 1.0) * vol;
+      gradient_of<4>(g, li, gl);
+      const double c = (kel ? kel[e] : 1.0) * vol;
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-         for (int j = 0; j < 4; ++j) Ke[i][j] = c * dot3(g[i], g[j]);
-#pragma unroll
-      for (int i = 0; i < 4; ++i) Fe[i] = f ? f[en[i]] * 0.25 * vol : 0.0;
-      if (bc) lift_bc<4>(en, code, bc, Ke, Fe);
+      for (int j = 0; j < 4; ++j) krow[j] = c * dot3(gl, g[j]);
+      frow = f ? f[node] * 0.25 * vol : 0.0;
+      if (bc) lift_row<4>(en, pos, code, bc, krow, frow);
       return true;
    }
 };
@@ -91,30 +130,32 @@ struct ConvDiffT3 {
    const double* v;
    const double* u_old;
    const double* bc;
-   __device__ __forceinline__ bool operator()(int64_t, const int32_t (&en)[3], double (&Ke)[3][3],
-                                              double (&Fe)[3]) const
+   __device__ __forceinline__ bool geometry_ok(const int32_t (&en)[3]) const
    {
       double g[3][3], area;
+      return tri3(xy, en, g, area);
+   }
+   __device__ __forceinline__ bool row(int64_t, const int32_t (&en)[3], int li, int64_t,
+                                       const int32_t (&pos)[3], double (&krow)[3],
+                                       double& frow) const
+   {
+      double g[3][3], area, gl[3];
       if (!tri3(xy, en, g, area)) return false;
-      double cc = kSixth * area, dd = 0.5 * cc, cl = kThird * area;
-      double v3[3] = {v[2 * en[0]] + v[2 * en[1]] + v[2 * en[2]],
-                      v[2 * en[0] + 1] + v[2 * en[1] + 1] + v[2 * en[2] + 1], 0.0};
-      double cv = kThird * kThird * area;
-      double M1[3][3];
+      gradient_of<3>(g, li, gl);
+      const double cc = kSixth * area, dd = 0.5 * cc, cl = kThird * area;
+      const double v3[3] = {v[2 * en[0]] + v[2 * en[1]] + v[2 * en[2]],
+                            v[2 * en[0] + 1] + v[2 * en[1] + 1] + v[2 * en[2] + 1], 0.0};
+      const double cv = kThird * kThird * area;
+      double m1row[3];
 #pragma unroll
-      for (int i = 0; i < 3; ++i)
-#pragma unroll
-         for (int j = 0; j < 3; ++j) {
-            double m1 = (i == j) ? cc + cl : dd;
-            M1[i][j] = dti * m1;
-            Ke[i][j] = M1[i][j] + (eps * area * dot3(g[i], g[j]) + cv * dot3(v3, g[j]));
-         }
-#pragma unroll
-      for (int i = 0; i < 3; ++i) Fe[i] = 0.0;
-      if (bc) lift_bc<3>(en, code, bc, Ke, Fe);
-#pragma unroll
-      for (int i = 0; i < 3; ++i)
-         Fe[i] += M1[i][0] * u_old[en[0]] + M1[i][1] * u_old[en[1]] + M1[i][2] * u_old[en[2]];
+      for (int j = 0; j < 3; ++j) {
+         const double m1 = (li == j) ? cc + cl : dd;
+         m1row[j] = dti * m1;
+         krow[j] = m1row[j] + (eps * area * dot3(gl, g[j]) + cv * dot3(v3, g[j]));
+      }
+      frow = 0.0;
+      if (bc) lift_row<3>(en, pos, code, bc, krow, frow);
+      frow += m1row[0] * u_old[en[0]] + m1row[1] * u_old[en[1]] + m1row[2] * u_old[en[2]];
       return true;
    }
 };
@@ -148,30 +189,22 @@ __global__ void __launch_bounds__(256) assemble_rows(int64_t nn, const int32_t* 
 #pragma unroll
          for (int j = NEN - 1; j > 0; --j)
             if (en[j] == (int32_t)i) li = j;
-         if (!r && li != 0) continue;   // no row here: only the Jacobian check of led elements
-         double Ke[NEN][NEN], Fe[NEN];
-         if (!el(e, en, Ke, Fe)) {
+         if (!r) {   // no row here: only the Jacobian check of the elements it leads
+            if (li == 0 && !el.geometry_ok(en)) atomicMin(bad, (int)e);
+            continue;
+         }
+         int32_t pos[NEN];
+         const int32_t* mp = emap + (e * NEN + li) * NEN;
+#pragma unroll
+         for (int j = 0; j < NEN; ++j) pos[j] = mp[j];
+         double krow[NEN], frow;
+         if (!el.row(e, en, li, i, pos, krow, frow)) {
             if (li == 0) atomicMin(bad, (int)e);
             continue;
          }
-         if (!r) continue;
-         // row li of the element, selected without dynamic register indexing
-         double krow[NEN], frow = 0.0;
 #pragma unroll
-         for (int j = 0; j < NEN; ++j) krow[j] = 0.0;
-#pragma unroll
-         for (int t = 0; t < NEN; ++t)
-            if (t == li) {
-#pragma unroll
-               for (int j = 0; j < NEN; ++j) krow[j] = Ke[t][j];
-               frow = Fe[t];
-            }
-         const int32_t* mp = emap + (e * NEN + li) * NEN;
-#pragma unroll
-         for (int j = 0; j < NEN; ++j) {
-            const int32_t pos = mp[j];
-            if (pos >= 0) a[pos] += krow[j];
-         }
+         for (int j = 0; j < NEN; ++j)
+            if (pos[j] >= 0) a[pos[j]] += krow[j];
          bi += frow;
       }
       if (r) b[r - 1] = bi;
@@ -189,7 +222,8 @@ void check_jacobian(const DBuf<int>& bad)
 
 // Launches the row-gather kernel for one element kind and checks Jacobians.
 template <class Elem>
-void assemble(ofg_mesh* m, ofg_matrix* A, const Elem& el, double* db, int node_fields)
+void assemble(ofg_mesh* m, ofg_matrix* A, const Elem& el, double* db, int node_fields,
+              int elem_fields)
 {
    OFG_REQUIRE(A->mesh == m, OFG_ERR_ARG, "matrix pattern was not built from this mesh");
    DBuf<int> bad(1);
@@ -198,7 +232,8 @@ void assemble(ofg_mesh* m, ofg_matrix* A, const Elem& el, double* db, int node_f
    if (m->nn) {
       const int nen = m->nen;
       double bytes = 4.0 * (m->nn + 1) + 8.0 * nen * m->ne + 8.0 * m->dim * m->nn + 8.0 * m->nn +
-                     4.0 * nen * nen * m->ne + 8.0 * node_fields * m->nn + 4.0 * (A->n + 1) +
+                     4.0 * nen * nen * m->ne + 8.0 * node_fields * m->nn +
+                     8.0 * elem_fields * m->ne + 4.0 * (A->n + 1) +
                      8.0 * A->nnz + 8.0 * A->n;
       int* worked = prof_begin();
       if (worked) OFG_CUDA(cudaMemsetAsync(worked, 1, sizeof(int), stream()));
@@ -237,9 +272,11 @@ int ofg_assemble_p1(ofg_mesh* m, ofg_matrix* A, const double* kel, const double*
       In<double> dk(kel, m->ne), df(f, m->nn), dbc(bc, m->nn);
       InOut<double> db(b, A->n, false);
       if (m->dim == 2)
-         assemble(m, A, LaplaceT3{m->coords.p, m->code.p, dk.d, df.d, dbc.d}, db.d, f ? 1 : 0);
+         assemble(m, A, LaplaceT3{m->coords.p, m->code.p, dk.d, df.d, dbc.d}, db.d, f ? 1 : 0,
+                  kel ? 1 : 0);
       else
-         assemble(m, A, DiffusionT4{m->coords.p, m->code.p, dk.d, df.d, dbc.d}, db.d, f ? 1 : 0);
+         assemble(m, A, DiffusionT4{m->coords.p, m->code.p, dk.d, df.d, dbc.d}, db.d, f ? 1 : 0,
+                  kel ? 1 : 0);
       db.finish();
    });
 }
@@ -253,7 +290,8 @@ int ofg_assemble_cd2d(ofg_mesh* m, ofg_matrix* A, double eps, const double* v, d
       OFG_REQUIRE(dt > 0, OFG_ERR_ARG, "time step must be positive");
       In<double> dv(v, 2 * m->nn), du(u_old, m->nn), dbc(bc, m->nn);
       InOut<double> db(b, A->n, false);
-      assemble(m, A, ConvDiffT3{m->coords.p, m->code.p, eps, 1. / dt, dv.d, du.d, dbc.d}, db.d, 3);
+      assemble(m, A, ConvDiffT3{m->coords.p, m->code.p, eps, 1. / dt, dv.d, du.d, dbc.d}, db.d, 3,
+               0);
       db.finish();
    });
 }

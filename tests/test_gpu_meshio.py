@@ -3,9 +3,10 @@ with the 2-D Laplace and 3-D diffusion problems, against the reference
 OFELI run on the same files (golden outputs in tests/golden/meshio.npz),
 and Mesh::put of device meshes.
 
-Bars as in the other parity tests: CSR pattern bit-exact; values, RHS and
-solutions within 1e-12 relative (BiCGStab solutions 1e-8); iteration counts
-within +-2; put output byte-identical."""
+Bars as in the other parity tests: CSR pattern, assembled values and RHS
+bit-exact; solutions within 1e-12 relative (BiCGStab solutions 1e-8);
+iteration counts within +-2; put output byte-identical; the device reader's
+mesh bit-identical to the host reader's."""
 import os
 
 import numpy as np
@@ -17,7 +18,6 @@ from ofeli_b200 import ofeli as F
 
 pytestmark = pytest.mark.gpu
 
-VAL_TOL = 1e-12
 SOL_TOL = 1e-12
 BICG_SOL_TOL = 1e-8
 IT_TOL = 2
@@ -58,8 +58,8 @@ def test_file_mesh_assembly(cuda, golden, key):
     A = eq.getMatrix()
     rp, ci = A.pattern()
     assert np.array_equal(rp, g[key + "_row_ptr"]) and np.array_equal(ci, g[key + "_col_ind"])
-    assert rel_err(A.values(), g[key + "_a"]) <= VAL_TOL
-    assert rel_err(eq.getRHS(), g[key + "_b"]) <= VAL_TOL
+    assert np.array_equal(A.values(), g[key + "_a"])
+    assert np.array_equal(eq.getRHS(), g[key + "_b"])
 
 
 @pytest.mark.parametrize("run", ["ring_CG_DILU", "ring_CG_DIAG", "ring_BICGSTAB_ILU",
