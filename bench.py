@@ -75,6 +75,9 @@ def parse():
                     help="transient2d: GMRES(30) preconditioner of the timed steps (the plain "
                          "ILU form is timed beside it)")
     ap.add_argument("--m3d", type=int, default=128, help="kuhn3d cells per side")
+    ap.add_argument("--mf-n", type=int, default=1024,
+                    help="meshfile2d: circles and nodes per circle of the annulus (the workload "
+                         "is 1024; smaller sizes are for profiling captures)")
     ap.add_argument("--inner-bits", type=int, default=32, choices=[32, 16])
     ap.add_argument("--prec", default="learned", choices=["jacobi", "learned"],
                     help="preconditioner of the FP32 inner iteration (learned: the network is "
@@ -1088,7 +1091,7 @@ def run_meshfile(args):
     capi.call("ofg_set_stream", ctypes.c_void_p(work_stream.cuda_stream))
     dev = torch.device("cuda", local)
     P_ = F._ptr
-    path, code, t_put = meshfile_write(MF_N, seed=SEED + rank)
+    path, code, t_put = meshfile_write(args.mf_n, seed=SEED + rank)
     size = os.path.getsize(path)
     mf0 = F.MeshFile(path)
     a0 = mf0.arrays()
