@@ -69,6 +69,9 @@ def parse():
     ap.add_argument("--nprob", type=int, default=1024,
                     help="batch2d: number of problems (the workload is 1024; smaller counts are "
                          "for profiling captures)")
+    ap.add_argument("--shard", action="store_true",
+                    help="batch2d with N > 1: split the problem list over the ranks by estimated "
+                         "cost (strong scaling) instead of one replica of it per rank")
     ap.add_argument("--batch-bits", type=int, default=32, choices=[32, 64],
                     help="batch2d: inner CG precision (32: FP32 CG inside FP64 refinement)")
     ap.add_argument("--tprec", default="DIAG", choices=["ILU", "DIAG"],
@@ -272,18 +275,12 @@ def run_ours(args):
     from ofeli_b200 import capi, fields
     from ofeli_b200 import ofeli as F
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from ofeli_b200 import ranks
+    world, rank, local = ranks.env()
     if not torch.cuda.is_available():
         raise SystemExit("bench.py needs a CUDA device")
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+    R = ranks.Ranks("nccl", torch.device("cuda", local))
     L = capi.lib()
     # one stream for torch and the library: ordering without extra syncs
     work_stream = torch.cuda.Stream(device=torch.device("cuda", local))
@@ -350,16 +347,9 @@ def run_ours(args):
         capi.call("ofg_insert_bc", mesh._h, P(x_dev), None, P(u_pin))
         return o, i, r
 
-    def barrier():
-        if dist:
-            dist.barrier()
+    barrier = R.barrier
 
-    def max_over_ranks(v):
-        if not dist:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    max_over_ranks = R.max
 
     for _ in range(args.warmup):
         step_device()
@@ -485,8 +475,7 @@ def run_ours(args):
     spmv64_bytes = 12.0 * A.nnz + 20.0 * n + 4.0
 
     if rank != 0:
-        if dist:
-            dist.destroy_process_group()
+        R.close()
         return 0
 
     peak, peak_kind = measured_peaks()
@@ -540,8 +529,7 @@ def run_ours(args):
     if plain:
         line["plain"]["solves_per_s"] = 1.0 / plain["solve_s"]
     print(json.dumps(line))
-    if dist:
-        dist.destroy_process_group()
+    R.close()
     return 0
 
 
@@ -605,23 +593,21 @@ def run_batch(args):
     from ofeli_b200 import capi, problems
     from ofeli_b200 import ofeli as F
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from ofeli_b200 import ranks
+    world, rank, local = ranks.env()
     if not torch.cuda.is_available():
         raise SystemExit("bench.py needs a CUDA device")
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+    R = ranks.Ranks("nccl", torch.device("cuda", local))
     work_stream = torch.cuda.Stream(device=torch.device("cuda", local))
     torch.cuda.set_stream(work_stream)
     capi.call("ofg_set_stream", ctypes.c_void_p(work_stream.cuda_stream))
     dev = torch.device("cuda", local)
-    meshes, k_host, f_host = problems.uneven_batch(SEED, count=args.nprob)
+    shard = args.shard and world > 1
+    mine = None
+    if shard:
+        mine = problems.partition_by_cost(problems.batch_costs(SEED, args.nprob), world)[rank]
+    meshes, k_host, f_host = problems.uneven_batch(SEED, count=args.nprob, indices=mine)
     sizes = problems.uneven_sizes(SEED, count=args.nprob)
     B = F.Batch(meshes)
     info = B.problem_info()
@@ -634,16 +620,9 @@ def run_batch(args):
     tune_s = time.perf_counter() - t0
     shape = F.Batch.config_shape(chosen)
 
-    def barrier():
-        if dist:
-            dist.barrier()
+    barrier = R.barrier
 
-    def max_over_ranks(v):
-        if not dist:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    max_over_ranks = R.max
 
     for _ in range(args.warmup):
         B.solve(100000, TOL)
@@ -734,17 +713,20 @@ def run_batch(args):
         del mats
 
     if rank != 0:
-        if dist:
-            dist.destroy_process_group()
+        R.close()
         return 0
     peak, peak_kind = measured_peaks()
     nbytes = batch_bytes(info, iters, bits=args.batch_bits)
     achieved = nbytes / (ms / args.steps * 1e-3) / 1e9
     cpu = cpu_baseline_batch(sizes, iters, info) if world == 1 else None
+    # problems solved per step by the whole job: the list once when sharded,
+    # a replica of it per rank otherwise
+    jobs = args.nprob if shard else world * B.nprob
     line = {
-        "metric": METRIC_BATCH, "value": world * args.steps * B.nprob / (ms / 1e3),
+        "metric": METRIC_BATCH, "value": jobs * args.steps / (ms / 1e3),
         "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "strong" if shard else "weak",
         "vs_baseline": None,
         "dtype": "f64" if args.batch_bits == 64 else "f64 (assembly, refinement, true residual, "
                  "dots) / f32 (inner CG)", "data": "synthetic",
@@ -761,7 +743,7 @@ def run_batch(args):
                    "iterations": {"min": int(iters.min()), "mean": float(iters.mean()),
                                   "max": int(iters.max())}},
         "gpu_launches": launches,
-        "e2e": {"value": world * args.steps * B.nprob / (e2e_ms / 1e3), "unit": UNIT,
+        "e2e": {"value": jobs * args.steps / (e2e_ms / 1e3), "unit": UNIT,
                 "h2d_bytes_per_step": 8 * (B.elements + B.nodes),
                 "d2h_bytes_per_step": 8 * B.nodes},
         "roofline": {"kernel": "batch_kernel (assembly + CG + DIAG, every problem)",
@@ -774,8 +756,7 @@ def run_batch(args):
         "clocks": clk,
     }
     print(json.dumps(line))
-    if dist:
-        dist.destroy_process_group()
+    R.close()
     return 0
 
 
@@ -835,18 +816,12 @@ def run_transient(args):
     from ofeli_b200 import capi
     from ofeli_b200 import ofeli as F
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from ofeli_b200 import ranks
+    world, rank, local = ranks.env()
     if not torch.cuda.is_available():
         raise SystemExit("bench.py needs a CUDA device")
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+    R = ranks.Ranks("nccl", torch.device("cuda", local))
     work_stream = torch.cuda.Stream(device=torch.device("cuda", local))
     torch.cuda.set_stream(work_stream)
     capi.call("ofg_set_stream", ctypes.c_void_p(work_stream.cuda_stream))
@@ -876,9 +851,7 @@ def run_transient(args):
         its.append(it)
         return it
 
-    def barrier():
-        if dist:
-            dist.barrier()
+    barrier = R.barrier
 
     for _ in range(args.warmup):
         step(u_dev, u_dev)
@@ -898,11 +871,7 @@ def run_transient(args):
     e1.record(work_stream)
     torch.cuda.synchronize()
     barrier()
-    ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = R.max(e0.elapsed_time(e1))
     clk = clocks.stop()
     launches = capi.launch_count() - launches0
     if any(i <= 0 for i in its):
@@ -931,7 +900,7 @@ def run_transient(args):
         step(u_pin, u_pin)
     g1.record(work_stream)
     torch.cuda.synchronize()
-    e2e_ms = max(g0.elapsed_time(g1), (time.perf_counter() - t0) * 1e3)
+    e2e_ms = R.max(max(g0.elapsed_time(g1), (time.perf_counter() - t0) * 1e3))
     # the plain form (OFELI's GMRES(30) + ILU) over 10 steps from the same
     # initial state
     plain = None
@@ -952,8 +921,7 @@ def run_transient(args):
                  "gmres_iterations_per_step": statistics.mean(its[1:]),
                  "true_rel_residual": F.residual(A, b_dev, x_dev)}
     if rank != 0:
-        if dist:
-            dist.destroy_process_group()
+        R.close()
         return 0
     cpu = cpu_baseline_transient() if world == 1 else None
     peak, peak_kind = measured_peaks()
@@ -990,8 +958,7 @@ def run_transient(args):
         "clocks": clk,
     }
     print(json.dumps(line))
-    if dist:
-        dist.destroy_process_group()
+    R.close()
     return 0
 
 
@@ -1074,18 +1041,12 @@ def run_meshfile(args):
     from ofeli_b200 import capi, fields
     from ofeli_b200 import ofeli as F
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from ofeli_b200 import ranks
+    world, rank, local = ranks.env()
     if not torch.cuda.is_available():
         raise SystemExit("bench.py needs a CUDA device")
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+    R = ranks.Ranks("nccl", torch.device("cuda", local))
     work_stream = torch.cuda.Stream(device=torch.device("cuda", local))
     torch.cuda.set_stream(work_stream)
     capi.call("ofg_set_stream", ctypes.c_void_p(work_stream.cuda_stream))
@@ -1128,9 +1089,7 @@ def run_meshfile(args):
         capi.call("ofg_assemble_p1", m._h, A._h, None, P_(f_pin), P_(bc_pin), P_(b_pin))
         del A, m
 
-    def barrier():
-        if dist:
-            dist.barrier()
+    barrier = R.barrier
 
     def timed(fn, k):
         barrier()
@@ -1145,11 +1104,7 @@ def run_meshfile(args):
         torch.cuda.synchronize()
         ms = max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3)
         barrier()
-        if dist:
-            t = torch.tensor([ms], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return R.max(ms)
 
     for _ in range(args.warmup):
         step_device()
@@ -1192,8 +1147,7 @@ def run_meshfile(args):
     del A, m
     os.remove(path)
     if rank != 0:
-        if dist:
-            dist.destroy_process_group()
+        R.close()
         return 0
     cpu = None
     if world == 1:
@@ -1241,8 +1195,7 @@ def run_meshfile(args):
         "clocks": clk,
     }
     print(json.dumps(line))
-    if dist:
-        dist.destroy_process_group()
+    R.close()
     return 0
 
 

@@ -25,11 +25,34 @@ def uneven_sizes(seed, count=1024, nmin=1000, nmax=64000):
     return np.maximum(2, np.rint(np.sqrt(nodes)).astype(np.int64) - 1)
 
 
-def uneven_batch(seed=1234, count=1024, nmin=1000, nmax=64000, k_grid=128):
+def partition_by_cost(costs, parts):
+    """Independent problems split over `parts` ranks by estimated cost
+    (longest first, each to the least loaded rank; ties to the lower rank):
+    a list of `parts` ascending index arrays."""
+    costs = np.asarray(costs, dtype=np.float64)
+    order = sorted(range(costs.size), key=lambda i: (-costs[i], i))
+    load = [0.0] * parts
+    out = [[] for _ in range(parts)]
+    for i in order:
+        r = min(range(parts), key=lambda j: (load[j], j))
+        out[r].append(i)
+        load[r] += costs[i]
+    return [np.array(sorted(o), dtype=np.int64) for o in out]
+
+
+def batch_costs(seed=1234, count=1024, nmin=1000, nmax=64000):
+    """Estimated cost of every problem of the batch: its node count."""
+    return (uneven_sizes(seed, count, nmin, nmax) + 1).astype(np.float64) ** 2
+
+
+def uneven_batch(seed=1234, count=1024, nmin=1000, nmax=64000, k_grid=128, indices=None):
     """(meshes, k, f): meshes on the device, k per element and f per node
-    concatenated in problem order."""
+    concatenated in problem order; `indices` selects a subset of the batch
+    (each problem keeps its own seeds)."""
     meshes, ks, fs = [], [], []
-    for p, nx in enumerate(uneven_sizes(seed, count, nmin, nmax)):
+    sizes = uneven_sizes(seed, count, nmin, nmax)
+    for p in (range(count) if indices is None else indices):
+        nx = sizes[p]
         s = seed * 7919 + p
         m = F.Mesh(0.0, 1.0, 0.0, 1.0, int(nx), int(nx), 1, 1, 1, 1)
         xy, elem, code, _ = m.arrays()
