@@ -83,13 +83,10 @@ __global__ void __launch_bounds__(kRedBlock, 8) mx_load_residual(int64_t n, int6
                                                               const double* __restrict__ r,
                                                               double scale,
                                                               const float* __restrict__ dinv,
-                                                              float* rr0, float* rr1, float* p,
-                                                              float* d, int fresh, MixState* S,
+                                                              float* rr, float* p, float* d,
+                                                              int fresh, MixState* S,
                                                               double* partials, unsigned* counter)
 {
-   // the learned iteration keeps r in two buffers, the current one by the
-   // parity of the iteration count
-   float* rr = (rr1 && (S->it & 1)) ? rr1 : rr0;
    double v[2] = {0.0, 0.0};
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < npad; i += stride) {
@@ -288,19 +285,18 @@ __device__ __forceinline__ float4 sell_quad(const int32_t* __restrict__ sp,
    return acc;
 }
 
-// t = G r (r the current residual buffer)
+// t = G r
 template <class V, class I>
 __global__ void __launch_bounds__(kRedBlock, 8) lg_lower(int64_t nquads, const int32_t* __restrict__ sp,
                                                       const I* __restrict__ scol,
                                                       const V* __restrict__ sval,
-                                                      const float* r0, const float* r1, float* t,
+                                                      const float* __restrict__ r, float* t,
                                                       const MixState* S, int* worked)
 {
    pdl_wait();
    pdl_release();
    if (S->pause) return;
    prof_mark(worked);
-   const float* __restrict__ r = (S->it & 1) ? r1 : r0;
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nquads; i += stride)
       *reinterpret_cast<float4*>(t + i * 4) = sell_quad(sp, scol, sval, r, i * 4);
@@ -314,7 +310,7 @@ __global__ void __launch_bounds__(kRedBlock, 8) lg_upper(int64_t nquads, const i
                                                       const I* __restrict__ scol,
                                                       const V* __restrict__ sval,
                                                       const float* __restrict__ t, float* z,
-                                                      const float* r0, const float* r1,
+                                                      const float* __restrict__ r,
                                                       const float* __restrict__ q, MixState* S,
                                                       double* partials, unsigned* counter, int fr,
                                                       int* worked)
@@ -323,7 +319,6 @@ __global__ void __launch_bounds__(kRedBlock, 8) lg_upper(int64_t nquads, const i
    pdl_release();
    if (S->pause) return;
    prof_mark(worked);
-   const float* __restrict__ r = (S->it & 1) ? r1 : r0;
    double v[2] = {0.0, 0.0};
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nquads; i += stride) {
@@ -343,148 +338,30 @@ __global__ void __launch_bounds__(kRedBlock, 8) lg_upper(int64_t nquads, const i
    }
 }
 
-// The learned iteration with two fused kernels.  Iteration k (S->it = k):
-//   mx_spmv_dir: p_k = z + beta p_{k-1} (p_k = z on a fresh start), formed
-//     for every gathered column and stored for the own rows, q = A p_k,
-//     alpha = rho / (p_k, q);
-//   lg_lower_upd: d += alpha p_k, r_{k+1} = r_k - alpha q for the own rows,
-//     t = G r_{k+1} with r_{k+1} formed for every gathered column,
-//     ||r_{k+1}|| and the stopping decisions of mx_update, then S->it = k+1;
-//   lg_upper: z = G^T t, rho and beta (as above).
-// Directions and residuals alternate between two buffers by the parity of
-// k, so a gather never meets a value written by the same kernel; the fused
-// forms use the same single-rounding expressions wherever a value is formed.
-__device__ __forceinline__ float dir_at(const float* __restrict__ z, const float* __restrict__ pp,
-                                        int c, float beta, int fresh)
-{
-   const float zc = __ldg(z + c);
-   return fresh ? zc : __fmaf_rn(beta, __ldg(pp + c), zc);
-}
-
-template <class T, class I>
-__global__ void __launch_bounds__(kRedBlock, 8) mx_spmv_dir(int64_t nquads, const int32_t* __restrict__ sp,
-                                                         const I* __restrict__ scol,
-                                                         const T* __restrict__ sval,
-                                                         const float* __restrict__ z, float* p0,
-                                                         float* p1, float* __restrict__ q,
-                                                         MixState* S, double* partials,
-                                                         unsigned* counter, int fresh, int* worked)
+// p = z + beta p (p = z on a fresh start)
+__global__ void __launch_bounds__(kRedBlock, 8) lg_direction(int64_t nquads,
+                                                          const float* __restrict__ z, float* p,
+                                                          const MixState* S, int fresh)
 {
    pdl_wait();
    pdl_release();
    if (S->pause) return;
-   prof_mark(worked);
-   const int it = S->it;
-   const float* __restrict__ pp = (it & 1) ? p0 : p1;
-   float* __restrict__ pn = (it & 1) ? p1 : p0;
    const float beta = fresh ? 0.f : (float)S->beta;
-   double v[1] = {0.0};
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
-   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nquads; t += stride) {
-      const int64_t r0 = t * 4;
-      const int64_t s = r0 >> 5;
-      const int lane0 = (int)(r0 & 31);
-      const int32_t beg = sp[s], w = (sp[s + 1] - beg) >> 5;
-      float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-      const I* cp = scol + beg + lane0;
-      const T* vp = sval + beg + lane0;
-#pragma unroll 8
-      for (int32_t k = 0; k < w; ++k) {
-         const int4 c = load_cols(cp + k * 32, r0);
-         const float4 a = load_vals(vp + k * 32);
-         acc.x += a.x * dir_at(z, pp, c.x, beta, fresh);
-         acc.y += a.y * dir_at(z, pp, c.y, beta, fresh);
-         acc.z += a.z * dir_at(z, pp, c.z, beta, fresh);
-         acc.w += a.w * dir_at(z, pp, c.w, beta, fresh);
-      }
-      *reinterpret_cast<float4*>(q + r0) = acc;
-      const float4 zi = *reinterpret_cast<const float4*>(z + r0);
-      float4 pi = zi;
-      if (!fresh) {
-         const float4 po = *reinterpret_cast<const float4*>(pp + r0);
-         pi = make_float4(__fmaf_rn(beta, po.x, zi.x), __fmaf_rn(beta, po.y, zi.y),
-                          __fmaf_rn(beta, po.z, zi.z), __fmaf_rn(beta, po.w, zi.w));
-      }
-      *reinterpret_cast<float4*>(pn + r0) = pi;
-      v[0] += (double)pi.x * acc.x + (double)pi.y * acc.y + (double)pi.z * acc.z +
-              (double)pi.w * acc.w;
-   }
-   double tt[1];
-   if (grid_reduce<1>(v, partials, counter, tt)) S->alpha = S->rho[it & 1] / tt[0];
-}
-
-__device__ __forceinline__ float res_at(const float* __restrict__ r, const float* __restrict__ q,
-                                        int c, float a)
-{
-   return __fmaf_rn(-a, __ldg(q + c), __ldg(r + c));
-}
-
-template <class V, class I>
-__global__ void __launch_bounds__(kRedBlock, 8) lg_lower_upd(int64_t nquads,
-                                                          const int32_t* __restrict__ sp,
-                                                          const I* __restrict__ scol,
-                                                          const V* __restrict__ sval, float* r0,
-                                                          float* r1, const float* __restrict__ q,
-                                                          const float* p0, const float* p1,
-                                                          float* __restrict__ d,
-                                                          float* __restrict__ t, MixState* S,
-                                                          double* partials, unsigned* counter,
-                                                          double delta, double tol, double scale,
-                                                          int max_inner, int mode, int* worked)
-{
-   pdl_wait();
-   pdl_release();
-   if (S->pause) return;
-   prof_mark(worked);
-   const int it = S->it;
-   const float* __restrict__ rc = (it & 1) ? r1 : r0;
-   float* __restrict__ rn = (it & 1) ? r0 : r1;
-   const float* __restrict__ p = (it & 1) ? p1 : p0;
-   const float a = (float)S->alpha;
-   double v[1] = {0.0};
-   int64_t stride = (int64_t)gridDim.x * blockDim.x;
+   float4* p4 = reinterpret_cast<float4*>(p);
+   const float4* z4 = reinterpret_cast<const float4*>(z);
    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nquads; i += stride) {
-      const int64_t r0i = i * 4;
-      const float4 ri = *reinterpret_cast<const float4*>(rc + r0i);
-      const float4 qi = *reinterpret_cast<const float4*>(q + r0i);
-      const float4 pi = *reinterpret_cast<const float4*>(p + r0i);
-      float4 di = *reinterpret_cast<const float4*>(d + r0i);
-      di = make_float4(__fmaf_rn(a, pi.x, di.x), __fmaf_rn(a, pi.y, di.y), __fmaf_rn(a, pi.z, di.z),
-                       __fmaf_rn(a, pi.w, di.w));
-      const float4 rv = make_float4(__fmaf_rn(-a, qi.x, ri.x), __fmaf_rn(-a, qi.y, ri.y),
-                                    __fmaf_rn(-a, qi.z, ri.z), __fmaf_rn(-a, qi.w, ri.w));
-      *reinterpret_cast<float4*>(d + r0i) = di;
-      *reinterpret_cast<float4*>(rn + r0i) = rv;
-      v[0] += (double)rv.x * rv.x + (double)rv.y * rv.y + (double)rv.z * rv.z + (double)rv.w * rv.w;
-      const int64_t s = r0i >> 5;
-      const int lane0 = (int)(r0i & 31);
-      const int32_t beg = sp[s], w = (sp[s + 1] - beg) >> 5;
-      float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-      const I* cp = scol + beg + lane0;
-      const V* vp = sval + beg + lane0;
-#pragma unroll 4
-      for (int32_t k = 0; k < w; ++k) {
-         const int4 c = load_cols(cp + k * 32, r0i);
-         const float4 g = load_vals(vp + k * 32);
-         acc.x += g.x * res_at(rc, q, c.x, a);
-         acc.y += g.y * res_at(rc, q, c.y, a);
-         acc.z += g.z * res_at(rc, q, c.z, a);
-         acc.w += g.w * res_at(rc, q, c.w, a);
+      const float4 zi = z4[i];
+      if (fresh) {
+         p4[i] = zi;
+         continue;
       }
-      *reinterpret_cast<float4*>(t + r0i) = acc;
-   }
-   double tt[1];
-   if (grid_reduce<1>(v, partials, counter, tt)) {
-      S->rn = sqrt(tt[0]);
-      const int itn = it + 1;
-      S->it = itn;
-      if (mode == 0) {
-         if (S->rn <= delta * S->rmark || S->rn * scale <= tol * S->bnorm || itn >= max_inner)
-            S->pause = 1;
-      }
-      else if (S->rn <= delta * S->res0 || itn >= max_inner) {
-         S->pause = 1;
-      }
+      float4 pi = p4[i];
+      pi.x = zi.x + beta * pi.x;
+      pi.y = zi.y + beta * pi.y;
+      pi.z = zi.z + beta * pi.z;
+      pi.w = zi.w + beta * pi.w;
+      p4[i] = pi;
    }
 }
 
@@ -558,18 +435,12 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
    const int64_t nv = npad > 0 ? npad : 4;
    DBuf<float> dinv(nv), rr(nv), p(nv), q(nv), d(nv);
    DBuf<float> tz(learned ? nv : 1), zz(learned ? nv : 1);
-   // the learned iteration's second residual and direction buffers
-   DBuf<float> rr1(learned ? nv : 1), p1(learned ? nv : 1);
    DBuf<double> r(n > 0 ? n : 1), q64(n > 0 ? n : 1);
    DBuf<MixState> S(1);
    DBuf<int> bad(1);
    bad.zero();
    p.zero();
    q.zero();
-   if (learned) {
-      p1.zero();
-      rr1.zero();
-   }
    const unsigned g = grid_for(std::max<int64_t>(n, nquads), kRedBlock, 8);
    DBuf<double> partials(((size_t)g + 1) * 4 + 4);
    DBuf<unsigned> counter(1);
@@ -590,56 +461,41 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
       count_launch();
       OFG_LAUNCH_CHECK();
    };
-   // the learned preconditioner's products: t = G r (plain, at the start of
-   // an outer iteration; fused with the update inside it), z = G^T t with
-   // rho and beta.  Algorithmic bytes: BF16 value + column index (2 or 4
-   // bytes) per entry, the gathered input(s), the outputs, and the own-row
-   // vectors of the fused update (r, q, p, d read; r, d written)
+   // z = G^T G r, rho, beta, then the new direction
+   // algorithmic bytes of the two factor products: BF16 value + column
+   // index (2 or 4 bytes) per entry, the gathered input and the output (and
+   // r, q for the reduction of the second)
    const double gidx = g16 ? 2.0 : 4.0;
-   double scale = 1.0;
-   using bf = __nv_bfloat16;
-   const bf* vl = reinterpret_cast<const bf*>(learned ? LP->gl->sell_valbf.p : nullptr);
-   const bf* vu = reinterpret_cast<const bf*>(learned ? LP->gu->sell_valbf.p : nullptr);
-   auto learned_lower = [&]() {
+   auto learned_direction = [&](int fr, int fresh) {
+      using bf = __nv_bfloat16;
+      const bf* vl = reinterpret_cast<const bf*>(learned ? LP->gl->sell_valbf.p : nullptr);
+      const bf* vu = reinterpret_cast<const bf*>(learned ? LP->gu->sell_valbf.p : nullptr);
       int* worked = prof_begin();
       if (g16)
          launch_pdl(lg_lower<bf, int16_t>, gq, kRedBlock, nquads, LP->gl->sell_ptr.p,
-                    LP->gl->sell_d16.p, vl, rr.p, rr1.p, tz.p, S.p, worked);
+                    LP->gl->sell_d16.p, vl, rr.p, tz.p, S.p, worked);
       else
          launch_pdl(lg_lower<bf, int32_t>, gq, kRedBlock, nquads, LP->gl->sell_ptr.p,
-                    LP->gl->sell_col.p, vl, rr.p, rr1.p, tz.p, S.p, worked);
+                    LP->gl->sell_col.p, vl, rr.p, tz.p, S.p, worked);
       prof_end(PROF_LEARNED_APPLY, (2.0 + gidx) * LP->gl->nnz + 8.0 * n);
-   };
-   auto learned_upper = [&](int fr) {
-      int* worked = prof_begin();
+      worked = prof_begin();
       if (g16)
          launch_pdl(lg_upper<bf, int16_t>, gq, kRedBlock, nquads, LP->gu->sell_ptr.p,
-                    LP->gu->sell_d16.p, vu, tz.p, zz.p, rr.p, rr1.p, q.p, S.p, partials.p,
-                    counter.p, fr, worked);
+                    LP->gu->sell_d16.p, vu, tz.p, zz.p, rr.p, q.p, S.p, partials.p, counter.p, fr,
+                    worked);
       else
          launch_pdl(lg_upper<bf, int32_t>, gq, kRedBlock, nquads, LP->gu->sell_ptr.p,
-                    LP->gu->sell_col.p, vu, tz.p, zz.p, rr.p, rr1.p, q.p, S.p, partials.p,
-                    counter.p, fr, worked);
+                    LP->gu->sell_col.p, vu, tz.p, zz.p, rr.p, q.p, S.p, partials.p, counter.p, fr,
+                    worked);
       prof_end(PROF_LEARNED_APPLY, (2.0 + gidx) * LP->gu->nnz + 16.0 * n);
-   };
-   auto learned_lower_update = [&]() {
-      int* worked = prof_begin();
-      if (g16)
-         launch_pdl(lg_lower_upd<bf, int16_t>, gq, kRedBlock, nquads, LP->gl->sell_ptr.p,
-                    LP->gl->sell_d16.p, vl, rr.p, rr1.p, q.p, p.p, p1.p, d.p, tz.p, S.p,
-                    partials.p, counter.p, inner_tol, tol, scale, max_inner, mode, worked);
-      else
-         launch_pdl(lg_lower_upd<bf, int32_t>, gq, kRedBlock, nquads, LP->gl->sell_ptr.p,
-                    LP->gl->sell_col.p, vl, rr.p, rr1.p, q.p, p.p, p1.p, d.p, tz.p, S.p,
-                    partials.p, counter.p, inner_tol, tol, scale, max_inner, mode, worked);
-      prof_end(PROF_LEARNED_APPLY, (2.0 + gidx) * LP->gl->nnz + 32.0 * n);
+      launch_pdl(lg_direction, gq, kRedBlock, nquads, zz.p, p.p, S.p, fresh);
    };
    MixState h{};
    true_residual(1);
    S.download(&h, 1);
    int n_outer = 0;
    // mode 1 solves for d in units of ||r||; mode 0 keeps absolute units
-   // (scale is declared with the launch helpers above)
+   double scale = 1.0;
    bool fresh = true;
    // stagnation watch of the learned iteration: the recursive residual must
    // halve within kStallIters iterations and stay finite, and the true
@@ -653,18 +509,11 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
          scale = h.rel * h.bnorm;
          fresh = true;
       }
-      mx_load_residual<<<gq, kRedBlock, 0, stream()>>>(n, npad, r.p, 1.0 / scale, jac, rr.p,
-                                                       learned ? rr1.p : nullptr, p.p, d.p,
-                                                       fresh ? 1 : 0, S.p, partials.p, counter.p);
+      mx_load_residual<<<gq, kRedBlock, 0, stream()>>>(n, npad, r.p, 1.0 / scale, jac, rr.p, p.p,
+                                                       d.p, fresh ? 1 : 0, S.p, partials.p,
+                                                       counter.p);
       count_launch();
-      // the learned iteration's first direction is formed by its first
-      // mx_spmv_dir (p = z on a fresh start, z + beta p with fr = 1 after a
-      // refinement in absolute units)
-      bool dir_fresh = fresh;
-      if (learned) {
-         learned_lower();
-         learned_upper(fresh ? 0 : 1);
-      }
+      if (learned) learned_direction(fresh ? 0 : 1, fresh ? 1 : 0);
       else if (!fresh) {
          mx_direction<<<gq, kRedBlock, 0, stream()>>>(nquads, rr.p, dinv.p, p.p, S.p);
          count_launch();
@@ -679,32 +528,6 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
             // launch: each one's blocks start while the previous one drains
             // its reduction tail
             int* worked = prof_begin();
-            if (learned) {
-               const int fr = dir_fresh ? 1 : 0;
-               dir_fresh = false;
-               if (inner_bits == 32 && a16)
-                  launch_pdl(mx_spmv_dir<float, int16_t>, gq, kRedBlock, nquads, A->sell_ptr.p,
-                             A->sell_d16.p, A->sell_val32.p, zz.p, p.p, p1.p, q.p, S.p,
-                             partials.p, counter.p, fr, worked);
-               else if (inner_bits == 32)
-                  launch_pdl(mx_spmv_dir<float, int32_t>, gq, kRedBlock, nquads, A->sell_ptr.p,
-                             A->sell_col.p, A->sell_val32.p, zz.p, p.p, p1.p, q.p, S.p,
-                             partials.p, counter.p, fr, worked);
-               else if (a16)
-                  launch_pdl(mx_spmv_dir<__nv_bfloat16, int16_t>, gq, kRedBlock, nquads,
-                             A->sell_ptr.p, A->sell_d16.p, v16.p, zz.p, p.p, p1.p, q.p, S.p,
-                             partials.p, counter.p, fr, worked);
-               else
-                  launch_pdl(mx_spmv_dir<__nv_bfloat16, int32_t>, gq, kRedBlock, nquads,
-                             A->sell_ptr.p, A->sell_col.p, v16.p, zz.p, p.p, p1.p, q.p, S.p,
-                             partials.p, counter.p, fr, worked);
-               // values + column indices, z and p_prev gathered, p and q written
-               prof_end(inner_bits == 32 ? PROF_SPMV32 : PROF_SPMV16,
-                        ((inner_bits == 32 ? 4.0 : 2.0) + aidx) * A->nnz + 16.0 * n + 4.0);
-               learned_lower_update();
-               learned_upper(0);
-               continue;
-            }
             if (inner_bits == 32 && a16)
                launch_pdl(mx_spmv<float, int16_t>, gq, kRedBlock, nquads, A->sell_ptr.p,
                           A->sell_d16.p, A->sell_val32.p, p.p, q.p, S.p, partials.p, counter.p,
@@ -723,9 +546,16 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
             // 16-bit offset) per entry, p gathered, q written, p read for the dot
             prof_end(inner_bits == 32 ? PROF_SPMV32 : PROF_SPMV16,
                      ((inner_bits == 32 ? 4.0 : 2.0) + aidx) * A->nnz + 12.0 * n + 4.0);
-            launch_pdl(mx_update<true>, gq, kRedBlock, nquads, d.p, p.p, rr.p, q.p, dinv.p, S.p,
-                       partials.p, counter.p, inner_tol, tol, scale, max_inner, mode);
-            launch_pdl(mx_direction, gq, kRedBlock, nquads, rr.p, dinv.p, p.p, S.p);
+            if (learned) {
+               launch_pdl(mx_update<false>, gq, kRedBlock, nquads, d.p, p.p, rr.p, q.p, jac, S.p,
+                          partials.p, counter.p, inner_tol, tol, scale, max_inner, mode);
+               learned_direction(0, 0);
+            }
+            else {
+               launch_pdl(mx_update<true>, gq, kRedBlock, nquads, d.p, p.p, rr.p, q.p, dinv.p, S.p,
+                          partials.p, counter.p, inner_tol, tol, scale, max_inner, mode);
+               launch_pdl(mx_direction, gq, kRedBlock, nquads, rr.p, dinv.p, p.p, S.p);
+            }
          }
          OFG_LAUNCH_CHECK();
          S.download(&h, 1);
