@@ -18,9 +18,11 @@
 // Errors raise OFELIException, as OFELI does.
 #pragma once
 
+#include <algorithm>
 #include <cmath>
 #include <cstddef>
 #include <cstdint>
+#include <cstdlib>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -258,6 +260,45 @@ class SpMatrix<real_t> {
       Mult(x, y);
       return y;
    }
+   // SpMatrix::TMult: y += A^T x (SpMatrix_impl.h:760-767, the intended
+   // product; OFELI's loop indexes the column one entry early)
+   void TMult(const Vect<real_t>& x, Vect<real_t>& y) const
+   {
+      y.resize(_n);
+      ofg_check(ofg_spmv_transpose_add(_h, x.data(), y.data()), "SpMatrix::TMult");
+   }
+   // SpMatrix::set(i,j,v) / add(i,j,v), 1-based (SpMatrix_impl.h:785-802); a
+   // pair outside the pattern throws (OFELI's add would write into the
+   // previous row instead).  For many entries, edit() applies them in one call.
+   void set(size_t i, size_t j, real_t v) { edit({i}, {j}, {v}, true); }
+   void add(size_t i, size_t j, real_t v) { edit({i}, {j}, {v}, false); }
+   void edit(const std::vector<size_t>& i, const std::vector<size_t>& j,
+             const std::vector<real_t>& v, bool set_values)
+   {
+      if (i.size() != j.size() || i.size() != v.size())
+         throw OFELIException("SpMatrix::edit: index and value arrays differ in size");
+      std::vector<int64_t> ii(i.begin(), i.end()), jj(j.begin(), j.end());
+      ofg_check(ofg_matrix_edit(_h, (int64_t)ii.size(), ii.data(), jj.data(), v.data(),
+                                set_values ? 1 : 0),
+                set_values ? "SpMatrix::set" : "SpMatrix::add");
+   }
+   // SpMatrix::DILUFactorize / ILUFactorize (SpMatrix_impl.h:837-878): id =
+   // 1-based diagonal positions, pivot = the inverted D-ILU pivots; returns
+   // 0, or the 1-based row of a zero pivot.  DILUSolve / ILUSolve / SSORSolve
+   // apply the factorisation of the matrix's current values.
+   int DILUFactorize(std::vector<size_t>& id, std::vector<real_t>& pivot) const;
+   int ILUFactorize(std::vector<size_t>& id, std::vector<real_t>& pivot) const
+   {
+      return DILUFactorize(id, pivot);
+   }
+   void DILUSolve(const std::vector<size_t>& id, const std::vector<real_t>& pivot,
+                  const Vect<real_t>& b, Vect<real_t>& x) const;
+   void ILUSolve(const std::vector<size_t>& id, const std::vector<real_t>& pivot,
+                 const Vect<real_t>& b, Vect<real_t>& x) const
+   {
+      DILUSolve(id, pivot, b, x);
+   }
+   void SSORSolve(const Vect<real_t>& b, Vect<real_t>& x) const;
    // SpMatrix::setSolver / solve (SpMatrix_impl.h:957-971)
    void setSolver(Iteration s = CG_SOLVER, Preconditioner p = DIAG_PREC, int max_it = 1000,
                   real_t toler = 1.e-8)
@@ -327,6 +368,43 @@ class Prec<real_t> {
    ofg_prec* _h = nullptr;
    int _type;
 };
+
+inline int SpMatrix<real_t>::DILUFactorize(std::vector<size_t>& id,
+                                           std::vector<real_t>& pivot) const
+{
+   ofg_prec* P = nullptr;
+   int rc = ofg_prec_create(_h, DILU_PREC, &P);
+   if (rc == OFG_ERR_PIVOT) {
+      // OFELI returns the row of the zero pivot; the message names it
+      std::string m = ofg_last_error();
+      size_t at = m.rfind(' ');
+      return at == std::string::npos ? 1 : std::max(1, std::atoi(m.c_str() + at + 1));
+   }
+   ofg_check(rc, "SpMatrix::DILUFactorize");
+   pivot.assign(_n, 0.0);
+   rc = ofg_prec_get_pivot(P, pivot.data());
+   ofg_prec_destroy(P);
+   ofg_check(rc, "SpMatrix::DILUFactorize");
+   pattern();
+   id.assign(_n, 0);
+   for (int64_t i = 0; i < _n; ++i)
+      for (int64_t k = _rp[i]; k < _rp[i + 1]; ++k)
+         if (_ci[k] == i + 1) id[i] = (size_t)k + 1;
+   return 0;
+}
+
+inline void SpMatrix<real_t>::DILUSolve(const std::vector<size_t>&, const std::vector<real_t>&,
+                                        const Vect<real_t>& b, Vect<real_t>& x) const
+{
+   Prec<real_t> P(*this, DILU_PREC);
+   P.solve(b, x);
+}
+
+inline void SpMatrix<real_t>::SSORSolve(const Vect<real_t>& b, Vect<real_t>& x) const
+{
+   Prec<real_t> P(*this, SSOR_PREC);
+   P.solve(b, x);
+}
 
 // ------------------------------------------------------------ CG, GMRes ----
 // Return: iterations when converged, -iterations otherwise (CG.h:99-157).

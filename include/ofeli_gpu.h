@@ -59,6 +59,13 @@ typedef struct ofg_mesh_file ofg_mesh_file;
 /* ---------------------------------------------------------------- runtime */
 const char* ofg_last_error(void);
 const char* ofg_version(void);
+/* Selects the device of the calling thread and creates its stream
+ * (optional: the first call on a device does the same).  No counterpart in
+ * OFELI, which has no device. */
+int ofg_init(int device);
+/* Waits for the library's work and frees its process-wide buffers (the mesh
+ * reader's pinned staging buffer); handles stay valid. */
+int ofg_shutdown(void);
 /* Selects the stream used by later calls (NULL = the library's own). */
 int ofg_set_stream(void* cuda_stream);
 void* ofg_get_stream(void);
@@ -68,7 +75,7 @@ int64_t ofg_launch_count(void);
  * disabling) resets the totals; while enabled (on >= 1), every on-th launch
  * of an instrumented kernel is bracketed by events on the library stream.  Families: "spmv64", "spmv32",
  * "spmv16" (SELL SpMV in FP64 / FP32 / BF16 values, inside the solvers too),
- * "sweep" (triangular sweeps), "assembly" (element colour launches),
+ * "sweep" (triangular sweeps), "assembly" (row-gather assembly launches),
  * "network_gemm" (tensor-core layer products of the learned preconditioner's
  * network), "learned_apply" (the two FP32 factor products inside
  * ofg_fcg_learned).
@@ -98,6 +105,15 @@ int ofg_matrix_clear(ofg_matrix* A);
 /* SpMatrix::Mult / MultAdd: y = A x, y += A x (SpMatrix_impl.h:729-745). */
 int ofg_spmv(const ofg_matrix* A, const double* x, double* y);
 int ofg_spmv_add(const ofg_matrix* A, const double* x, double* y);
+/* SpMatrix::TMult: y += A^T x, each y entry accumulating in ascending row
+ * order as OFELI's loop intends (SpMatrix_impl.h:760-767; OFELI's loop reads
+ * the previous entry's column, see entries.cu). */
+int ofg_spmv_transpose_add(ofg_matrix* A, const double* x, double* y);
+/* SpMatrix::set(i,j,v) (set = 1) / add(i,j,v) (set = 0) for `count` entries,
+ * 1-based indices, applied in order (SpMatrix_impl.h:785-802); a pair outside
+ * the pattern stops the batch with OFG_ERR_ARG. */
+int ofg_matrix_edit(ofg_matrix* A, int64_t count, const int64_t* i, const int64_t* j,
+                    const double* v, int set);
 /* Device-only SpMV with an explicit layout choice, for measurement:
  * kind 0 = CSR warp-segment kernel, 1 = SELL-32 kernel. */
 int ofg_spmv_device(const ofg_matrix* A, int kind, const double* d_x, double* d_y);

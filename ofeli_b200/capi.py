@@ -32,10 +32,14 @@ SIGNATURES = {
     "ofg_set_stream": (_i32, [_p]),
     "ofg_get_stream": (_p, []),
     "ofg_launch_count": (_i64, []),
+    "ofg_init": (_i32, [_i32]),
+    "ofg_shutdown": (_i32, []),
     "ofg_profile_enable": (_i32, [_i32]),
     "ofg_profile_read": (_i32, [ctypes.c_char_p, _pi64, _pd, _pd]),
     "ofg_matrix_create": (_i32, [_i64, _i64, _p, _p, _pp]),
     "ofg_matrix_destroy": (_i32, [_p]),
+    "ofg_spmv_transpose_add": (_i32, [_p, _p, _p]),
+    "ofg_matrix_edit": (_i32, [_p, _i64, _p, _p, _p, _i32]),
     "ofg_matrix_info": (_i32, [_p, _pi64, _pi64]),
     "ofg_matrix_get_pattern": (_i32, [_p, _p, _p]),
     "ofg_matrix_set_values": (_i32, [_p, _p]),

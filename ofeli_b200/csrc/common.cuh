@@ -59,6 +59,8 @@ int guarded(const char* fn, F&& f)
 
 // ----------------------------------------------------------- stream, count --
 cudaStream_t stream();
+// frees the mesh-file reader's pinned staging buffer (meshio.cu)
+void meshio_release_staging();
 int num_sms();
 void count_launch(int n = 1);
 

@@ -37,6 +37,13 @@ struct ofg_matrix {
    int max_row = 0;
    double avg_row = 0;
 
+   // column-major copy of the pattern for the transposed product (built on
+   // first use): column c's entries t_ptr[c] .. t_ptr[c+1], their rows in
+   // ascending order and their CSR positions
+   ofg::DBuf<int64_t> t_ptr;
+   ofg::DBuf<int32_t> t_row, t_pos;
+   bool t_ready = false;
+
    // element-to-CSR map of the mesh this pattern came from
    ofg_mesh* mesh = nullptr;
    ofg::DBuf<int32_t> emap;  // ne * nen * nen, -1 where a DOF is imposed

@@ -1035,6 +1035,18 @@ char* pinned_staging(size_t n)
    return g_pin;
 }
 
+}  // namespace
+
+void ofg::meshio_release_staging()
+{
+   std::lock_guard<std::mutex> lock(g_pin_mu);
+   if (g_pin) cudaFreeHost(g_pin);
+   g_pin = nullptr;
+   g_pin_cap = 0;
+}
+
+namespace {
+
 // The file into the staging buffer (parallel reads), NUL-terminated.
 size_t read_pinned(const char* path, char*& buf)
 {

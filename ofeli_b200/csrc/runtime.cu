@@ -189,6 +189,24 @@ void* ofg_get_stream(void)
 
 int64_t ofg_launch_count(void) { return ofg::g_launches.load(); }
 
+int ofg_init(int device)
+{
+   return ofg::guarded("ofg_init", [&] {
+      OFG_REQUIRE(device >= 0, OFG_ERR_ARG, "device must be >= 0");
+      OFG_CUDA(cudaSetDevice(device));
+      OFG_CUDA(cudaStreamSynchronize(ofg::stream()));
+   });
+}
+
+int ofg_shutdown(void)
+{
+   return ofg::guarded("ofg_shutdown", [&] {
+      OFG_CUDA(cudaStreamSynchronize(ofg::stream()));
+      ofg::prof_collect();
+      ofg::meshio_release_staging();
+   });
+}
+
 int ofg_profile_enable(int on)
 {
    return ofg::guarded("ofg_profile_enable", [&] {

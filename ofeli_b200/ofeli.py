@@ -316,6 +316,30 @@ class SpMatrix:
     def __mul__(self, x):
         return self.Mult(x)
 
+    def TMult(self, x, y):
+        """SpMatrix::TMult: y += A^T x (the intended product of
+        SpMatrix_impl.h:760-767)."""
+        x = _f64(x, self.n)
+        _call("ofg_spmv_transpose_add", self._h, _ptr(x), _ptr(y))
+        return y
+
+    def edit(self, i, j, v, set_values):
+        """SpMatrix::set / add for many 1-based (i, j, v), applied in order."""
+        i = np.ascontiguousarray(i, dtype=np.int64).reshape(-1)
+        j = np.ascontiguousarray(j, dtype=np.int64).reshape(-1)
+        v = np.ascontiguousarray(v, dtype=np.float64).reshape(-1)
+        if not (i.size == j.size == v.size):
+            raise OFELIException("index and value arrays differ in size")
+        _call("ofg_matrix_edit", self._h, i.size, _ptr(i), _ptr(j), _ptr(v), 1 if set_values else 0)
+
+    def set(self, i, j, v):
+        """SpMatrix::set(i, j, v), 1-based (SpMatrix_impl.h:785-795)."""
+        self.edit([i], [j], [v], True)
+
+    def add(self, i, j, v):
+        """SpMatrix::add(i, j, v), 1-based (SpMatrix_impl.h:797-802)."""
+        self.edit([i], [j], [v], False)
+
     def __del__(self):
         if getattr(self, "_h", None) and capi is not None and capi._lib is not None:
             capi.lib().ofg_matrix_destroy(self._h)

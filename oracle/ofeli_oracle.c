@@ -353,6 +353,38 @@ void or_spmv(int64_t n, const int64_t* row_ptr, const int64_t* col_ind, const do
    }
 }
 
+/* SpMatrix::TMult, the product its loop intends (SpMatrix_impl.h:760-767):
+ * y[col] += a * x[row] over the rows in ascending order, into y as given.
+ * (The loop itself reads col_ind one entry early.) */
+void or_spmv_transpose_add(int64_t n, const int64_t* row_ptr, const int64_t* col_ind,
+                           const double* a, const double* x, double* y)
+{
+   for (int64_t i = 0; i < n; ++i)
+      for (int64_t k = row_ptr[i]; k < row_ptr[i + 1]; ++k) y[col_ind[k] - 1] += a[k] * x[i];
+}
+
+/* SpMatrix::set / add (SpMatrix_impl.h:785-802) for count 1-based pairs in
+ * order, with _col_index's linear row search (:1009-1015); returns the index
+ * of the first pair outside the pattern, or -1. */
+int64_t or_matrix_edit(int64_t n, const int64_t* row_ptr, const int64_t* col_ind, double* a,
+                       int64_t count, const int64_t* ii, const int64_t* jj, const double* v,
+                       int set)
+{
+   for (int64_t e = 0; e < count; ++e) {
+      int64_t i = ii[e], j = jj[e], found = -1;
+      if (i < 1 || i > n || j < 1 || j > n) return e;
+      for (int64_t k = row_ptr[i - 1]; k < row_ptr[i]; ++k)
+         if (col_ind[k] == j) {
+            found = k;
+            break;
+         }
+      if (found < 0) return e;
+      if (set) a[found] = v[e];
+      else a[found] += v[e];
+   }
+   return -1;
+}
+
 static double norm2(int64_t n, const double* x)
 {
    double s = 0;

@@ -47,6 +47,11 @@ int64_t or_assemble_cd2d(int64_t nn, int64_t ne, const double* xy, const int32_t
 /* a14: y = A x (SpMatrix::Mult) */
 void or_spmv(int64_t n, const int64_t* row_ptr, const int64_t* col_ind, const double* a,
              const double* x, double* y);
+void or_spmv_transpose_add(int64_t n, const int64_t* row_ptr, const int64_t* col_ind,
+                           const double* a, const double* x, double* y);
+int64_t or_matrix_edit(int64_t n, const int64_t* row_ptr, const int64_t* col_ind, double* a,
+                       int64_t count, const int64_t* ii, const int64_t* jj, const double* v,
+                       int set);
 /* a18: Prec setup.  id (n) receives the 1-based position after the diagonal
  * (OFELI's "id"), pivot (n) the inverse pivots / diagonal.  Returns 0 or
  * -(row+1) on a zero pivot. */

@@ -67,6 +67,9 @@ def lib():
                                   ctypes.c_double]
         L.or_bicgstab.restype = ctypes.c_int
         L.or_insert_bc.argtypes = [_i64, _p, _p, _p, _p]
+        L.or_spmv_transpose_add.argtypes = [_i64, _p, _p, _p, _p, _p]
+        L.or_matrix_edit.argtypes = [_i64, _p, _p, _p, _i64, _p, _p, _p, ctypes.c_int]
+        L.or_matrix_edit.restype = _i64
         _lib = L
     return _lib
 
@@ -135,6 +138,23 @@ def spmv(rp, ci, a, x):
     y = np.zeros(rp.size - 1)
     lib().or_spmv(rp.size - 1, _ptr(rp), _ptr(ci), _ptr(a), _ptr(x), _ptr(y))
     return y
+
+
+def spmv_transpose_add(rp, ci, a, x, y):
+    y = np.array(y, dtype=np.float64)
+    lib().or_spmv_transpose_add(rp.size - 1, _ptr(rp), _ptr(ci), _ptr(a), _ptr(x), _ptr(y))
+    return y
+
+
+def matrix_edit(rp, ci, a, i, j, v, set_values):
+    """(new values, index of the first pair outside the pattern or -1)."""
+    a = np.array(a, dtype=np.float64)
+    i = np.ascontiguousarray(i, dtype=np.int64)
+    j = np.ascontiguousarray(j, dtype=np.int64)
+    v = np.ascontiguousarray(v, dtype=np.float64)
+    bad = lib().or_matrix_edit(rp.size - 1, _ptr(rp), _ptr(ci), _ptr(a), i.size, _ptr(i), _ptr(j),
+                               _ptr(v), 1 if set_values else 0)
+    return a, int(bad)
 
 
 def prec_setup(ptype, rp, ci, a):

@@ -345,3 +345,56 @@ def test_bicgstab_edges(cuda):
         xo, ito = O.bicgstab(rp, ci, g["a"], g["b"], pt, 5, 1e-10)
         assert it == ito == -6
         assert rel_err(x, xo) <= 1e-10
+
+
+def test_tmult_matches_oracle(p2d65):
+    """SpMatrix::TMult (y += A^T x) against the oracle's row-ordered loop, bit
+    for bit, on the assembled 65^2 matrix and on a non-symmetric pattern
+    whose rows list their columns out of order."""
+    g, _, _, eq = p2d65
+    A = eq.getMatrix()
+    rp, ci = A.pattern()
+    rng = np.random.default_rng(8)
+    x, y0 = rng.standard_normal(A.n), rng.standard_normal(A.n)
+    y = A.TMult(x, y0.copy())
+    assert np.array_equal(y, O.spmv_transpose_add(rp, ci, A.values(), x, y0))
+    n = 300
+    rows = [rng.choice(n, size=rng.integers(1, 9), replace=False) + 1 for _ in range(n)]
+    rp2 = np.concatenate([[0], np.cumsum([r.size for r in rows])]).astype(np.int64)
+    ci2 = np.concatenate(rows).astype(np.int64)
+    a2 = rng.standard_normal(ci2.size)
+    B = F.SpMatrix(rp2, ci2, a2)
+    x2, y2 = rng.standard_normal(n), rng.standard_normal(n)
+    assert np.array_equal(B.TMult(x2, y2.copy()), O.spmv_transpose_add(rp2, ci2, a2, x2, y2))
+
+
+def test_matrix_set_add_in_order(p2d65):
+    """SpMatrix::set / add batches (repeated pairs included) applied in
+    order, as the oracle's loop does; a pair outside the pattern raises
+    after the pairs before it."""
+    g, _, _, eq = p2d65
+    A = eq.getMatrix()
+    rp, ci = A.pattern()
+    rng = np.random.default_rng(9)
+    rows = rng.integers(1, A.n + 1, 500)
+    ks = rp[rows - 1] + rng.integers(0, 10 ** 6, 500) % (rp[rows] - rp[rows - 1])
+    cols = ci[ks]
+    rows, cols = np.concatenate([rows, rows[:50]]), np.concatenate([cols, cols[:50]])
+    vals = rng.standard_normal(rows.size)
+    a0 = A.values()
+    for set_values in (False, True):
+        A.set_values(a0)
+        A.edit(rows, cols, vals, set_values)
+        want, bad = O.matrix_edit(rp, ci, a0, rows, cols, vals, set_values)
+        assert bad == -1 and np.array_equal(A.values(), want)
+    A.set_values(a0)
+    A.add(1, 1, 0.5)
+    assert A.values()[rp[0]] == a0[rp[0]] + 0.5
+    bad_rows = np.array([1, 1, 2])
+    bad_cols = np.array([1, A.n, 2])   # (1, n) is outside the pattern
+    A.set_values(a0)
+    with pytest.raises(F.OFELIException):
+        A.edit(bad_rows, bad_cols, np.ones(3), False)
+    want, bad = O.matrix_edit(rp, ci, a0, bad_rows, bad_cols, np.ones(3), False)
+    assert bad == 1 and np.array_equal(A.values(), want)
+    A.set_values(a0)
