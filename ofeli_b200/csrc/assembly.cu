@@ -179,12 +179,21 @@ __global__ void __launch_bounds__(256) assemble_rows(int64_t nn, const int32_t* 
       if (r)
          for (int32_t k = row_ptr[r - 1]; k < row_ptr[r]; ++k) a[k] = 0.0;
       double bi = 0.0;
-      const int32_t q1 = n2e_ptr[i + 1];
-      for (int32_t q = n2e_ptr[i]; q < q1; ++q) {
-         const int64_t e = n2e[q];
+      const int32_t q0 = n2e_ptr[i], q1 = n2e_ptr[i + 1];
+      int64_t e_next = q0 < q1 ? n2e[q0] : 0;
+      int32_t en_next[NEN];
+#pragma unroll
+      for (int j = 0; j < NEN; ++j) en_next[j] = q0 < q1 ? elem[NEN * e_next + j] : 0;
+      for (int32_t q = q0; q < q1; ++q) {
+         const int64_t e = e_next;
          int32_t en[NEN];
 #pragma unroll
-         for (int j = 0; j < NEN; ++j) en[j] = elem[NEN * e + j];
+         for (int j = 0; j < NEN; ++j) en[j] = en_next[j];
+         if (q + 1 < q1) {
+            e_next = n2e[q + 1];
+#pragma unroll
+            for (int j = 0; j < NEN; ++j) en_next[j] = elem[NEN * e_next + j];
+         }
          int li = 0;
 #pragma unroll
          for (int j = NEN - 1; j > 0; --j)
