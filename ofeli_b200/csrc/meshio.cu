@@ -774,7 +774,8 @@ using namespace ofg;
 
 // ------------------------------------------------------ device reading --
 // ofg_mesh_read: the file's bytes are read into a pinned staging buffer and
-// copied to the device once; the host walks the XML structure (tags are few)
+// copied to the device once, piece by piece as they are read; the host walks
+// the XML structure (tags are few)
 // and the Nodes / Elements / Sides texts are tokenised and converted by
 // kernels, straight into the device mesh's buffers.
 //
@@ -1047,8 +1048,10 @@ void ofg::meshio_release_staging()
 
 namespace {
 
-// The file into the staging buffer (parallel reads), NUL-terminated.
-size_t read_pinned(const char* path, char*& buf)
+// The file into the staging buffer by a team of threads, NUL-terminated,
+// and on to the device: each thread copies every piece it has read (4 MiB at
+// most) to `db` at once, so the transfer overlaps the reading.
+size_t read_to_device(const char* path, char*& buf, DBuf<char>& db)
 {
    int fd = ::open(path, O_RDONLY);
    if (fd < 0) throw Error(OFG_ERR_ARG, std::string("cannot open ") + path);
@@ -1060,13 +1063,26 @@ size_t read_pinned(const char* path, char*& buf)
    const size_t size = size_t(st.st_size);
    try {
       buf = pinned_staging(size + 1);
+      db.alloc(((size + 15) & ~size_t(15)) + 32);
+      int device = 0;
+      OFG_CUDA(cudaGetDevice(&device));
+      const cudaStream_t st_ = stream();
+      constexpr size_t kPiece = size_t(4) << 20;
       int T = team_size(size >> 2);
       parallel_for(T, [&](int t) {
-         size_t a = size * size_t(t) / size_t(T), z = size * size_t(t + 1) / size_t(T);
+         OFG_CUDA(cudaSetDevice(device));
+         size_t a = size * size_t(t) / size_t(T);
+         const size_t z = size * size_t(t + 1) / size_t(T);
          while (a < z) {
-            ssize_t r = ::pread(fd, buf + a, z - a, off_t(a));
-            if (r <= 0) throw Error(OFG_ERR_ARG, std::string("read error on ") + path);
-            a += size_t(r);
+            const size_t e = std::min(z, a + kPiece);
+            size_t p = a;
+            while (p < e) {
+               ssize_t r = ::pread(fd, buf + p, e - p, off_t(p));
+               if (r <= 0) throw Error(OFG_ERR_ARG, std::string("read error on ") + path);
+               p += size_t(r);
+            }
+            OFG_CUDA(cudaMemcpyAsync(db.p + a, buf + a, e - a, cudaMemcpyHostToDevice, st_));
+            a = e;
          }
       });
    }
@@ -1113,9 +1129,8 @@ bool read_device(const char* path, ofg_mesh** out)
 {
    std::lock_guard<std::mutex> lock(g_pin_mu);
    char* hb = nullptr;
-   const size_t size = read_pinned(path, hb);
-   DBuf<char> db(((size + 15) & ~size_t(15)) + 32);
-   if (size) OFG_CUDA(cudaMemcpyAsync(db.p, hb, size, cudaMemcpyHostToDevice, stream()));
+   DBuf<char> db;
+   const size_t size = read_to_device(path, hb, db);
    ofg_mesh_file meta;
    Reader rd{&meta};
    std::vector<Reader::Deferred> blocks;
