@@ -172,7 +172,7 @@ class Mesh {
 
  private:
    explicit Mesh(ofg_mesh* h) : _h(h) { info(); }
-   void info() { ofg_check(ofg_mesh_info(_h, &_dim, &_nn, &_ne, &_neq, nullptr), "Mesh"); }
+   void info() { ofg_check(ofg_mesh_info(_h, &_dim, &_nn, &_ne, &_neq), "Mesh"); }
    ofg_mesh* _h = nullptr;
    std::string _path;   // the file a mesh was read from (put writes its content)
    int _dim = 0;

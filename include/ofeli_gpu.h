@@ -145,8 +145,7 @@ int ofg_mesh_create_kuhn(int64_t M, ofg_mesh** out);
 int ofg_mesh_create(int dim, int64_t nn, const double* coords, int64_t ne, const int32_t* elem,
                     const int32_t* code, ofg_mesh** out);
 int ofg_mesh_destroy(ofg_mesh* m);
-int ofg_mesh_info(const ofg_mesh* m, int* dim, int64_t* nn, int64_t* ne, int64_t* neq,
-                  int* ncolors);
+int ofg_mesh_info(const ofg_mesh* m, int* dim, int64_t* nn, int64_t* ne, int64_t* neq);
 int ofg_mesh_get(const ofg_mesh* m, double* coords, int32_t* elem, int32_t* code, int64_t* dof);
 /* Node::setCoord for every node (coordinates only; topology unchanged). */
 int ofg_mesh_set_coords(ofg_mesh* m, const double* coords);

@@ -18,7 +18,7 @@ SOURCES = ["runtime.cu", "matrix.cu", "mesh.cu", "assembly.cu", "prec.cu", "kryl
            "meshio.cu", "entries.cu"]
 # per-source flags: the element arithmetic is kept free of fused multiply-adds
 # so that assembled values round exactly as OFELI's (separate multiply and add)
-EXTRA = {"assembly.cu": ["--fmad=false"]}
+EXTRA = {"assembly.cu": ["--fmad=false"], "batch.cu": ["--fmad=false"]}
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
          "-Xcompiler", "-fPIC", "-Xcompiler", "-O2", "--expt-relaxed-constexpr"]

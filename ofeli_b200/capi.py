@@ -54,7 +54,7 @@ SIGNATURES = {
     "ofg_mesh_create_kuhn": (_i32, [_i64, _pp]),
     "ofg_mesh_create": (_i32, [_i32, _i64, _p, _i64, _p, _p, _pp]),
     "ofg_mesh_destroy": (_i32, [_p]),
-    "ofg_mesh_info": (_i32, [_p, _pi32, _pi64, _pi64, _pi64, _pi32]),
+    "ofg_mesh_info": (_i32, [_p, _pi32, _pi64, _pi64, _pi64]),
     "ofg_mesh_get": (_i32, [_p, _p, _p, _p, _p]),
     "ofg_mesh_set_coords": (_i32, [_p, _p]),
     "ofg_matrix_create_from_mesh": (_i32, [_p, _pp]),

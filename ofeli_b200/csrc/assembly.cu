@@ -29,137 +29,6 @@ namespace {
 
 using namespace elem;
 
-// Each element kind computes row li of its element matrix and RHS -- the row
-// of the thread's own node i = en[li] -- with the arithmetic of the full
-// element computation (the same products and sums in the same order), and
-// lifts imposed values as Equation::updateBC does
-// (include/equations/Equation_impl.h:160-176): a column j whose DOF is
-// imposed (CSR position -1 in the element map) with code > 0 subtracts
-// Ke(li, j) * bc(en[j]).  Only the node's own source value and the imposed
-// columns' codes and values are loaded.
-
-template <int NEN>
-__device__ __forceinline__ void lift_row(const int32_t (&en)[NEN], const int32_t (&pos)[NEN],
-                                         const int32_t* code, const double* bc,
-                                         const double (&krow)[NEN], double& frow)
-{
-#pragma unroll
-   for (int j = 0; j < NEN; ++j)
-      if (pos[j] < 0 && code[en[j]] > 0) frow -= krow[j] * bc[en[j]];
-}
-
-// g[li] without dynamic register indexing
-template <int NEN>
-__device__ __forceinline__ void gradient_of(const double (&g)[NEN][3], int li, double (&gl)[3])
-{
-   gl[0] = g[0][0], gl[1] = g[0][1], gl[2] = g[0][2];
-#pragma unroll
-   for (int t = 1; t < NEN; ++t)
-      if (t == li) gl[0] = g[t][0], gl[1] = g[t][1], gl[2] = g[t][2];
-}
-
-// Laplace2DT3::LHS (times k) + BodyRHS: Ke = area*(g_i.g_j)*k, Fe = f*area/3
-// (src/equations/laplace/Laplace2DT3.cpp:131-143)
-struct LaplaceT3 {
-   static constexpr int NEN = 3;
-   const double* xy;
-   const int32_t* code;
-   const double* kel;
-   const double* f;
-   const double* bc;
-   __device__ __forceinline__ bool geometry_ok(const int32_t (&en)[3]) const
-   {
-      double g[3][3], area;
-      return tri3(xy, en, g, area);
-   }
-   __device__ __forceinline__ bool row(int64_t e, const int32_t (&en)[3], int li, int64_t node,
-                                       const int32_t (&pos)[3], double (&krow)[3],
-                                       double& frow) const
-   {
-      double g[3][3], area, gl[3];
-      if (!tri3(xy, en, g, area)) return false;
-      gradient_of<3>(g, li, gl);
-      const double k = kel ? kel[e] : 1.0;
-#pragma unroll
-      for (int j = 0; j < 3; ++j) krow[j] = area * dot3(gl, g[j]) * k;
-      frow = f ? f[node] * area * kThird : 0.0;
-      if (bc) lift_row<3>(en, pos, code, bc, krow, frow);
-      return true;
-   }
-};
-
-// DC3DT4::Diffusion(k) + BodyRHS: Ke = (k*vol)*(g_i.g_j), Fe = f*vol/4
-// (src/equations/therm/DC3DT4.cpp:128-135, 207-211)
-struct DiffusionT4 {
-   static constexpr int NEN = 4;
-   const double* xyz;
-   const int32_t* code;
-   const double* kel;
-   const double* f;
-   const double* bc;
-   __device__ __forceinline__ bool geometry_ok(const int32_t (&en)[4]) const
-   {
-      double g[4][3], vol;
-      return tet4(xyz, en, g, vol);
-   }
-   __device__ __forceinline__ bool row(int64_t e, const int32_t (&en)[4], int li, int64_t node,
-                                       const int32_t (&pos)[4], double (&krow)[4],
-                                       double& frow) const
-   {
-      double g[4][3], vol, gl[3];
-      if (!tet4(xyz, en, g, vol)) return false;
-      gradient_of<4>(g, li, gl);
-      const double c = (kel ? kel[e] : 1.0) * vol;
-#pragma unroll
-      for (int j = 0; j < 4; ++j) krow[j] = c * dot3(gl, g[j]);
-      frow = f ? f[node] * 0.25 * vol : 0.0;
-      if (bc) lift_row<4>(en, pos, code, bc, krow, frow);
-      return true;
-   }
-};
-
-// DC2DT3 under backward Euler (include/equations/therm/Equa_Therm.h:162-218):
-// eA1 = Capacity + LCapacity (src/equations/therm/DC2DT3.cpp:121-138),
-// eA0 = Diffusion(eps) + Convection (:141-147, 185-207),
-// eMat = eA1/dt + eA0, eRHS = updateBC + (eA1/dt) u_old.
-struct ConvDiffT3 {
-   static constexpr int NEN = 3;
-   const double* xy;
-   const int32_t* code;
-   double eps, dti;
-   const double* v;
-   const double* u_old;
-   const double* bc;
-   __device__ __forceinline__ bool geometry_ok(const int32_t (&en)[3]) const
-   {
-      double g[3][3], area;
-      return tri3(xy, en, g, area);
-   }
-   __device__ __forceinline__ bool row(int64_t, const int32_t (&en)[3], int li, int64_t,
-                                       const int32_t (&pos)[3], double (&krow)[3],
-                                       double& frow) const
-   {
-      double g[3][3], area, gl[3];
-      if (!tri3(xy, en, g, area)) return false;
-      gradient_of<3>(g, li, gl);
-      const double cc = kSixth * area, dd = 0.5 * cc, cl = kThird * area;
-      const double v3[3] = {v[2 * en[0]] + v[2 * en[1]] + v[2 * en[2]],
-                            v[2 * en[0] + 1] + v[2 * en[1] + 1] + v[2 * en[2] + 1], 0.0};
-      const double cv = kThird * kThird * area;
-      double m1row[3];
-#pragma unroll
-      for (int j = 0; j < 3; ++j) {
-         const double m1 = (li == j) ? cc + cl : dd;
-         m1row[j] = dti * m1;
-         krow[j] = m1row[j] + (eps * area * dot3(gl, g[j]) + cv * dot3(v3, g[j]));
-      }
-      frow = 0.0;
-      if (bc) lift_row<3>(en, pos, code, bc, krow, frow);
-      frow += m1row[0] * u_old[en[0]] + m1row[1] * u_old[en[1]] + m1row[2] * u_old[en[2]];
-      return true;
-   }
-};
-
 // One thread per node: the node's CSR row and RHS entry, gathered over its
 // elements in ascending order (see the file comment).
 template <class Elem>
@@ -172,50 +41,12 @@ __global__ void __launch_bounds__(256) assemble_rows(int64_t nn, const int32_t* 
                                                      double* __restrict__ a, double* __restrict__ b,
                                                      int* bad)
 {
-   constexpr int NEN = Elem::NEN;
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += stride) {
       const int32_t r = dof[i];   // 1-based equation, 0 for an imposed node
-      if (r)
-         for (int32_t k = row_ptr[r - 1]; k < row_ptr[r]; ++k) a[k] = 0.0;
-      double bi = 0.0;
-      const int32_t q0 = n2e_ptr[i], q1 = n2e_ptr[i + 1];
-      int64_t e_next = q0 < q1 ? n2e[q0] : 0;
-      int32_t en_next[NEN];
-#pragma unroll
-      for (int j = 0; j < NEN; ++j) en_next[j] = q0 < q1 ? elem[NEN * e_next + j] : 0;
-      for (int32_t q = q0; q < q1; ++q) {
-         const int64_t e = e_next;
-         int32_t en[NEN];
-#pragma unroll
-         for (int j = 0; j < NEN; ++j) en[j] = en_next[j];
-         if (q + 1 < q1) {
-            e_next = n2e[q + 1];
-#pragma unroll
-            for (int j = 0; j < NEN; ++j) en_next[j] = elem[NEN * e_next + j];
-         }
-         int li = 0;
-#pragma unroll
-         for (int j = NEN - 1; j > 0; --j)
-            if (en[j] == (int32_t)i) li = j;
-         if (!r) {   // no row here: only the Jacobian check of the elements it leads
-            if (li == 0 && !el.geometry_ok(en)) atomicMin(bad, (int)e);
-            continue;
-         }
-         int32_t pos[NEN];
-         const int32_t* mp = emap + (e * NEN + li) * NEN;
-#pragma unroll
-         for (int j = 0; j < NEN; ++j) pos[j] = mp[j];
-         double krow[NEN], frow;
-         if (!el.row(e, en, li, i, pos, krow, frow)) {
-            if (li == 0) atomicMin(bad, (int)e);
-            continue;
-         }
-#pragma unroll
-         for (int j = 0; j < NEN; ++j)
-            if (pos[j] >= 0) a[pos[j]] += krow[j];
-         bi += frow;
-      }
+      const double bi =
+         gather_node_rows(i, r, n2e_ptr[i], n2e_ptr[i + 1], n2e, elem, emap, row_ptr, el, a,
+                          [&](int64_t e) { atomicMin(bad, (int)e); });
       if (r) b[r - 1] = bi;
    }
 }

@@ -1,10 +1,11 @@
 // batch.cu -- many independent P1 problems of uneven size, assembled and
 // solved in one persistent launch.
 //
-// The problems' meshes, patterns, element-to-CSR maps and element colourings
-// are concatenated once (ofg_batch_create).  One launch of batch_kernel then
-// does, for every problem: Equation::build() (coloured, atomic-free element
-// scatter, the colours separated by block barriers), CG with the diagonal
+// The problems' meshes, patterns, element-to-CSR maps and node-to-element
+// lists are concatenated once (ofg_batch_create).  One launch of
+// batch_kernel then does, for every problem: Equation::build() (each node
+// gathers its CSR row over its elements in ascending order, as the
+// single-problem kernel does, so the values are OFELI's bit for bit), CG with the diagonal
 // preconditioner in FP64 (OFELI's CG recurrence, include/solvers/CG.h:99-157)
 // to the relative residual `toler`, a check of the FP64 true residual
 // ||b - A x|| / ||b|| (the iteration continues from the true residual if the
@@ -13,8 +14,8 @@
 // Work is taken from a queue, most work first.  Without clusters a block owns
 // one problem at a time, so all reductions are block-local.  With
 // thread-block clusters (4 or 8 blocks) a problem larger than one block's
-// fair share of the total is solved by the whole cluster -- rows, nonzeros,
-// element colours and nodes split among its blocks, cluster barriers
+// fair share of the total is solved by the whole cluster -- rows, nonzeros
+// and nodes split among its blocks, cluster barriers
 // between the phases, dot products summed over the blocks in rank order
 // through distributed shared memory -- and smaller problems are taken one
 // per block of the cluster, so that the largest problems no longer set the
@@ -36,8 +37,8 @@ namespace {
 using namespace elem;
 
 struct BatchProblem {
-   int64_t node_off, elem_off, row_off, rp_off, nnz_off, color_base;
-   int32_t nn, ne, n, ncolors;
+   int64_t node_off, elem_off, row_off, rp_off, nnz_off, n2p_off, n2e_off;
+   int32_t nn, ne, n, pad;
 };
 
 // a work item: `count` problems order[first ..] taken one per block of a
@@ -57,8 +58,8 @@ struct BatchArgs {
    const int32_t* elem;
    const int32_t* code;
    const int32_t* dof;
-   const int64_t* color_ptr;
-   const int32_t* color_elems;
+   const int32_t* n2e_ptr;   // node-to-element lists, per problem (nn + 1 entries)
+   const int32_t* n2e;
    const int32_t* emap;
    // matrices and vectors
    const int32_t* row_ptr;
@@ -148,7 +149,7 @@ __device__ __forceinline__ int ld_cluster(const int* p, unsigned rank)
 
 // The blocks working on one problem: one block (size 1: block barriers and
 // block reductions), or the whole cluster (size > 1: each block owns a
-// contiguous share of rows, nonzeros, element colours and nodes; cluster
+// contiguous share of rows, nonzeros and nodes; cluster
 // barriers; reductions summed over the blocks in rank order through
 // distributed shared memory, double-buffered exchange slots).
 template <int THREADS>
@@ -373,50 +374,28 @@ __device__ void solve_problem(const BatchArgs& a, int pid, Team<THREADS>& T)
    const int nnz = rp[n];
    const int r0 = (int)T.lo(n), r1 = (int)T.hi(n);
 
-   // ---- Equation::build(): zero, then one pass per element colour
-   for (int64_t k = T.lo(nnz) + tid; k < T.hi(nnz); k += THREADS) val[k] = 0.0;
-   for (int i = r0 + tid; i < r1; i += THREADS) b[i] = 0.0;
-   T.bar();
-   for (int c = 0; c < P.ncolors; ++c) {
-      const int64_t beg = a.color_ptr[P.color_base + c];
-      const int64_t cnt = a.color_ptr[P.color_base + c + 1] - beg;
-      for (int64_t t = beg + T.lo(cnt) + tid; t < beg + T.hi(cnt); t += THREADS) {
-         const int64_t e = a.color_elems[P.elem_off + t];
-         const int32_t* ep = a.elem + (P.elem_off + e) * NEN;
-         int32_t en[NEN];
-#pragma unroll
-         for (int i = 0; i < NEN; ++i) en[i] = ep[i];
-         // Laplace2DT3::LHS (times k) + BodyRHS, or DC3DT4::Diffusion(k) +
-         // BodyRHS: the operation order of the single-problem kernels
-         double g[NEN][3], meas;
-         bool ok;
-         if constexpr (NEN == 3) ok = tri3(xy, en, g, meas);
-         else ok = tet4(xy, en, g, meas);
-         if (!ok) {
-            atomicMin(a.bad, (int)(P.elem_off + e));
-            continue;
-         }
-         const double k = a.kel ? a.kel[P.elem_off + e] : 1.0;
-         double Ke[NEN][NEN], Fe[NEN];
-         if constexpr (NEN == 3) {
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-               for (int j = 0; j < 3; ++j) Ke[i][j] = meas * dot3(g[i], g[j]) * k;
-#pragma unroll
-            for (int i = 0; i < 3; ++i) Fe[i] = a.f ? a.f[P.node_off + en[i]] * meas * kThird : 0.0;
-         }
-         else {
-            const double c4 = k * meas;
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-               for (int j = 0; j < 4; ++j) Ke[i][j] = c4 * dot3(g[i], g[j]);
-#pragma unroll
-            for (int i = 0; i < 4; ++i) Fe[i] = a.f ? a.f[P.node_off + en[i]] * 0.25 * meas : 0.0;
-         }
-         if (a.bc) lift_bc<NEN>(en, code, a.bc + P.node_off, Ke, Fe);
-         scatter<NEN>(P.elem_off + e, en, dof, a.emap, Ke, Fe, val, b);
+   // ---- Equation::build(): each node gathers its CSR row and RHS entry
+   // over its elements in ascending order (the single-problem kernel's
+   // arithmetic and order: OFELI's values bit for bit)
+   {
+      const int32_t* np = a.n2e_ptr + P.n2p_off;
+      const int32_t* lists = a.n2e + P.n2e_off;
+      const int32_t* elem = a.elem + P.elem_off * NEN;
+      const int32_t* emap = a.emap + P.elem_off * NEN * NEN;
+      const double* kel = a.kel ? a.kel + P.elem_off : nullptr;
+      const double* f = a.f ? a.f + P.node_off : nullptr;
+      const double* bc = a.bc ? a.bc + P.node_off : nullptr;
+      auto report = [&](int64_t e) { atomicMin(a.bad, (int)(P.elem_off + e)); };
+      for (int64_t i = T.lo(P.nn) + tid; i < T.hi(P.nn); i += THREADS) {
+         const int32_t ri = dof[i];
+         double bi;
+         if constexpr (NEN == 3)
+            bi = gather_node_rows(i, ri, np[i], np[i + 1], lists, elem, emap, rp,
+                                  LaplaceT3{xy, code, kel, f, bc}, val, report);
+         else
+            bi = gather_node_rows(i, ri, np[i], np[i + 1], lists, elem, emap, rp,
+                                  DiffusionT4{xy, code, kel, f, bc}, val, report);
+         if (ri) b[ri - 1] = bi;
       }
       T.bar();
    }
@@ -676,8 +655,7 @@ struct ofg_batch {
    ofg::DBuf<int32_t> order;
    ofg::DBuf<int> queue, bad, iters;
    ofg::DBuf<double> coords;
-   ofg::DBuf<int32_t> elem, code, dof, color_elems, emap, row_ptr, col, dpos;
-   ofg::DBuf<int64_t> color_ptr;
+   ofg::DBuf<int32_t> elem, code, dof, n2e_ptr, n2e, emap, row_ptr, col, dpos;
    ofg::DBuf<double> val, b, x, r, p, q, dinv, kel, f, bc, u, res;
    bool have_bc = false;
    int config = 4;  // index into kConfigs
@@ -722,8 +700,8 @@ BatchArgs args_of(ofg_batch* B)
    a.elem = B->elem.p;
    a.code = B->code.p;
    a.dof = B->dof.p;
-   a.color_ptr = B->color_ptr.p;
-   a.color_elems = B->color_elems.p;
+   a.n2e_ptr = B->n2e_ptr.p;
+   a.n2e = B->n2e.p;
    a.emap = B->emap.p;
    a.row_ptr = B->row_ptr.p;
    a.col = B->col.p;
@@ -897,7 +875,6 @@ int ofg_batch_create(int nprob, ofg_mesh* const* meshes, ofg_batch** out)
          B->dim = meshes[0]->dim;
          B->nen = meshes[0]->nen;
          std::vector<ofg_matrix*> mats(nprob, nullptr);
-         int64_t ncolor_tot = 0;
          for (int p = 0; p < nprob; ++p) {
             ofg_mesh* m = meshes[p];
             OFG_REQUIRE(m && m->dim == B->dim, OFG_ERR_ARG, "batch meshes must share one dimension");
@@ -911,18 +888,18 @@ int ofg_batch_create(int nprob, ofg_mesh* const* meshes, ofg_batch** out)
             P.row_off = B->nrows;
             P.rp_off = B->nrows + p;
             P.nnz_off = B->nnz;
-            P.color_base = ncolor_tot + p;
+            P.n2p_off = B->nn + p;
+            P.n2e_off = B->ne * m->nen;
             P.nn = (int32_t)m->nn;
             P.ne = (int32_t)m->ne;
             P.n = (int32_t)mats[p]->n;
-            ensure_colors(m);
-            P.ncolors = (int32_t)m->color_ptr.size() - 1;
+
             B->probs.push_back(P);
             B->nn += m->nn;
             B->ne += m->ne;
             B->nrows += mats[p]->n;
             B->nnz += mats[p]->nnz;
-            ncolor_tot += P.ncolors;
+
             ensure_dpos(mats[p]);
             OFG_REQUIRE(mats[p]->dpos_complete, OFG_ERR_PIVOT, "a row has no diagonal entry");
          }
@@ -932,12 +909,12 @@ int ofg_batch_create(int nprob, ofg_mesh* const* meshes, ofg_batch** out)
          B->elem.alloc(B->ne * nen);
          B->code.alloc(B->nn);
          B->dof.alloc(B->nn);
-         B->color_elems.alloc(B->ne);
+         B->n2e_ptr.alloc(B->nn + nprob);
+         B->n2e.alloc(B->ne * nen);
          B->emap.alloc(B->ne * nen * nen);
          B->row_ptr.alloc(B->nrows + nprob);
          B->col.alloc(B->nnz);
          B->dpos.alloc(B->nrows);
-         std::vector<int64_t> cptr;
          for (int p = 0; p < nprob; ++p) {
             ofg_mesh* m = meshes[p];
             ofg_matrix* A = mats[p];
@@ -946,15 +923,13 @@ int ofg_batch_create(int nprob, ofg_mesh* const* meshes, ofg_batch** out)
             gather(B->elem, P.elem_off * nen, m->elem.p, m->ne * nen);
             gather(B->code, P.node_off, m->code.p, m->nn);
             gather(B->dof, P.node_off, m->dof.p, m->nn);
-            gather(B->color_elems, P.elem_off, m->color_elems.p, m->ne);
+            gather(B->n2e_ptr, P.n2p_off, m->n2e_ptr.p, m->nn + 1);
+            gather(B->n2e, P.n2e_off, m->n2e.p, m->ne * nen);
             gather(B->emap, P.elem_off * nen * nen, A->emap.p, m->ne * nen * nen);
             gather(B->row_ptr, P.rp_off, A->row_ptr.p, A->n + 1);
             gather(B->col, P.nnz_off, A->col.p, A->nnz);
             gather(B->dpos, P.row_off, A->dpos.p, A->n);
-            cptr.insert(cptr.end(), m->color_ptr.begin(), m->color_ptr.end());
          }
-         B->color_ptr.alloc(cptr.size());
-         B->color_ptr.upload(cptr.data(), cptr.size());
          OFG_CUDA(cudaStreamSynchronize(stream()));
          for (auto* A : mats) delete A;
          // work estimate until iteration counts are measured: rows x

@@ -1,6 +1,6 @@
-// element.cuh -- P1 element geometry, element matrices' building blocks and
-// the scatter into CSR values, shared by the assembly kernels (assembly.cu)
-// and the batched solver (batch.cu).
+// element.cuh -- P1 element geometry, the element rows of the equations on
+// the path and the row gather into CSR values, shared by the assembly kernel
+// (assembly.cu) and the batched solver (batch.cu).
 #pragma once
 
 #include "internal.cuh"
@@ -69,38 +69,194 @@ __device__ __forceinline__ bool tet4(const double* xyz, const int32_t* en, doubl
    return true;
 }
 
+// Each element kind computes row li of its element matrix and RHS -- the row
+// of the thread's own node i = en[li] -- with the arithmetic of the full
+// element computation (the same products and sums in the same order), and
+// lifts imposed values as Equation::updateBC does
+// (include/equations/Equation_impl.h:160-176): a column j whose DOF is
+// imposed (CSR position -1 in the element map) with code > 0 subtracts
+// Ke(li, j) * bc(en[j]).  Only the node's own source value and the imposed
+// columns' codes and values are loaded.
+
 template <int NEN>
-__device__ __forceinline__ void scatter(int64_t e, const int32_t* en, const int32_t* dof,
-                                        const int32_t* __restrict__ emap, const double (&Ke)[NEN][NEN],
-                                        const double (&Fe)[NEN], double* a, double* b)
+__device__ __forceinline__ void lift_row(const int32_t (&en)[NEN], const int32_t (&pos)[NEN],
+                                         const int32_t* code, const double* bc,
+                                         const double (&krow)[NEN], double& frow)
 {
-   const int32_t* mp = emap + e * NEN * NEN;
 #pragma unroll
-   for (int i = 0; i < NEN; ++i) {
-      int32_t r = dof[en[i]];
-      if (!r) continue;
-#pragma unroll
-      for (int j = 0; j < NEN; ++j) {
-         int32_t pos = mp[i * NEN + j];
-         if (pos >= 0) a[pos] += Ke[i][j];
-      }
-      b[r - 1] += Fe[i];
-   }
+   for (int j = 0; j < NEN; ++j)
+      if (pos[j] < 0 && code[en[j]] > 0) frow -= krow[j] * bc[en[j]];
 }
 
-// Equation::updateBC (include/equations/Equation_impl.h:160-176)
+// g[li] without dynamic register indexing
 template <int NEN>
-__device__ __forceinline__ void lift_bc(const int32_t* en, const int32_t* code, const double* bc,
-                                        const double (&Ke)[NEN][NEN], double (&Fe)[NEN])
+__device__ __forceinline__ void gradient_of(const double (&g)[NEN][3], int li, double (&gl)[3])
 {
+   gl[0] = g[0][0], gl[1] = g[0][1], gl[2] = g[0][2];
 #pragma unroll
-   for (int j = 0; j < NEN; ++j) {
-      if (code[en[j]] > 0) {
-         double v = bc[en[j]];
-#pragma unroll
-         for (int i = 0; i < NEN; ++i) Fe[i] -= Ke[i][j] * v;
-      }
+   for (int t = 1; t < NEN; ++t)
+      if (t == li) gl[0] = g[t][0], gl[1] = g[t][1], gl[2] = g[t][2];
+}
+
+// Laplace2DT3::LHS (times k) + BodyRHS: Ke = area*(g_i.g_j)*k, Fe = f*area/3
+// (src/equations/laplace/Laplace2DT3.cpp:131-143)
+struct LaplaceT3 {
+   static constexpr int NEN = 3;
+   const double* xy;
+   const int32_t* code;
+   const double* kel;
+   const double* f;
+   const double* bc;
+   __device__ __forceinline__ bool geometry_ok(const int32_t (&en)[3]) const
+   {
+      double g[3][3], area;
+      return tri3(xy, en, g, area);
    }
+   __device__ __forceinline__ bool row(int64_t e, const int32_t (&en)[3], int li, int64_t node,
+                                       const int32_t (&pos)[3], double (&krow)[3],
+                                       double& frow) const
+   {
+      double g[3][3], area, gl[3];
+      if (!tri3(xy, en, g, area)) return false;
+      gradient_of<3>(g, li, gl);
+      const double k = kel ? kel[e] : 1.0;
+#pragma unroll
+      for (int j = 0; j < 3; ++j) krow[j] = area * dot3(gl, g[j]) * k;
+      frow = f ? f[node] * area * kThird : 0.0;
+      if (bc) lift_row<3>(en, pos, code, bc, krow, frow);
+      return true;
+   }
+};
+
+// DC3DT4::Diffusion(k) + BodyRHS: Ke = (k*vol)*(g_i.g_j), Fe = f*vol/4
+// (src/equations/therm/DC3DT4.cpp:128-135, 207-211)
+struct DiffusionT4 {
+   static constexpr int NEN = 4;
+   const double* xyz;
+   const int32_t* code;
+   const double* kel;
+   const double* f;
+   const double* bc;
+   __device__ __forceinline__ bool geometry_ok(const int32_t (&en)[4]) const
+   {
+      double g[4][3], vol;
+      return tet4(xyz, en, g, vol);
+   }
+   __device__ __forceinline__ bool row(int64_t e, const int32_t (&en)[4], int li, int64_t node,
+                                       const int32_t (&pos)[4], double (&krow)[4],
+                                       double& frow) const
+   {
+      double g[4][3], vol, gl[3];
+      if (!tet4(xyz, en, g, vol)) return false;
+      gradient_of<4>(g, li, gl);
+      const double c = (kel ? kel[e] : 1.0) * vol;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) krow[j] = c * dot3(gl, g[j]);
+      frow = f ? f[node] * 0.25 * vol : 0.0;
+      if (bc) lift_row<4>(en, pos, code, bc, krow, frow);
+      return true;
+   }
+};
+
+// DC2DT3 under backward Euler (include/equations/therm/Equa_Therm.h:162-218):
+// eA1 = Capacity + LCapacity (src/equations/therm/DC2DT3.cpp:121-138),
+// eA0 = Diffusion(eps) + Convection (:141-147, 185-207),
+// eMat = eA1/dt + eA0, eRHS = updateBC + (eA1/dt) u_old.
+struct ConvDiffT3 {
+   static constexpr int NEN = 3;
+   const double* xy;
+   const int32_t* code;
+   double eps, dti;
+   const double* v;
+   const double* u_old;
+   const double* bc;
+   __device__ __forceinline__ bool geometry_ok(const int32_t (&en)[3]) const
+   {
+      double g[3][3], area;
+      return tri3(xy, en, g, area);
+   }
+   __device__ __forceinline__ bool row(int64_t, const int32_t (&en)[3], int li, int64_t,
+                                       const int32_t (&pos)[3], double (&krow)[3],
+                                       double& frow) const
+   {
+      double g[3][3], area, gl[3];
+      if (!tri3(xy, en, g, area)) return false;
+      gradient_of<3>(g, li, gl);
+      const double cc = kSixth * area, dd = 0.5 * cc, cl = kThird * area;
+      const double v3[3] = {v[2 * en[0]] + v[2 * en[1]] + v[2 * en[2]],
+                            v[2 * en[0] + 1] + v[2 * en[1] + 1] + v[2 * en[2] + 1], 0.0};
+      const double cv = kThird * kThird * area;
+      double m1row[3];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+         const double m1 = (li == j) ? cc + cl : dd;
+         m1row[j] = dti * m1;
+         krow[j] = m1row[j] + (eps * area * dot3(gl, g[j]) + cv * dot3(v3, g[j]));
+      }
+      frow = 0.0;
+      if (bc) lift_row<3>(en, pos, code, bc, krow, frow);
+      frow += m1row[0] * u_old[en[0]] + m1row[1] * u_old[en[1]] + m1row[2] * u_old[en[2]];
+      return true;
+   }
+};
+
+// The rows of one node, gathered over its elements in ascending order:
+// zeroes the node's CSR row (when it has an equation), adds its row of each
+// element there and returns the RHS entry; the Jacobian of an element is
+// checked by the thread of its first node and a bad element reported through
+// report(e).  Used by the single-problem kernel (assembly.cu) and the
+// batched solver (batch.cu).  The connectivity of the next element is loaded
+// while the current one is computed.
+template <class Elem, class Report>
+__device__ __forceinline__ double gather_node_rows(int64_t i, int32_t r, int32_t q0, int32_t q1,
+                                                   const int32_t* __restrict__ n2e,
+                                                   const int32_t* __restrict__ elem,
+                                                   const int32_t* __restrict__ emap,
+                                                   const int32_t* __restrict__ row_ptr,
+                                                   const Elem& el, double* __restrict__ a,
+                                                   Report&& report)
+{
+   constexpr int NEN = Elem::NEN;
+   if (r)
+      for (int32_t k = row_ptr[r - 1]; k < row_ptr[r]; ++k) a[k] = 0.0;
+   double bi = 0.0;
+   int64_t e_next = q0 < q1 ? n2e[q0] : 0;
+   int32_t en_next[NEN];
+#pragma unroll
+   for (int j = 0; j < NEN; ++j) en_next[j] = q0 < q1 ? elem[NEN * e_next + j] : 0;
+   for (int32_t q = q0; q < q1; ++q) {
+      const int64_t e = e_next;
+      int32_t en[NEN];
+#pragma unroll
+      for (int j = 0; j < NEN; ++j) en[j] = en_next[j];
+      if (q + 1 < q1) {
+         e_next = n2e[q + 1];
+#pragma unroll
+         for (int j = 0; j < NEN; ++j) en_next[j] = elem[NEN * e_next + j];
+      }
+      int li = 0;
+#pragma unroll
+      for (int j = NEN - 1; j > 0; --j)
+         if (en[j] == (int32_t)i) li = j;
+      if (!r) {   // no row here: only the Jacobian check of the elements it leads
+         if (li == 0 && !el.geometry_ok(en)) report(e);
+         continue;
+      }
+      int32_t pos[NEN];
+      const int32_t* mp = emap + (e * NEN + li) * NEN;
+#pragma unroll
+      for (int j = 0; j < NEN; ++j) pos[j] = mp[j];
+      double krow[NEN], frow;
+      if (!el.row(e, en, li, i, pos, krow, frow)) {
+         if (li == 0) report(e);
+         continue;
+      }
+#pragma unroll
+      for (int j = 0; j < NEN; ++j)
+         if (pos[j] >= 0) a[pos[j]] += krow[j];
+      bi += frow;
+   }
+   return bi;
 }
 
 }  // namespace elem

@@ -58,11 +58,6 @@ struct ofg_mesh {
    ofg::DBuf<int32_t> dof;    // nn, 1-based equation number or 0
    // node -> element adjacency (elements in ascending order)
    ofg::DBuf<int32_t> n2e_ptr, n2e;
-   // element colouring (the batched solver's assembly; built by
-   // ofg::ensure_colors on first use): elements of colour c are
-   // color_elems[color_ptr[c] .. color_ptr[c+1]); no two share a node
-   std::vector<int64_t> color_ptr;
-   ofg::DBuf<int32_t> color_elems;
    // the structured rectangle's cells and line codes (rect_nx < 0 otherwise),
    // kept for the sides Mesh::put writes
    int64_t rect_nx = -1, rect_ny = -1;
@@ -134,8 +129,6 @@ void spmv_csr(const ofg_matrix* A, const double* x, double* y, bool add);
 void spmv_sell(const ofg_matrix* A, const double* x, double* y, const int* skip = nullptr);
 void matrix_touch(ofg_matrix* A);
 void matrix_finish_pattern(ofg_matrix* A);
-// element colouring of a mesh, computed on first use (mesh.cu)
-void ensure_colors(ofg_mesh* m);
 // a mesh with its coordinate, connectivity and code buffers allocated, and
 // the rest (equation numbers from the codes, node-to-element lists) built
 // once those hold the mesh (mesh.cu)

@@ -11,9 +11,8 @@
 //     (dof_i, dof_j) pair of every element, sorts and uniques.  Here each row
 //     gathers the DOFs of the elements around its node, sorts and uniques
 //     them in registers: same set, same order, no global sort.
-//   * element colouring (sequential greedy on the host, node bitmasks) makes
-//     the assembly scatter free of atomics: elements of one colour share no
-//     node, hence no CSR row.
+//   * node-to-element lists (elements ascending per node), from which the
+//     assembly gathers each row in OFELI's element order.
 #include <algorithm>
 #include <numeric>
 
@@ -287,37 +286,6 @@ ofg_mesh* new_mesh(int dim, int64_t nn, int64_t ne)
    return m;
 }
 
-// Element colouring for the batched solver's block-level assembly (computed
-// on first use): greedy on the host, the colour of an element is the lowest
-// one not yet used by any element touching one of its nodes.
-void ensure_colors(ofg_mesh* m)
-{
-   if (!m->color_ptr.empty()) return;
-   const int64_t nn = m->nn, ne = m->ne;
-   std::vector<int32_t> el = m->elem.to_host(ne * m->nen);
-   std::vector<uint64_t> used(nn, 0);
-   std::vector<int32_t> color(ne);
-   int ncol = 0;
-   for (int64_t e = 0; e < ne; ++e) {
-      uint64_t u = 0;
-      for (int a = 0; a < m->nen; ++a) u |= used[el[e * m->nen + a]];
-      OFG_REQUIRE(~u != 0, OFG_ERR_PATTERN, "more than 64 element colours needed");
-      int c = __builtin_ctzll(~u);
-      color[e] = c;
-      ncol = std::max(ncol, c + 1);
-      for (int a = 0; a < m->nen; ++a) used[el[e * m->nen + a]] |= (1ULL << c);
-   }
-   m->color_ptr.assign(ncol + 1, 0);
-   for (int64_t e = 0; e < ne; ++e) m->color_ptr[color[e] + 1]++;
-   for (int c = 0; c < ncol; ++c) m->color_ptr[c + 1] += m->color_ptr[c];
-   std::vector<int32_t> order(ne);
-   std::vector<int64_t> fillp(m->color_ptr.begin(), m->color_ptr.end() - 1);
-   for (int64_t e = 0; e < ne; ++e) order[fillp[color[e]]++] = (int32_t)e;
-   m->color_elems.alloc(ne > 0 ? ne : 1);
-   if (ne) m->color_elems.upload(order.data(), ne);
-   OFG_CUDA(cudaStreamSynchronize(stream()));   // `order` is a pageable source
-}
-
 }  // namespace ofg
 
 using namespace ofg;
@@ -426,7 +394,7 @@ int ofg_mesh_destroy(ofg_mesh* m)
    });
 }
 
-int ofg_mesh_info(const ofg_mesh* m, int* dim, int64_t* nn, int64_t* ne, int64_t* neq, int* ncolors)
+int ofg_mesh_info(const ofg_mesh* m, int* dim, int64_t* nn, int64_t* ne, int64_t* neq)
 {
    return guarded("ofg_mesh_info", [&] {
       OFG_REQUIRE(m, OFG_ERR_ARG, "null mesh");
@@ -434,7 +402,6 @@ int ofg_mesh_info(const ofg_mesh* m, int* dim, int64_t* nn, int64_t* ne, int64_t
       if (nn) *nn = m->nn;
       if (ne) *ne = m->ne;
       if (neq) *neq = m->neq;
-      if (ncolors) *ncolors = m->color_ptr.empty() ? 0 : (int)m->color_ptr.size() - 1;
    });
 }
 

@@ -1287,7 +1287,7 @@ int ofg_mesh_file_from_mesh(const ofg_mesh* m, ofg_mesh_file** out)
       OFG_REQUIRE(m && out, OFG_ERR_ARG, "null argument");
       int dim = 0;
       int64_t nn = 0, ne = 0;
-      OFG_REQUIRE(ofg_mesh_info(m, &dim, &nn, &ne, nullptr, nullptr) == OFG_OK, OFG_ERR_ARG,
+      OFG_REQUIRE(ofg_mesh_info(m, &dim, &nn, &ne, nullptr) == OFG_OK, OFG_ERR_ARG,
                   ofg_last_error());
       std::unique_ptr<ofg_mesh_file> f(new ofg_mesh_file());
       f->dim = dim, f->nb_dof = 1, f->nn = nn, f->ne = ne;

@@ -97,11 +97,11 @@ class Mesh:
         return cls(_handle=h)
 
     def _info(self):
-        d, nc = ctypes.c_int(), ctypes.c_int()
+        d = ctypes.c_int()
         nn, ne, neq = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
         _call("ofg_mesh_info", self._h, ctypes.byref(d), ctypes.byref(nn), ctypes.byref(ne),
-              ctypes.byref(neq), ctypes.byref(nc))
-        self.dim, self.nn, self.ne, self.neq, self.ncolors = d.value, nn.value, ne.value, neq.value, nc.value
+              ctypes.byref(neq))
+        self.dim, self.nn, self.ne, self.neq = d.value, nn.value, ne.value, neq.value
 
     def getNbNodes(self):
         return self.nn

@@ -48,7 +48,7 @@ def test_null_arguments_are_rejected_with_status():
     assert b"null" in L.ofg_last_error()
     assert L.ofg_spmv(None, None, None) == -1
     assert L.ofg_prec_create(None, 1, None) == -1
-    assert L.ofg_mesh_info(None, None, None, None, None, None) == -1
+    assert L.ofg_mesh_info(None, None, None, None, None) == -1
 
 
 def test_profile_family_names():
