@@ -66,6 +66,11 @@ int ofg_init(int device);
 /* Waits for the library's work and frees its process-wide buffers (the mesh
  * reader's pinned staging buffer); handles stay valid. */
 int ofg_shutdown(void);
+/* Failure detection check: one device thread waits, with the bounded wait
+ * of the triangular sweeps, for a value that nothing produces; the call
+ * returns OFG_ERR_TIMEOUT after about two seconds and the context stays
+ * usable.  No counterpart in OFELI. */
+int ofg_selftest_wait(void);
 /* Selects the stream used by later calls (NULL = the library's own). */
 int ofg_set_stream(void* cuda_stream);
 void* ofg_get_stream(void);

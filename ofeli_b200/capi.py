@@ -34,6 +34,7 @@ SIGNATURES = {
     "ofg_launch_count": (_i64, []),
     "ofg_init": (_i32, [_i32]),
     "ofg_shutdown": (_i32, []),
+    "ofg_selftest_wait": (_i32, []),
     "ofg_profile_enable": (_i32, [_i32]),
     "ofg_profile_read": (_i32, [ctypes.c_char_p, _pi64, _pd, _pd]),
     "ofg_matrix_create": (_i32, [_i64, _i64, _p, _p, _pp]),

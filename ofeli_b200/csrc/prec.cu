@@ -95,6 +95,12 @@ __device__ __forceinline__ double wait_value(const double* p, int* status)
    return is_sentinel(v) ? wait_value_slow(p, status) : v;
 }
 
+// One thread waits, as a sweep does, for a value that nothing produces.
+__global__ void wait_selftest(const double* p, int* status, double* out)
+{
+   if (blockIdx.x == 0 && threadIdx.x == 0) *out = wait_value(p, status);
+}
+
 template <int MODE>
 __device__ __forceinline__ double finish_row(double s, double bi, double pv)
 {
@@ -950,6 +956,23 @@ int ofg_prec_apply(ofg_prec* P, const double* b, double* x)
       prec_apply_device(P, db.d, dx.d);
       dx.finish();
       check_status(P);
+   });
+}
+
+int ofg_selftest_wait(void)
+{
+   return guarded("ofg_selftest_wait", [&] {
+      DBuf<double> cell(2);
+      DBuf<int> status(1);
+      status.zero();
+      fill_sentinel(cell.p, 1);
+      wait_selftest<<<1, 32, 0, stream()>>>(cell.p, status.p, cell.p + 1);
+      count_launch();
+      OFG_LAUNCH_CHECK();
+      int h = 0;
+      status.download(&h, 1);
+      if (h) throw Error(OFG_ERR_TIMEOUT, "the bounded wait ran out, as intended");
+      throw Error(OFG_ERR_ARG, "the wait ended without its value");
    });
 }
 

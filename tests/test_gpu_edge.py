@@ -148,3 +148,46 @@ def test_kernels_are_launched(cuda):
     A = F.SpMatrix(rp, ci, a)
     F.CG(A, F.Prec(A, F.ILU_PREC), b, np.zeros(A.n), 100, 1e-10)
     assert capi.launch_count() - before > 10
+
+
+def test_bounded_wait_times_out_and_context_survives(cuda):
+    """Failure detection without a fault: a device wait on a value nothing
+    produces ends with OFG_ERR_TIMEOUT (the sweeps' bounded wait), and the
+    next solve on the same context works."""
+    from ofeli_b200 import capi
+    rc = capi.lib().ofg_selftest_wait()
+    assert rc == -6, capi.lib().ofg_last_error()
+    xy, elem, code = O.mesh2d(8, 8)
+    dof, n = O.number_equations(code)
+    rp, ci = O.node_graph(elem, 3, dof, n)
+    a, b = O.assemble(2, xy, elem, dof, code, n, rp, ci, f=np.ones(code.size))
+    A = F.SpMatrix(rp, ci, a)
+    x = np.zeros(n)
+    it = F.CG(A, F.Prec(A, F.DILU_PREC), b, x, 100, 1e-10)
+    _, it0 = O.cg(rp, ci, a, b, O.DILU, 100, 1e-10)
+    assert it == it0 > 0
+
+
+@pytest.mark.parametrize("solver", ["CG", "GMRES"])
+def test_nan_rhs_returns_like_oracle(cuda, solver):
+    """A NaN in b (host-side fault injection): the solvers run to their
+    iteration cap and return OFELI's failure code, as the oracle does; no
+    hang, and the context stays usable."""
+    xy, elem, code = O.mesh2d(8, 8)
+    dof, n = O.number_equations(code)
+    rp, ci = O.node_graph(elem, 3, dof, n)
+    a, b = O.assemble(2, xy, elem, dof, code, n, rp, ci, f=np.ones(code.size))
+    b = b.copy()
+    b[5] = np.nan
+    A = F.SpMatrix(rp, ci, a)
+    x = np.zeros(n)
+    if solver == "CG":
+        it = F.CG(A, F.Prec(A, F.DIAG_PREC), b, x, 20, 1e-10)
+        _, it0 = O.cg(rp, ci, a, b, O.DIAG, 20, 1e-10)
+    else:
+        it = F.GMRes(A, F.Prec(A, F.DIAG_PREC), b, x, 5, 20, 1e-10)
+        _, it0 = O.gmres(rp, ci, a, b, O.DIAG, 5, 20, 1e-10)
+    assert it == it0 and it <= 0
+    x2 = np.zeros(n)
+    b2 = np.nan_to_num(b)
+    assert F.CG(A, F.Prec(A, F.DIAG_PREC), b2, x2, 200, 1e-10) > 0
