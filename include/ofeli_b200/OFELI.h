@@ -44,6 +44,9 @@ inline void ofg_check(int status, const char* what)
       throw OFELIException(std::string(what) + ": " + ofg_last_error());
 }
 
+// OFELI's time schemes on the path (include/equations/Equa.h:124-137)
+enum TimeScheme { NONE = 0, FORWARD_EULER = 1, BACKWARD_EULER = 2, CRANK_NICOLSON = 3 };
+
 enum Iteration {
    DIRECT_SOLVER = 1, CG_SOLVER = 2, CGS_SOLVER = 3, BICG_SOLVER = 4, BICG_STAB_SOLVER = 5,
    GMRES_SOLVER = 6
@@ -599,11 +602,19 @@ class DC2DT3 {
       _x.setSize(_A.size());
    }
    void setDirichlet(const Vect<real_t>& bc) { _bc = &bc; }
+   // Equa::setTransient: FORWARD_EULER, BACKWARD_EULER (default) or CRANK_NICOLSON
+   void setTransient(TimeScheme s)
+   {
+      if (s != FORWARD_EULER && s != BACKWARD_EULER && s != CRANK_NICOLSON)
+         throw OFELIException("DC2DT3::setTransient: unsupported time scheme");
+      _scheme = s;
+   }
    void build()
    {
       _b.setSize(_A.size());
-      ofg_check(ofg_assemble_cd2d(_mesh->handle(), _A.handle(), _eps, _v->data(), _dt, _u->data(),
-                                  _bc ? _bc->data() : nullptr, _b.data()),
+      ofg_check(ofg_assemble_cd2d_scheme(_mesh->handle(), _A.handle(), _eps, _v->data(), _dt,
+                                         (int)_scheme, _u->data(), _bc ? _bc->data() : nullptr,
+                                         _b.data()),
                 "DC2DT3::build");
    }
    int step(Preconditioner p = ILU_PREC, size_t m = 30, int max_it = 1000, real_t toler = 1e-10)
@@ -623,6 +634,7 @@ class DC2DT3 {
    Vect<real_t>* _u;
    const Vect<real_t>* _v;
    real_t _eps, _dt;
+   TimeScheme _scheme = BACKWARD_EULER;
    SpMatrix<real_t> _A;
    const Vect<real_t>* _bc = nullptr;
    Vect<real_t> _b, _x;

@@ -177,6 +177,12 @@ int ofg_assemble_p1(ofg_mesh* m, ofg_matrix* A, const double* kel, const double*
  * (dti*eA1)*u_old plus the updateBC lift. */
 int ofg_assemble_cd2d(ofg_mesh* m, ofg_matrix* A, double eps, const double* v, double dt,
                       const double* u_old, const double* bc, double* b);
+/* The same under OFELI's time schemes (enum TimeScheme,
+ * include/equations/Equa.h:124-137): FORWARD_EULER 1 (eMat = eA1/dt, RHS
+ * (eA1/dt - eA0) u_old), BACKWARD_EULER 2 (as above), CRANK_NICOLSON 3
+ * (eMat = eA1/dt + eA0/2, RHS (eA1/dt - eA0/2) u_old). */
+int ofg_assemble_cd2d_scheme(ofg_mesh* m, ofg_matrix* A, double eps, const double* v, double dt,
+                             int scheme, const double* u_old, const double* bc, double* b);
 /* Vect::insertBC (include/linear_algebra/Vect_impl.h:1098-1130): nodal
  * vector from the equation-space solution x and bc (may be NULL). */
 int ofg_insert_bc(const ofg_mesh* m, const double* x, const double* bc, double* u);

@@ -61,6 +61,7 @@ SIGNATURES = {
     "ofg_matrix_create_from_mesh": (_i32, [_p, _pp]),
     "ofg_assemble_p1": (_i32, [_p, _p, _p, _p, _p, _p]),
     "ofg_assemble_cd2d": (_i32, [_p, _p, _d, _p, _d, _p, _p, _p]),
+    "ofg_assemble_cd2d_scheme": (_i32, [_p, _p, _d, _p, _d, _i32, _p, _p, _p]),
     "ofg_insert_bc": (_i32, [_p, _p, _p, _p]),
     "ofg_mesh_file_read": (_i32, [ctypes.c_char_p, _pp]),
     "ofg_mesh_file_write": (_i32, [_p, ctypes.c_char_p]),

@@ -121,19 +121,27 @@ int ofg_assemble_p1(ofg_mesh* m, ofg_matrix* A, const double* kel, const double*
    });
 }
 
-int ofg_assemble_cd2d(ofg_mesh* m, ofg_matrix* A, double eps, const double* v, double dt,
-                      const double* u_old, const double* bc, double* b)
+int ofg_assemble_cd2d_scheme(ofg_mesh* m, ofg_matrix* A, double eps, const double* v, double dt,
+                             int scheme, const double* u_old, const double* bc, double* b)
 {
-   return guarded("ofg_assemble_cd2d", [&] {
+   return guarded("ofg_assemble_cd2d_scheme", [&] {
       OFG_REQUIRE(m && A && b && v && u_old, OFG_ERR_ARG, "null argument");
       OFG_REQUIRE(m->dim == 2, OFG_ERR_ARG, "DC2DT3 needs a 2-D mesh");
       OFG_REQUIRE(dt > 0, OFG_ERR_ARG, "time step must be positive");
+      OFG_REQUIRE(scheme == 1 || scheme == 2 || scheme == 3, OFG_ERR_ARG,
+                  "scheme must be FORWARD_EULER (1), BACKWARD_EULER (2) or CRANK_NICOLSON (3)");
       In<double> dv(v, 2 * m->nn), du(u_old, m->nn), dbc(bc, m->nn);
       InOut<double> db(b, A->n, false);
-      assemble(m, A, ConvDiffT3{m->coords.p, m->code.p, eps, 1. / dt, dv.d, du.d, dbc.d}, db.d, 3,
-               0);
+      assemble(m, A, ConvDiffT3{m->coords.p, m->code.p, eps, 1. / dt, dv.d, du.d, dbc.d, scheme},
+               db.d, 3, 0);
       db.finish();
    });
+}
+
+int ofg_assemble_cd2d(ofg_mesh* m, ofg_matrix* A, double eps, const double* v, double dt,
+                      const double* u_old, const double* bc, double* b)
+{
+   return ofg_assemble_cd2d_scheme(m, A, eps, v, dt, 2, u_old, bc, b);
 }
 
 int ofg_insert_bc(const ofg_mesh* m, const double* x, const double* bc, double* u)

@@ -158,10 +158,14 @@ struct DiffusionT4 {
    }
 };
 
-// DC2DT3 under backward Euler (include/equations/therm/Equa_Therm.h:162-218):
-// eA1 = Capacity + LCapacity (src/equations/therm/DC2DT3.cpp:121-138),
-// eA0 = Diffusion(eps) + Convection (:141-147, 185-207),
-// eMat = eA1/dt + eA0, eRHS = updateBC + (eA1/dt) u_old.
+// DC2DT3 under OFELI's time schemes (Equa_Therm::build,
+// include/equations/therm/Equa_Therm.h:162-218): eA1 = Capacity + LCapacity
+// (src/equations/therm/DC2DT3.cpp:121-138), eA0 = Diffusion(eps) +
+// Convection (:141-147, 185-207); with dti = 1/dt,
+//   BACKWARD_EULER (2): eMat = dti eA1 + eA0,       eRHS += (dti eA1) u_old
+//   FORWARD_EULER  (1): eMat = dti eA1,             eRHS += (dti eA1 - eA0) u_old
+//   CRANK_NICOLSON (3): eMat = dti eA1 + 0.5 eA0,   eRHS += (dti eA1 - 0.5 eA0) u_old
+// after updateBC has lifted the imposed values with eMat.
 struct ConvDiffT3 {
    static constexpr int NEN = 3;
    const double* xy;
@@ -170,6 +174,7 @@ struct ConvDiffT3 {
    const double* v;
    const double* u_old;
    const double* bc;
+   int scheme;
    __device__ __forceinline__ bool geometry_ok(const int32_t (&en)[3]) const
    {
       double g[3][3], area;
@@ -186,16 +191,23 @@ struct ConvDiffT3 {
       const double v3[3] = {v[2 * en[0]] + v[2 * en[1]] + v[2 * en[2]],
                             v[2 * en[0] + 1] + v[2 * en[1] + 1] + v[2 * en[2] + 1], 0.0};
       const double cv = kThird * kThird * area;
-      double m1row[3];
+      double m1row[3], a0row[3];
 #pragma unroll
       for (int j = 0; j < 3; ++j) {
          const double m1 = (li == j) ? cc + cl : dd;
          m1row[j] = dti * m1;
-         krow[j] = m1row[j] + (eps * area * dot3(gl, g[j]) + cv * dot3(v3, g[j]));
+         a0row[j] = eps * area * dot3(gl, g[j]) + cv * dot3(v3, g[j]);
+         krow[j] = scheme == 1 ? m1row[j] : scheme == 3 ? m1row[j] + 0.5 * a0row[j]
+                                                        : m1row[j] + a0row[j];
       }
       frow = 0.0;
       if (bc) lift_row<3>(en, pos, code, bc, krow, frow);
-      frow += m1row[0] * u_old[en[0]] + m1row[1] * u_old[en[1]] + m1row[2] * u_old[en[2]];
+      double r[3];
+#pragma unroll
+      for (int j = 0; j < 3; ++j)
+         r[j] = scheme == 1 ? m1row[j] - a0row[j] : scheme == 3 ? m1row[j] - 0.5 * a0row[j]
+                                                                : m1row[j];
+      frow += r[0] * u_old[en[0]] + r[1] * u_old[en[1]] + r[2] * u_old[en[2]];
       return true;
    }
 };

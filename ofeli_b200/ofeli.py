@@ -30,6 +30,8 @@ IDENT_PREC, DIAG_PREC, DILU_PREC, ILU_PREC, SSOR_PREC = 0, 1, 2, 3, 4
 # no OFELI counterpart: M = G^T G predicted by a trained network (LearnedNet)
 LEARNED_PREC = 5
 DIRECT_SOLVER, CG_SOLVER, CGS_SOLVER, BICG_SOLVER, BICG_STAB_SOLVER, GMRES_SOLVER = 1, 2, 3, 4, 5, 6
+# OFELI's TimeScheme values (include/equations/Equa.h:124-137) on the path
+FORWARD_EULER, BACKWARD_EULER, CRANK_NICOLSON = 1, 2, 3
 OFELI_EPSMCH = 2.220446049250313e-16
 
 
@@ -758,15 +760,18 @@ Laplace3DT4 = DC3DT4
 
 
 class DC2DT3:
-    """DC2DT3 under backward Euler: capacity (consistent + lumped, as OFELI's
+    """DC2DT3 transient steps: capacity (consistent + lumped, as OFELI's
     shared CAPACITY bit gives), diffusion eps, convection by the nodal
-    velocity; one build() per time step (include/equations/therm/Equa_Therm.h)."""
+    velocity, under backward Euler (default), forward Euler or
+    Crank-Nicolson (setTransient); one build() per time step
+    (include/equations/therm/Equa_Therm.h:162-218)."""
 
-    def __init__(self, mesh, u0, v, eps, dt):
+    def __init__(self, mesh, u0, v, eps, dt, scheme=BACKWARD_EULER):
         self.mesh = mesh
         self.u = _f64(u0, mesh.nn).copy()
         self.v = _f64(v, 2 * mesh.nn)
         self.eps, self.dt = eps, dt
+        self.setTransient(scheme)
         self._A = SpMatrix(mesh)
         self._bc = None
         self.x = np.zeros(self._A.n)
@@ -774,10 +779,16 @@ class DC2DT3:
     def setDirichlet(self, bc):
         self._bc = _f64(bc, self.mesh.nn)
 
+    def setTransient(self, scheme):
+        """Equa::setTransient: FORWARD_EULER, BACKWARD_EULER or CRANK_NICOLSON."""
+        if scheme not in (FORWARD_EULER, BACKWARD_EULER, CRANK_NICOLSON):
+            raise OFELIException("unsupported time scheme %r" % (scheme,))
+        self.scheme = scheme
+
     def build(self):
         self._b = np.zeros(self._A.n)
-        _call("ofg_assemble_cd2d", self.mesh._h, self._A._h, self.eps, _ptr(self.v), self.dt,
-              _ptr(self.u), _ptr(self._bc), _ptr(self._b))
+        _call("ofg_assemble_cd2d_scheme", self.mesh._h, self._A._h, self.eps, _ptr(self.v),
+              self.dt, self.scheme, _ptr(self.u), _ptr(self._bc), _ptr(self._b))
         return self._A, self._b
 
     def step(self, prec=ILU_PREC, m=30, max_it=1000, toler=1e-10, solver=GMRES_SOLVER):

@@ -295,10 +295,11 @@ int64_t or_assemble_p1(int dim, int64_t nn, int64_t ne, const double* coords, co
  * (src/equations/therm/DC2DT3.cpp:121-138); Diffusion (eps, :141-147);
  * Convection by the element-summed nodal velocity (:185-207); eMat = dti*eA1
  * + eA0; eRHS = updateBC + (dti*eA1)*u_old. */
-int64_t or_assemble_cd2d(int64_t nn, int64_t ne, const double* xy, const int32_t* elem,
-                         const int64_t* dof, const int32_t* code, double eps, const double* v,
-                         double dt, const double* u_old, const double* bc, int64_t n,
-                         const int64_t* row_ptr, const int64_t* col_ind, double* a, double* b)
+int64_t or_assemble_cd2d_scheme(int64_t nn, int64_t ne, const double* xy, const int32_t* elem,
+                                const int64_t* dof, const int32_t* code, double eps,
+                                const double* v, double dt, int scheme, const double* u_old,
+                                const double* bc, int64_t n, const int64_t* row_ptr,
+                                const int64_t* col_ind, double* a, double* b)
 {
    (void)nn;
    memset(a, 0, sizeof(double) * (size_t)row_ptr[n]);
@@ -327,17 +328,43 @@ int64_t or_assemble_cd2d(int64_t nn, int64_t ne, const double* xy, const int32_t
       c = THIRD * THIRD * area * 1.0;
       for (int i = 0; i < 3; ++i)
          for (int j = 0; j < 3; ++j) A0[3 * i + j] += c * pdot(v3, g[j]);
-      for (int q = 0; q < 9; ++q) Ke[q] = dti * A1[q] + A0[q];
+      /* Equa_Therm::build (include/equations/therm/Equa_Therm.h:191-208):
+         eMat and the matrix applied to u_old by scheme (1 forward Euler,
+         2 backward Euler, 3 Crank-Nicolson) */
+      double R[9];
+      for (int q = 0; q < 9; ++q) {
+         if (scheme == 1) {
+            Ke[q] = dti * A1[q];
+            R[q] = dti * A1[q] - A0[q];
+         }
+         else if (scheme == 3) {
+            Ke[q] = dti * A1[q] + 0.5 * A0[q];
+            R[q] = dti * A1[q] - 0.5 * A0[q];
+         }
+         else {
+            Ke[q] = dti * A1[q] + A0[q];
+            R[q] = dti * A1[q];
+         }
+      }
       for (int i = 0; i < 3; ++i) Fe[i] = 0.0;
       if (bc) update_bc(3, en, code, Ke, bc, Fe);
       for (int i = 0; i < 3; ++i) {
          double s = 0.0;
-         for (int j = 0; j < 3; ++j) s += (dti * A1[3 * i + j]) * u_old[en[j]];
+         for (int j = 0; j < 3; ++j) s += R[3 * i + j] * u_old[en[j]];
          Fe[i] += s;
       }
       scatter(3, en, dof, Ke, Fe, row_ptr, col_ind, a, b);
    }
    return 0;
+}
+
+int64_t or_assemble_cd2d(int64_t nn, int64_t ne, const double* xy, const int32_t* elem,
+                         const int64_t* dof, const int32_t* code, double eps, const double* v,
+                         double dt, const double* u_old, const double* bc, int64_t n,
+                         const int64_t* row_ptr, const int64_t* col_ind, double* a, double* b)
+{
+   return or_assemble_cd2d_scheme(nn, ne, xy, elem, dof, code, eps, v, dt, 2, u_old, bc, n,
+                                  row_ptr, col_ind, a, b);
 }
 
 /* ------------------------------------------------------------ algebra ---- */

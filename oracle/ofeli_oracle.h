@@ -40,6 +40,11 @@ int64_t or_assemble_p1(int dim, int64_t nn, int64_t ne, const double* coords, co
 /* a9: one backward-Euler build of DC2DT3 (capacity bit 0x20 = consistent +
  * lumped, diffusion eps, convection by the nodal velocity v[2*nn]); u_old is
  * the nodal field of the previous step. */
+int64_t or_assemble_cd2d_scheme(int64_t nn, int64_t ne, const double* xy, const int32_t* elem,
+                                const int64_t* dof, const int32_t* code, double eps,
+                                const double* v, double dt, int scheme, const double* u_old,
+                                const double* bc, int64_t n, const int64_t* row_ptr,
+                                const int64_t* col_ind, double* a, double* b);
 int64_t or_assemble_cd2d(int64_t nn, int64_t ne, const double* xy, const int32_t* elem,
                          const int64_t* dof, const int32_t* code, double eps, const double* v,
                          double dt, const double* u_old, const double* bc, int64_t n,

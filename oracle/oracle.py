@@ -53,6 +53,10 @@ def lib():
         L.or_assemble_cd2d.argtypes = [_i64, _i64, _p, _p, _p, _p, ctypes.c_double, _p,
                                        ctypes.c_double, _p, _p, _i64, _p, _p, _p, _p]
         L.or_assemble_cd2d.restype = _i64
+        L.or_assemble_cd2d_scheme.argtypes = [_i64, _i64, _p, _p, _p, _p, ctypes.c_double, _p,
+                                              ctypes.c_double, ctypes.c_int, _p, _p, _i64, _p,
+                                              _p, _p, _p]
+        L.or_assemble_cd2d_scheme.restype = _i64
         L.or_spmv.argtypes = [_i64, _p, _p, _p, _p, _p]
         L.or_prec_setup.argtypes = [ctypes.c_int, _i64, _p, _p, _p, _p, _p]
         L.or_prec_setup.restype = _i64
@@ -122,13 +126,15 @@ def assemble(dim, coords, elem, dof, code, n, rp, ci, k=None, f=None, bc=None):
     return a, b
 
 
-def assemble_cd2d(xy, elem, dof, code, n, rp, ci, eps, v, dt, u_old, bc=None):
+def assemble_cd2d(xy, elem, dof, code, n, rp, ci, eps, v, dt, u_old, bc=None, scheme=2):
+    """scheme: OFELI's TimeScheme (1 forward Euler, 2 backward Euler, 3
+    Crank-Nicolson)."""
     ne = elem.size // 3
     a = np.zeros(int(rp[-1]))
     b = np.zeros(n)
-    ret = lib().or_assemble_cd2d(code.size, ne, _ptr(xy), _ptr(elem), _ptr(dof), _ptr(code),
-                                 eps, _ptr(v), dt, _ptr(u_old), _ptr(bc), n, _ptr(rp), _ptr(ci),
-                                 _ptr(a), _ptr(b))
+    ret = lib().or_assemble_cd2d_scheme(code.size, ne, _ptr(xy), _ptr(elem), _ptr(dof),
+                                        _ptr(code), eps, _ptr(v), dt, scheme, _ptr(u_old),
+                                        _ptr(bc), n, _ptr(rp), _ptr(ci), _ptr(a), _ptr(b))
     if ret < 0:
         raise ValueError("non-positive Jacobian in element %d" % (-ret))
     return a, b

@@ -7,7 +7,7 @@
 // Usage (all inputs are little-endian binaries written by the caller):
 //   ofeli_ref p2d  NX NY   SOLVER PREC TOL MAXIT INDIR OUTDIR
 //   ofeli_ref p3d  M       SOLVER PREC TOL MAXIT INDIR OUTDIR
-//   ofeli_ref cd2d NX NY   NSTEPS DT EPS PREC TOL MAXIT INDIR OUTDIR
+//   ofeli_ref cd2d NX NY   NSTEPS DT EPS SOLVER PREC TOL MAXIT INDIR OUTDIR [BE|FE|CN]
 //   ofeli_ref mget FILE INDIR OUTDIR            (Mesh::get, dump, Mesh::put)
 //   ofeli_ref mrect NX NY CX0 CXN CY0 CYN INDIR OUTDIR  (Mesh(rect), dump, put)
 //   ofeli_ref mlap FILE SOLVER PREC TOL MAXIT INDIR OUTDIR
@@ -506,7 +506,13 @@ int run_cd2d(int argc, char** argv)
    eq.setTerms(PDE_Terms::CONVECTION);
    eq.setInput(EType::VELOCITY, v);
    eq.setDirichlet(bc);
-   eq.setTransient(BACKWARD_EULER);
+   // optional time scheme after OUTDIR: BE (default), FE, CN
+   TimeScheme scheme = BACKWARD_EULER;
+   if (argc >= 14) {
+      std::string sc = argv[13];
+      scheme = sc == "FE" ? FORWARD_EULER : sc == "CN" ? CRANK_NICOLSON : BACKWARD_EULER;
+   }
+   eq.setTransient(scheme);
    eq.set_dt(dt);
 
    Vect<real_t>& b = *eq.rhs();

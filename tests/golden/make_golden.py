@@ -152,6 +152,25 @@ def case_bicgstab():
     save("bicgstab", arrays, meta)
 
 
+def case_cd2d_schemes():
+    """The 17x17 convection-diffusion steps of case_cd2d under OFELI's other
+    time schemes: forward Euler and Crank-Nicolson, GMRES(30) + ILU, 5 steps."""
+    nx, steps, dt, eps = 16, 5, 1e-3, 1e-3
+    xy, elem, code = O.mesh2d(nx, nx)
+    P = xy.reshape(-1, 2)
+    u0 = np.exp(-((P[:, 0] - 0.3) ** 2 + (P[:, 1] - 0.5) ** 2) / (2 * 0.05 ** 2))
+    u0[code > 0] = 0.0
+    v = np.stack([-(P[:, 1] - 0.5), P[:, 0] - 0.5], axis=1).reshape(-1)
+    arrays, meta = {}, {"nx": nx, "steps": steps, "dt": dt, "eps": eps, "tol": 1e-10, "m": 30,
+                        "schemes": {"FE": 1, "CN": 3}}
+    for name in ("FE", "CN"):
+        info, out = O.run_reference(["cd2d", nx, nx, steps, dt, eps, "GMRES30", "ILU", 1e-10, 2000],
+                                    {"u0": u0, "v": v}, extra=[name])
+        arrays.update({name + "_a0": out["a"], name + "_b0": out["b0"], name + "_u": out["u"],
+                       name + "_iters": out["iters"]})
+    save("cd2d_schemes", arrays, meta)
+
+
 # nb_dof 2 with negative and multi-digit marks, the "tria" alias, attributes
 # in either order (one pair written without a blank between them), tabs and a
 # CR, comments outside the blocks, a node no element uses, element code 3
@@ -260,3 +279,4 @@ if __name__ == "__main__":
     case_cd2d()
     case_bicgstab()
     case_meshio()
+    case_cd2d_schemes()

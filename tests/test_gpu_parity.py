@@ -398,3 +398,26 @@ def test_matrix_set_add_in_order(p2d65):
     want, bad = O.matrix_edit(rp, ci, a0, bad_rows, bad_cols, np.ones(3), False)
     assert bad == 1 and np.array_equal(A.values(), want)
     A.set_values(a0)
+
+
+@pytest.mark.parametrize("name", ["FE", "CN"])
+def test_transient_time_schemes(name):
+    """Forward Euler and Crank-Nicolson DC2DT3 steps (Equa_Therm::build):
+    first-step matrix and RHS bit-exact, iterations +-2, field 1e-12."""
+    g, info = load_golden("cd2d_schemes")
+    nx = info["nx"]
+    mesh = F.Mesh(0.0, 1.0, 0.0, 1.0, nx, nx)
+    xy, _, code, _ = mesh.arrays()
+    P = xy.reshape(-1, 2)
+    u0 = np.exp(-((P[:, 0] - 0.3) ** 2 + (P[:, 1] - 0.5) ** 2) / (2 * 0.05 ** 2))
+    u0[code > 0] = 0.0
+    v = np.stack([-(P[:, 1] - 0.5), P[:, 0] - 0.5], axis=1).reshape(-1)
+    scheme = {"FE": F.FORWARD_EULER, "CN": F.CRANK_NICOLSON}[name]
+    eq = F.DC2DT3(mesh, u0, v, info["eps"], info["dt"], scheme)
+    eq.setDirichlet(np.zeros(mesh.nn))
+    A, b = eq.build()
+    assert np.array_equal(A.values(), g[name + "_a0"]) and np.array_equal(b, g[name + "_b0"])
+    its = [eq.step(prec=F.ILU_PREC, m=info["m"], max_it=2000, toler=info["tol"])
+           for _ in range(info["steps"])]
+    assert all(abs(a - b) <= IT_TOL for a, b in zip(its, g[name + "_iters"]))
+    assert rel_err(eq.u, g[name + "_u"]) <= SOL_TOL

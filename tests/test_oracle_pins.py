@@ -174,3 +174,32 @@ def test_bicgstab_cd2d_bit_exact():
         u = O.insert_bc(code, x)
     assert its == list(z["cd2d_iters"])
     assert np.array_equal(u, z["cd2d_u"])
+
+
+@pytest.mark.parametrize("name", ["FE", "CN"])
+def test_cd2d_schemes_bit_exact(name):
+    """OFELI's forward Euler and Crank-Nicolson steps of DC2DT3
+    (Equa_Therm::build) restated: first-step matrix and RHS, iteration
+    counts and the final field equal the reference's."""
+    g, info = load_golden("cd2d_schemes")
+    nx, dt, eps = info["nx"], info["dt"], info["eps"]
+    scheme = info["schemes"][name]
+    xy, elem, code = O.mesh2d(nx, nx)
+    P = xy.reshape(-1, 2)
+    u = np.exp(-((P[:, 0] - 0.3) ** 2 + (P[:, 1] - 0.5) ** 2) / (2 * 0.05 ** 2))
+    u[code > 0] = 0.0
+    v = np.stack([-(P[:, 1] - 0.5), P[:, 0] - 0.5], axis=1).reshape(-1)
+    dof, n = O.number_equations(code)
+    rp, ci = O.node_graph(elem, 3, dof, n)
+    x = np.zeros(n)
+    its = []
+    for s in range(info["steps"]):
+        a, b = O.assemble_cd2d(xy, elem, dof, code, n, rp, ci, eps, v, dt, u,
+                               bc=np.zeros(code.size), scheme=scheme)
+        if s == 0:
+            assert np.array_equal(a, g[name + "_a0"]) and np.array_equal(b, g[name + "_b0"])
+        x, it = O.gmres(rp, ci, a, b, O.ILU, info["m"], 2000, info["tol"], x0=x)
+        its.append(it)
+        u = O.insert_bc(code, x)
+    assert its == list(g[name + "_iters"])
+    assert np.array_equal(u, g[name + "_u"])
