@@ -269,7 +269,10 @@ int ofg_bicgstab(ofg_prec* P, const double* b, double* x, int max_it, double tol
                  double* res);
 /* Mixed-precision solve: FP64 iterative refinement whose correction is
  * computed by Jacobi-preconditioned CG in FP32 (inner_bits 32) or with BF16
- * matrix values and FP32 vectors (inner_bits 16); FP64 only for b - A x,
+ * matrix values and FP32 vectors (inner_bits 16); inner_bits 0 picks BF16
+ * values when every value of A is exactly representable in BF16 (the
+ * iteration is then the FP32 one, bit for bit, with 2 bytes less per entry)
+ * and FP32 values otherwise; FP64 only for b - A x,
  * x += correction and the accumulation of dot products.  No counterpart in
  * OFELI (its solvers are FP64 only).
  *   mode 0: one FP32 CG sequence; a refinement (FP64 true residual
@@ -349,7 +352,8 @@ int ofg_learned_gemm_check(ofg_learned* L, int layer, int64_t rows, const uint16
  * the network must outlive it. */
 int ofg_prec_create_learned(ofg_learned* L, ofg_matrix* A, ofg_prec** out);
 /* Flexible CG with the learned preconditioner, in FP32 (inner_bits 32) or
- * with BF16 matrix values (16), inside FP64 iterative refinement; the
+ * with BF16 matrix values (16, or 0 for BF16 only when lossless, as in
+ * ofg_solve_mixed), inside FP64 iterative refinement; the
  * arguments and results are those of ofg_solve_mixed.  When the learned
  * iteration stagnates (residual not halved in 500 iterations, not finite, or
  * three refinements without a 10% gain) the solve continues with the plain

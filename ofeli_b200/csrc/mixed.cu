@@ -50,6 +50,22 @@ __global__ void cast_values(int64_t total, const double* __restrict__ src, T* ds
       dst[i] = (T)src[i];
 }
 
+// BF16 copy of the values; *inexact = 1 when some value does not come back
+// unchanged from BF16 (a NaN never does)
+__global__ void cast_bf16_exact(int64_t total, const double* __restrict__ src, __nv_bfloat16* dst,
+                                int* inexact)
+{
+   int64_t stride = (int64_t)gridDim.x * blockDim.x;
+   int lost = 0;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+      const double v = src[i];
+      const __nv_bfloat16 h = (__nv_bfloat16)v;
+      dst[i] = h;
+      lost |= (double)__bfloat162float(h) != v;
+   }
+   if (__syncthreads_or(lost) && threadIdx.x == 0) atomicOr(inexact, 1);
+}
+
 // r = b - q (FP64); ||r||, ||b|| (first call); convergence test
 __global__ void __launch_bounds__(kRedBlock, 8) mx_residual(int64_t n, const double* __restrict__ b,
                                                          const double* __restrict__ q, double* r,
@@ -403,7 +419,8 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
    const bool learned = LP != nullptr;
    OFG_REQUIRE(learned || prec_type == OFG_DIAG || prec_type == OFG_IDENT, OFG_ERR_ARG,
                "mixed-precision inner solver supports DIAG and IDENT");
-   OFG_REQUIRE(inner_bits == 32 || inner_bits == 16, OFG_ERR_ARG, "inner_bits must be 32 or 16");
+   OFG_REQUIRE(inner_bits == 32 || inner_bits == 16 || inner_bits == 0, OFG_ERR_ARG,
+               "inner_bits must be 32, 16 or 0 (automatic)");
    OFG_REQUIRE(mode == 0 || mode == 1, OFG_ERR_ARG, "mode must be 0 or 1");
    OFG_REQUIRE(inner_tol > 0 && inner_tol < 1, OFG_ERR_ARG, "inner_tol must be in (0, 1)");
    const int64_t n = A->n;
@@ -424,12 +441,23 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
    // structured meshes): 2 bytes less per entry streamed by every SpMV
    const bool a16 = ensure_sell_d16(A);
    const double aidx = a16 ? 2.0 : 4.0;
+   // bad[0]: zero diagonal entry; bad[1]: a value of A is not exact in BF16
+   DBuf<int> bad(2);
+   bad.zero();
    DBuf<__nv_bfloat16> v16;
    if (inner_bits == 32) ensure_sell32(A);
-   else {
+   else if (inner_bits == 16) {
       v16.alloc(A->sell_val.n);
       cast_values<__nv_bfloat16><<<grid_for(A->sell_val.n, 256), 256, 0, stream()>>>(
          A->sell_val.n, A->sell_val.p, v16.p);
+      count_launch();
+   }
+   else {
+      // automatic: BF16 values only when the copy is lossless, so that the
+      // inner iteration is the FP32 one with 2 bytes less per entry
+      v16.alloc(A->sell_val.n);
+      cast_bf16_exact<<<grid_for(A->sell_val.n, 256), 256, 0, stream()>>>(
+         A->sell_val.n, A->sell_val.p, v16.p, bad.p + 1);
       count_launch();
    }
    const int64_t nv = npad > 0 ? npad : 4;
@@ -437,8 +465,6 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
    DBuf<float> tz(learned ? nv : 1), zz(learned ? nv : 1);
    DBuf<double> r(n > 0 ? n : 1), q64(n > 0 ? n : 1);
    DBuf<MixState> S(1);
-   DBuf<int> bad(1);
-   bad.zero();
    p.zero();
    q.zero();
    const unsigned g = grid_for(std::max<int64_t>(n, nquads), kRedBlock, 8);
@@ -448,9 +474,17 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
    inv_diag32<<<grid_for(nv, 256), 256, 0, stream()>>>(n, npad, A->dpos.p, A->val.p, dinv.p,
                                                         prec_type == OFG_IDENT ? 1 : 0, bad.p);
    count_launch();
-   int hb = 0;
-   bad.download(&hb, 1);
-   OFG_REQUIRE(!hb, OFG_ERR_PIVOT, "zero diagonal entry");
+   int hb[2] = {0, 0};
+   bad.download(hb, 2);
+   OFG_REQUIRE(!hb[0], OFG_ERR_PIVOT, "zero diagonal entry");
+   int bits = inner_bits;
+   if (inner_bits == 0) {
+      bits = hb[1] ? 32 : 16;
+      if (bits == 32) {
+         v16.release();
+         ensure_sell32(A);
+      }
+   }
    const float* jac = learned ? nullptr : dinv.p;
    const unsigned gq = grid_for(nquads, kRedBlock, 8);
    const unsigned gn = grid_for(n, kRedBlock, 8);
@@ -528,11 +562,11 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
             // launch: each one's blocks start while the previous one drains
             // its reduction tail
             int* worked = prof_begin();
-            if (inner_bits == 32 && a16)
+            if (bits == 32 && a16)
                launch_pdl(mx_spmv<float, int16_t>, gq, kRedBlock, nquads, A->sell_ptr.p,
                           A->sell_d16.p, A->sell_val32.p, p.p, q.p, S.p, partials.p, counter.p,
                           worked);
-            else if (inner_bits == 32)
+            else if (bits == 32)
                launch_pdl(mx_spmv<float, int32_t>, gq, kRedBlock, nquads, A->sell_ptr.p,
                           A->sell_col.p, A->sell_val32.p, p.p, q.p, S.p, partials.p, counter.p,
                           worked);
@@ -544,8 +578,8 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
                           A->sell_col.p, v16.p, p.p, q.p, S.p, partials.p, counter.p, worked);
             // algorithmic bytes: value (4 or 2) + column index (4, or 2 as a
             // 16-bit offset) per entry, p gathered, q written, p read for the dot
-            prof_end(inner_bits == 32 ? PROF_SPMV32 : PROF_SPMV16,
-                     ((inner_bits == 32 ? 4.0 : 2.0) + aidx) * A->nnz + 12.0 * n + 4.0);
+            prof_end(bits == 32 ? PROF_SPMV32 : PROF_SPMV16,
+                     ((bits == 32 ? 4.0 : 2.0) + aidx) * A->nnz + 12.0 * n + 4.0);
             if (learned) {
                launch_pdl(mx_update<false>, gq, kRedBlock, nquads, d.p, p.p, rr.p, q.p, jac, S.p,
                           partials.p, counter.p, inner_tol, tol, scale, max_inner, mode);
@@ -593,7 +627,7 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
       if (!std::isfinite(h.rel)) OFG_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), stream()));
       if (fell_back) *fell_back = 1;
       int o2 = 0, i2 = 0;
-      solve_mixed(A, OFG_DIAG, inner_bits, mode, b, x, std::max(1, max_outer - n_outer),
+      solve_mixed(A, OFG_DIAG, bits, mode, b, x, std::max(1, max_outer - n_outer),
                   std::max(1, max_inner - h.it), inner_tol, tol, &o2, &i2, true_res, nullptr,
                   nullptr);
       *outer = n_outer + o2;

@@ -436,7 +436,8 @@ def solve_mixed(A, b, x, prec=DIAG_PREC, inner_bits=32, toler=1e-10, max_outer=2
                 max_inner=1000000, inner_tol=0.05, mode=0):
     """FP64 iterative refinement around an FP32 (or BF16-matrix) PCG; mode 0
     keeps the CG direction across refinements, mode 1 restarts the inner CG.
-    Returns (refinement steps, inner iterations, FP64 true relative residual)."""
+    inner_bits 0 takes BF16 matrix values when every value of A is exact in
+    BF16 and FP32 values otherwise.  Returns (refinement steps, inner iterations, FP64 true relative residual)."""
     b = _f64(b, A.n)
     o, i, r = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
     _call("ofg_solve_mixed", A._h, prec, inner_bits, mode, _ptr(b), _ptr(x), max_outer,
@@ -541,8 +542,8 @@ class LearnedNet:
 def fcg_learned(P, b, x, inner_bits=32, toler=1e-10, max_outer=200, max_inner=1000000,
                 inner_tol=0.05):
     """Flexible CG with the learned preconditioner in FP32 inside FP64
-    refinement, falling back to the plain Jacobi iteration on stagnation.
-    Returns (refinement steps, inner iterations, FP64 true relative residual,
+    refinement, falling back to the plain Jacobi iteration on stagnation
+    (inner_bits as in solve_mixed).  Returns (refinement steps, inner iterations, FP64 true relative residual,
     fell_back)."""
     b = _f64(b, P.A.n)
     o, i, r, fb = ctypes.c_int(), ctypes.c_int(), ctypes.c_double(), ctypes.c_int()

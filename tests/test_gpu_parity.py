@@ -292,6 +292,50 @@ def test_mixed_precision_column_offset_formats(cuda, permute):
     assert rel_err(x, xref) <= 1e-6
 
 
+def solve_counting_formats(A, b, bits):
+    """solve_mixed with the given inner_bits; returns (x, outer, inner,
+    residual, SpMV launches with FP32 values, with BF16 values)."""
+    from ofeli_b200 import capi
+    x = np.zeros(A.n)
+    capi.profile_enable(1)
+    try:
+        outer, inner, res = F.solve_mixed(A, b, x, prec=F.DIAG_PREC, inner_bits=bits,
+                                          toler=1e-10)
+        n32, n16 = capi.profile_read("spmv32")[0], capi.profile_read("spmv16")[0]
+    finally:
+        capi.profile_enable(0)
+    return x, outer, inner, res, n32, n16
+
+
+@pytest.mark.parametrize("exact", [True, False])
+def test_mixed_precision_automatic_value_format(cuda, exact, p2d65):
+    """inner_bits 0 streams BF16 matrix values only when every value of A
+    comes back unchanged from BF16.  The 65x65 Laplacian (values -1, 0, 4)
+    takes that path, and the solve is bit for bit the one with FP32 values;
+    the same matrix scaled symmetrically, D A D with D = diag(1 .. 1.3), has
+    values that BF16 does not hold and takes the FP32 path, bit for bit the
+    inner_bits 32 solve."""
+    import torch
+    g, _, _, _ = p2d65
+    a = g["a"]
+    if not exact:
+        rp = g["row_ptr"].astype(np.int64)
+        rows = np.repeat(np.arange(rp.size - 1), np.diff(rp))
+        d = 1.0 + 0.3 * np.random.default_rng(5).random(rp.size - 1)
+        a = a * d[rows] * d[g["col_ind"].astype(np.int64) - 1]
+    lossless = np.array_equal(torch.from_numpy(a).to(torch.bfloat16).to(torch.float64).numpy(), a)
+    assert lossless == exact
+    A = F.SpMatrix(g["row_ptr"].astype(np.int64), g["col_ind"].astype(np.int64), a)
+    auto = solve_counting_formats(A, g["b"], 0)
+    fp32 = solve_counting_formats(A, g["b"], 32)
+    assert auto[3] <= 1e-10 and F.residual(A, g["b"], auto[0]) <= 1e-10
+    assert (auto[4] == 0 and auto[5] > 0) if exact else (auto[4] > 0 and auto[5] == 0)
+    assert np.array_equal(auto[0], fp32[0]) and auto[1:4] == fp32[1:4]
+    if exact:
+        bf16 = solve_counting_formats(A, g["b"], 16)
+        assert np.array_equal(auto[0], bf16[0]) and auto[1:4] == bf16[1:4]
+
+
 @pytest.mark.parametrize("prec", ["DIAG", "ILU"])
 def test_bicgstab_matches_reference(cuda, prec):
     """BiCGStab on the 65x65 system against OFELI's own run (golden
