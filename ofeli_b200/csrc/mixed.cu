@@ -192,11 +192,12 @@ __global__ void __launch_bounds__(kRedBlock, 8) mx_spmv(int64_t nquads, const in
    if (grid_reduce<1>(v, partials, counter, t)) S->alpha = S->rho[S->it & 1] / t[0];
 }
 
-// d += alpha p, r -= alpha q; ||r||, (r, D r) when JAC; decides when the
-// host must refine (mode 0) or stop the inner solve (mode 1)
+// r -= alpha q; ||r||, (r, D r) when JAC; decides when the host must refine
+// (mode 0) or stop the inner solve (mode 1).  The matching d += alpha p is
+// made by the direction kernel, which reads p anyway (or by mx_flush_d when
+// this iteration pauses the loop).
 template <bool JAC>
-__global__ void __launch_bounds__(kRedBlock, 8) mx_update(int64_t nquads, float* d,
-                                                       const float* __restrict__ p, float* rr,
+__global__ void __launch_bounds__(kRedBlock, 8) mx_update(int64_t nquads, float* rr,
                                                        const float* __restrict__ q,
                                                        const float* __restrict__ dinv, MixState* S,
                                                        double* partials, unsigned* counter,
@@ -209,17 +210,13 @@ __global__ void __launch_bounds__(kRedBlock, 8) mx_update(int64_t nquads, float*
    const float a = (float)S->alpha;
    double v[2] = {0.0, 0.0};
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
-   float4* d4 = reinterpret_cast<float4*>(d);
    float4* r4 = reinterpret_cast<float4*>(rr);
-   const float4* p4 = reinterpret_cast<const float4*>(p);
    const float4* q4 = reinterpret_cast<const float4*>(q);
    const float4* m4 = reinterpret_cast<const float4*>(dinv);
    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nquads; i += stride) {
-      const float4 pi = p4[i], qi = q4[i];
-      float4 di = d4[i], ri = r4[i];
-      di.x += a * pi.x; di.y += a * pi.y; di.z += a * pi.z; di.w += a * pi.w;
+      const float4 qi = q4[i];
+      float4 ri = r4[i];
       ri.x -= a * qi.x; ri.y -= a * qi.y; ri.z -= a * qi.z; ri.w -= a * qi.w;
-      d4[i] = di;
       r4[i] = ri;
       v[0] += (double)ri.x * ri.x + (double)ri.y * ri.y + (double)ri.z * ri.z + (double)ri.w * ri.w;
       if (JAC) {
@@ -246,24 +243,36 @@ __global__ void __launch_bounds__(kRedBlock, 8) mx_update(int64_t nquads, float*
    }
 }
 
-// p = D r + beta p, beta = rho_it / rho_{it-1}
+// d += alpha p with this iteration's alpha and p (upd_d), then the new
+// direction
+__device__ __forceinline__ void add_alpha_p(float4* d4, int64_t i, float a, const float4& pi)
+{
+   float4 di = d4[i];
+   di.x += a * pi.x; di.y += a * pi.y; di.z += a * pi.z; di.w += a * pi.w;
+   d4[i] = di;
+}
+
+// (d += alpha p;) p = D r + beta p, beta = rho_it / rho_{it-1}
 __global__ void __launch_bounds__(kRedBlock, 8) mx_direction(int64_t nquads,
                                                           const float* __restrict__ rr,
                                                           const float* __restrict__ dinv, float* p,
-                                                          const MixState* S)
+                                                          float* d, int upd_d, const MixState* S)
 {
    pdl_wait();
    pdl_release();
    if (S->pause) return;
    const int it = S->it;
    const float beta = (float)(S->rho[it & 1] / S->rho[(it + 1) & 1]);
+   const float a = (float)S->alpha;
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
    float4* p4 = reinterpret_cast<float4*>(p);
+   float4* d4 = reinterpret_cast<float4*>(d);
    const float4* r4 = reinterpret_cast<const float4*>(rr);
    const float4* m4 = reinterpret_cast<const float4*>(dinv);
    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nquads; i += stride) {
       const float4 ri = r4[i], mi = m4[i];
       float4 pi = p4[i];
+      if (upd_d) add_alpha_p(d4, i, a, pi);
       pi.x = ri.x * mi.x + beta * pi.x;
       pi.y = ri.y * mi.y + beta * pi.y;
       pi.z = ri.z * mi.z + beta * pi.z;
@@ -354,17 +363,20 @@ __global__ void __launch_bounds__(kRedBlock, 8) lg_upper(int64_t nquads, const i
    }
 }
 
-// p = z + beta p (p = z on a fresh start)
+// (d += alpha p;) p = z + beta p (p = z on a fresh start)
 __global__ void __launch_bounds__(kRedBlock, 8) lg_direction(int64_t nquads,
                                                           const float* __restrict__ z, float* p,
-                                                          const MixState* S, int fresh)
+                                                          float* d, int upd_d, const MixState* S,
+                                                          int fresh)
 {
    pdl_wait();
    pdl_release();
    if (S->pause) return;
    const float beta = fresh ? 0.f : (float)S->beta;
+   const float a = (float)S->alpha;
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
    float4* p4 = reinterpret_cast<float4*>(p);
+   float4* d4 = reinterpret_cast<float4*>(d);
    const float4* z4 = reinterpret_cast<const float4*>(z);
    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nquads; i += stride) {
       const float4 zi = z4[i];
@@ -373,12 +385,26 @@ __global__ void __launch_bounds__(kRedBlock, 8) lg_direction(int64_t nquads,
          continue;
       }
       float4 pi = p4[i];
+      if (upd_d) add_alpha_p(d4, i, a, pi);
       pi.x = zi.x + beta * pi.x;
       pi.y = zi.y + beta * pi.y;
       pi.z = zi.z + beta * pi.z;
       pi.w = zi.w + beta * pi.w;
       p4[i] = pi;
    }
+}
+
+// d += alpha p for the iteration that paused the loop (its direction kernel
+// returned early)
+__global__ void mx_flush_d(int64_t nquads, float* d, const float* __restrict__ p,
+                           const MixState* S)
+{
+   const float a = (float)S->alpha;
+   int64_t stride = (int64_t)gridDim.x * blockDim.x;
+   float4* d4 = reinterpret_cast<float4*>(d);
+   const float4* p4 = reinterpret_cast<const float4*>(p);
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nquads; i += stride)
+      add_alpha_p(d4, i, a, p4[i]);
 }
 
 // x += scale * d (FP64)
@@ -500,7 +526,7 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
    // index (2 or 4 bytes) per entry, the gathered input and the output (and
    // r, q for the reduction of the second)
    const double gidx = g16 ? 2.0 : 4.0;
-   auto learned_direction = [&](int fr, int fresh) {
+   auto learned_direction = [&](int fr, int fresh, int upd_d) {
       using bf = __nv_bfloat16;
       const bf* vl = reinterpret_cast<const bf*>(learned ? LP->gl->sell_valbf.p : nullptr);
       const bf* vu = reinterpret_cast<const bf*>(learned ? LP->gu->sell_valbf.p : nullptr);
@@ -522,7 +548,7 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
                     LP->gu->sell_col.p, vu, tz.p, zz.p, rr.p, q.p, S.p, partials.p, counter.p, fr,
                     worked);
       prof_end(PROF_LEARNED_APPLY, (2.0 + gidx) * LP->gu->nnz + 16.0 * n);
-      launch_pdl(lg_direction, gq, kRedBlock, nquads, zz.p, p.p, S.p, fresh);
+      launch_pdl(lg_direction, gq, kRedBlock, nquads, zz.p, p.p, d.p, upd_d, S.p, fresh);
    };
    MixState h{};
    true_residual(1);
@@ -547,9 +573,9 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
                                                        d.p, fresh ? 1 : 0, S.p, partials.p,
                                                        counter.p);
       count_launch();
-      if (learned) learned_direction(fresh ? 0 : 1, fresh ? 1 : 0);
+      if (learned) learned_direction(fresh ? 0 : 1, fresh ? 1 : 0, 0);
       else if (!fresh) {
-         mx_direction<<<gq, kRedBlock, 0, stream()>>>(nquads, rr.p, dinv.p, p.p, S.p);
+         mx_direction<<<gq, kRedBlock, 0, stream()>>>(nquads, rr.p, dinv.p, p.p, d.p, 0, S.p);
          count_launch();
       }
       fresh = false;
@@ -581,14 +607,14 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
             prof_end(bits == 32 ? PROF_SPMV32 : PROF_SPMV16,
                      ((bits == 32 ? 4.0 : 2.0) + aidx) * A->nnz + 12.0 * n + 4.0);
             if (learned) {
-               launch_pdl(mx_update<false>, gq, kRedBlock, nquads, d.p, p.p, rr.p, q.p, jac, S.p,
+               launch_pdl(mx_update<false>, gq, kRedBlock, nquads, rr.p, q.p, jac, S.p,
                           partials.p, counter.p, inner_tol, tol, scale, max_inner, mode);
-               learned_direction(0, 0);
+               learned_direction(0, 0, 1);
             }
             else {
-               launch_pdl(mx_update<true>, gq, kRedBlock, nquads, d.p, p.p, rr.p, q.p, dinv.p, S.p,
+               launch_pdl(mx_update<true>, gq, kRedBlock, nquads, rr.p, q.p, dinv.p, S.p,
                           partials.p, counter.p, inner_tol, tol, scale, max_inner, mode);
-               launch_pdl(mx_direction, gq, kRedBlock, nquads, rr.p, dinv.p, p.p, S.p);
+               launch_pdl(mx_direction, gq, kRedBlock, nquads, rr.p, dinv.p, p.p, d.p, 1, S.p);
             }
          }
          OFG_LAUNCH_CHECK();
@@ -606,6 +632,10 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
          batch = std::min(batch * 2, 64);
       }
       if (stalled) break;
+      // the iteration that paused the loop skipped its direction kernel,
+      // which would have made its d += alpha p
+      mx_flush_d<<<gq, kRedBlock, 0, stream()>>>(nquads, d.p, p.p, S.p);
+      count_launch();
       // refinement step in FP64
       mx_correct<<<gn, kRedBlock, 0, stream()>>>(n, x, d.p, scale);
       count_launch();
