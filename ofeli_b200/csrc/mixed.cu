@@ -150,15 +150,42 @@ __device__ __forceinline__ int4 load_cols(const int16_t* p, int64_t r0)
    return make_int4(r + d.x, r + 1 + d.y, r + 2 + d.z, r + 3 + d.w);
 }
 
-// q = A p over four rows per thread, (p, q) -> alpha
+// When the host must refine (mode 0) or stop the inner solve (mode 1).
+struct StopRule {
+   double delta, tol, scale;
+   int max_inner, mode;
+};
+
+// Decision after iteration `it` from ||r||^2: every block of the deciding
+// kernel takes it from the same totals; block 0 records ||r||, the count
+// and the pause for the host and the later kernels.
+__device__ __forceinline__ bool decide_pause(MixState* S, double rr2, int it, const StopRule& st)
+{
+   const double rn = sqrt(rr2);
+   bool stop;
+   if (st.mode == 0)
+      // refine when the residual fell by delta, or when the recurrence says
+      // the FP64 target is reached
+      stop = rn <= st.delta * S->rmark || rn * st.scale <= st.tol * S->bnorm || it >= st.max_inner;
+   else
+      stop = rn <= st.delta * S->res0 || it >= st.max_inner;
+   if (blockIdx.x == 0 && threadIdx.x == 0) {
+      S->rn = rn;
+      S->it = it;
+      if (stop) S->pause = 1;
+   }
+   return stop;
+}
+
+// q = A p over four rows per thread; (p, q) left as per-block partials for
+// mx_update
 template <class T, class I>
 __global__ void __launch_bounds__(kRedBlock, 8) mx_spmv(int64_t nquads, const int32_t* __restrict__ sp,
                                                      const I* __restrict__ scol,
                                                      const T* __restrict__ sval,
                                                      const float* __restrict__ p,
-                                                     float* __restrict__ q, MixState* S,
-                                                     double* partials, unsigned* counter,
-                                                     int* worked)
+                                                     float* __restrict__ q, const MixState* S,
+                                                     double* pq, int* worked)
 {
    pdl_wait();
    pdl_release();
@@ -188,26 +215,29 @@ __global__ void __launch_bounds__(kRedBlock, 8) mx_spmv(int64_t nquads, const in
       v[0] += (double)pr.x * acc.x + (double)pr.y * acc.y + (double)pr.z * acc.z +
               (double)pr.w * acc.w;
    }
-   double t[1];
-   if (grid_reduce<1>(v, partials, counter, t)) S->alpha = S->rho[S->it & 1] / t[0];
+   block_partials<1>(v, pq);
 }
 
-// r -= alpha q; ||r||, (r, D r) when JAC; decides when the host must refine
-// (mode 0) or stop the inner solve (mode 1).  The matching d += alpha p is
-// made by the direction kernel, which reads p anyway (or by mx_flush_d when
-// this iteration pauses the loop).
+// alpha = rho_it / (p, q) from the SpMV's partials (it = iterations done);
+// r -= alpha q; ||r|| and, when JAC, (r, D r) left as partials for the
+// kernel that decides (lg_lower or mx_direction).  The matching
+// d += alpha p is made by the direction kernel, which reads p anyway (or by
+// mx_flush_d when this iteration pauses the loop).
 template <bool JAC>
 __global__ void __launch_bounds__(kRedBlock, 8) mx_update(int64_t nquads, float* rr,
                                                        const float* __restrict__ q,
                                                        const float* __restrict__ dinv, MixState* S,
-                                                       double* partials, unsigned* counter,
-                                                       double delta, double tol, double scale,
-                                                       int max_inner, int mode)
+                                                       const double* __restrict__ pq,
+                                                       double* rpart, int it)
 {
    pdl_wait();
    pdl_release();
    if (S->pause) return;
-   const float a = (float)S->alpha;
+   double pqt[1];
+   partials_total<1>(pq, gridDim.x, pqt);
+   const double alpha = S->rho[it & 1] / pqt[0];
+   if (blockIdx.x == 0 && threadIdx.x == 0) S->alpha = alpha;
+   const float a = (float)alpha;
    double v[2] = {0.0, 0.0};
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
    float4* r4 = reinterpret_cast<float4*>(rr);
@@ -225,22 +255,7 @@ __global__ void __launch_bounds__(kRedBlock, 8) mx_update(int64_t nquads, float*
                  (double)ri.z * (ri.z * mi.z) + (double)ri.w * (ri.w * mi.w);
       }
    }
-   double t[2];
-   if (grid_reduce<2>(v, partials, counter, t)) {
-      S->rn = sqrt(t[0]);
-      const int it = S->it + 1;
-      if (JAC) S->rho[it & 1] = t[1];
-      S->it = it;
-      if (mode == 0) {
-         // refine when the residual fell by delta, or when the recurrence
-         // says the FP64 target is reached
-         if (S->rn <= delta * S->rmark || S->rn * scale <= tol * S->bnorm || it >= max_inner)
-            S->pause = 1;
-      }
-      else if (S->rn <= delta * S->res0 || it >= max_inner) {
-         S->pause = 1;
-      }
-   }
+   block_partials<2>(v, rpart);
 }
 
 // d += alpha p with this iteration's alpha and p (upd_d), then the new
@@ -252,17 +267,32 @@ __device__ __forceinline__ void add_alpha_p(float4* d4, int64_t i, float a, cons
    d4[i] = di;
 }
 
-// (d += alpha p;) p = D r + beta p, beta = rho_it / rho_{it-1}
+// After iteration `it` (decide): the stop decision and rho_it = (r, D r)
+// from mx_update's partials; then (d += alpha p;) p = D r + beta p,
+// beta = rho_it / rho_{it-1}.  Right after a refinement (no decide) rho_it
+// is the one mx_load_residual stored.
 __global__ void __launch_bounds__(kRedBlock, 8) mx_direction(int64_t nquads,
                                                           const float* __restrict__ rr,
                                                           const float* __restrict__ dinv, float* p,
-                                                          float* d, int upd_d, const MixState* S)
+                                                          float* d, int upd_d, MixState* S,
+                                                          const double* __restrict__ rpart, int it,
+                                                          int decide, StopRule st)
 {
    pdl_wait();
    pdl_release();
    if (S->pause) return;
-   const int it = S->it;
-   const float beta = (float)(S->rho[it & 1] / S->rho[(it + 1) & 1]);
+   double rho;
+   if (decide) {
+      double tot[2];
+      partials_total<2>(rpart, gridDim.x, tot);
+      rho = tot[1];
+      if (blockIdx.x == 0 && threadIdx.x == 0) S->rho[it & 1] = rho;
+      if (decide_pause(S, tot[0], it, st)) return;
+   }
+   else {
+      rho = S->rho[it & 1];
+   }
+   const float beta = (float)(rho / S->rho[(it + 1) & 1]);
    const float a = (float)S->alpha;
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
    float4* p4 = reinterpret_cast<float4*>(p);
@@ -310,35 +340,39 @@ __device__ __forceinline__ float4 sell_quad(const int32_t* __restrict__ sp,
    return acc;
 }
 
-// t = G r
+// After iteration `it` (decide): the stop decision from mx_update's
+// partials; then t = G r
 template <class V, class I>
 __global__ void __launch_bounds__(kRedBlock, 8) lg_lower(int64_t nquads, const int32_t* __restrict__ sp,
                                                       const I* __restrict__ scol,
                                                       const V* __restrict__ sval,
                                                       const float* __restrict__ r, float* t,
-                                                      const MixState* S, int* worked)
+                                                      MixState* S, const double* __restrict__ rpart,
+                                                      int it, int decide, StopRule st, int* worked)
 {
    pdl_wait();
    pdl_release();
    if (S->pause) return;
+   if (decide) {
+      double tot[2];
+      partials_total<2>(rpart, gridDim.x, tot);
+      if (decide_pause(S, tot[0], it, st)) return;
+   }
    prof_mark(worked);
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nquads; i += stride)
       *reinterpret_cast<float4*>(t + i * 4) = sell_quad(sp, scol, sval, r, i * 4);
 }
 
-// z = G^T t; rho = (r, z); beta of the next direction: flexible
-// (Polak-Ribiere) -alpha (z, q) / rho_old, or rho / rho_old right after a
-// refinement replaced r (fr = 1)
+// z = G^T t; (r, z) and (q, z) left as partials for lg_direction
 template <class V, class I>
 __global__ void __launch_bounds__(kRedBlock, 8) lg_upper(int64_t nquads, const int32_t* __restrict__ sp,
                                                       const I* __restrict__ scol,
                                                       const V* __restrict__ sval,
                                                       const float* __restrict__ t, float* z,
                                                       const float* __restrict__ r,
-                                                      const float* __restrict__ q, MixState* S,
-                                                      double* partials, unsigned* counter, int fr,
-                                                      int* worked)
+                                                      const float* __restrict__ q, const MixState* S,
+                                                      double* cpart, int* worked)
 {
    pdl_wait();
    pdl_release();
@@ -354,25 +388,31 @@ __global__ void __launch_bounds__(kRedBlock, 8) lg_upper(int64_t nquads, const i
       v[0] += (double)ri.x * zi.x + (double)ri.y * zi.y + (double)ri.z * zi.z + (double)ri.w * zi.w;
       v[1] += (double)qi.x * zi.x + (double)qi.y * zi.y + (double)qi.z * zi.z + (double)qi.w * zi.w;
    }
-   double tt[2];
-   if (grid_reduce<2>(v, partials, counter, tt)) {
-      const int it = S->it;
-      const double old = S->rho[(it + 1) & 1];
-      S->rho[it & 1] = tt[0];
-      S->beta = fr ? tt[0] / old : -S->alpha * tt[1] / old;
-   }
+   block_partials<2>(v, cpart);
 }
 
-// (d += alpha p;) p = z + beta p (p = z on a fresh start)
+// rho_it = (r, z) from lg_upper's partials; beta of the new direction:
+// flexible (Polak-Ribiere) -alpha (z, q) / rho_{it-1}, or rho_it / rho_{it-1}
+// right after a refinement replaced r (fr = 1); then (d += alpha p;)
+// p = z + beta p (p = z on a fresh start)
 __global__ void __launch_bounds__(kRedBlock, 8) lg_direction(int64_t nquads,
                                                           const float* __restrict__ z, float* p,
-                                                          float* d, int upd_d, const MixState* S,
-                                                          int fresh)
+                                                          float* d, int upd_d, MixState* S,
+                                                          const double* __restrict__ cpart, int it,
+                                                          int fr, int fresh)
 {
    pdl_wait();
    pdl_release();
    if (S->pause) return;
-   const float beta = fresh ? 0.f : (float)S->beta;
+   double tot[2];
+   partials_total<2>(cpart, gridDim.x, tot);
+   const double old = S->rho[(it + 1) & 1];
+   const double bd = fr ? tot[0] / old : -S->alpha * tot[1] / old;
+   if (blockIdx.x == 0 && threadIdx.x == 0) {
+      S->rho[it & 1] = tot[0];
+      S->beta = bd;
+   }
+   const float beta = fresh ? 0.f : (float)bd;
    const float a = (float)S->alpha;
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
    float4* p4 = reinterpret_cast<float4*>(p);
@@ -513,6 +553,13 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
    }
    const float* jac = learned ? nullptr : dinv.p;
    const unsigned gq = grid_for(nquads, kRedBlock, 8);
+   // per-block partials of the reductions that the next kernel finishes:
+   // (p, q) of the SpMV, ||r||^2 and (r, D r) of the update, (r, z) and
+   // (q, z) of the product with G^T
+   DBuf<double> red(5 * (size_t)gq + 1);
+   double* const pq = red.p;
+   double* const rpart = red.p + gq;
+   double* const cpart = red.p + 3 * (size_t)gq;
    const unsigned gn = grid_for(n, kRedBlock, 8);
    auto true_residual = [&](int first) {
       spmv_sell(A, x, q64.p);
@@ -526,29 +573,29 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
    // index (2 or 4 bytes) per entry, the gathered input and the output (and
    // r, q for the reduction of the second)
    const double gidx = g16 ? 2.0 : 4.0;
-   auto learned_direction = [&](int fr, int fresh, int upd_d) {
+   auto learned_direction = [&](int fr, int fresh, int upd_d, int it, int decide,
+                                const StopRule& st) {
       using bf = __nv_bfloat16;
       const bf* vl = reinterpret_cast<const bf*>(learned ? LP->gl->sell_valbf.p : nullptr);
       const bf* vu = reinterpret_cast<const bf*>(learned ? LP->gu->sell_valbf.p : nullptr);
       int* worked = prof_begin();
       if (g16)
          launch_pdl(lg_lower<bf, int16_t>, gq, kRedBlock, nquads, LP->gl->sell_ptr.p,
-                    LP->gl->sell_d16.p, vl, rr.p, tz.p, S.p, worked);
+                    LP->gl->sell_d16.p, vl, rr.p, tz.p, S.p, rpart, it, decide, st, worked);
       else
          launch_pdl(lg_lower<bf, int32_t>, gq, kRedBlock, nquads, LP->gl->sell_ptr.p,
-                    LP->gl->sell_col.p, vl, rr.p, tz.p, S.p, worked);
+                    LP->gl->sell_col.p, vl, rr.p, tz.p, S.p, rpart, it, decide, st, worked);
       prof_end(PROF_LEARNED_APPLY, (2.0 + gidx) * LP->gl->nnz + 8.0 * n);
       worked = prof_begin();
       if (g16)
          launch_pdl(lg_upper<bf, int16_t>, gq, kRedBlock, nquads, LP->gu->sell_ptr.p,
-                    LP->gu->sell_d16.p, vu, tz.p, zz.p, rr.p, q.p, S.p, partials.p, counter.p, fr,
-                    worked);
+                    LP->gu->sell_d16.p, vu, tz.p, zz.p, rr.p, q.p, S.p, cpart, worked);
       else
          launch_pdl(lg_upper<bf, int32_t>, gq, kRedBlock, nquads, LP->gu->sell_ptr.p,
-                    LP->gu->sell_col.p, vu, tz.p, zz.p, rr.p, q.p, S.p, partials.p, counter.p, fr,
-                    worked);
+                    LP->gu->sell_col.p, vu, tz.p, zz.p, rr.p, q.p, S.p, cpart, worked);
       prof_end(PROF_LEARNED_APPLY, (2.0 + gidx) * LP->gu->nnz + 16.0 * n);
-      launch_pdl(lg_direction, gq, kRedBlock, nquads, zz.p, p.p, d.p, upd_d, S.p, fresh);
+      launch_pdl(lg_direction, gq, kRedBlock, nquads, zz.p, p.p, d.p, upd_d, S.p, cpart, it, fr,
+                 fresh);
    };
    MixState h{};
    true_residual(1);
@@ -573,9 +620,11 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
                                                        d.p, fresh ? 1 : 0, S.p, partials.p,
                                                        counter.p);
       count_launch();
-      if (learned) learned_direction(fresh ? 0 : 1, fresh ? 1 : 0, 0);
+      const StopRule st{inner_tol, tol, scale, max_inner, mode};
+      if (learned) learned_direction(fresh ? 0 : 1, fresh ? 1 : 0, 0, h.it, 0, st);
       else if (!fresh) {
-         mx_direction<<<gq, kRedBlock, 0, stream()>>>(nquads, rr.p, dinv.p, p.p, d.p, 0, S.p);
+         mx_direction<<<gq, kRedBlock, 0, stream()>>>(nquads, rr.p, dinv.p, p.p, d.p, 0, S.p, rpart,
+                                                      h.it, 0, st);
          count_launch();
       }
       fresh = false;
@@ -583,38 +632,41 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
       double mark_rn = h.rel * h.bnorm / scale;
       int batch = 8;
       for (;;) {
+         // iterations done when the batch starts; the kernels of the batch's
+         // k-th iteration get it0 + k (and it0 + k + 1 once it is done)
+         const int it0 = h.it;
          for (int k = 0; k < batch; ++k) {
+            const int cur = it0 + k;
             // the kernels of an iteration chain with programmatic dependent
             // launch: each one's blocks start while the previous one drains
             // its reduction tail
             int* worked = prof_begin();
             if (bits == 32 && a16)
                launch_pdl(mx_spmv<float, int16_t>, gq, kRedBlock, nquads, A->sell_ptr.p,
-                          A->sell_d16.p, A->sell_val32.p, p.p, q.p, S.p, partials.p, counter.p,
-                          worked);
+                          A->sell_d16.p, A->sell_val32.p, p.p, q.p, S.p, pq, worked);
             else if (bits == 32)
                launch_pdl(mx_spmv<float, int32_t>, gq, kRedBlock, nquads, A->sell_ptr.p,
-                          A->sell_col.p, A->sell_val32.p, p.p, q.p, S.p, partials.p, counter.p,
-                          worked);
+                          A->sell_col.p, A->sell_val32.p, p.p, q.p, S.p, pq, worked);
             else if (a16)
                launch_pdl(mx_spmv<__nv_bfloat16, int16_t>, gq, kRedBlock, nquads, A->sell_ptr.p,
-                          A->sell_d16.p, v16.p, p.p, q.p, S.p, partials.p, counter.p, worked);
+                          A->sell_d16.p, v16.p, p.p, q.p, S.p, pq, worked);
             else
                launch_pdl(mx_spmv<__nv_bfloat16, int32_t>, gq, kRedBlock, nquads, A->sell_ptr.p,
-                          A->sell_col.p, v16.p, p.p, q.p, S.p, partials.p, counter.p, worked);
+                          A->sell_col.p, v16.p, p.p, q.p, S.p, pq, worked);
             // algorithmic bytes: value (4 or 2) + column index (4, or 2 as a
             // 16-bit offset) per entry, p gathered, q written, p read for the dot
             prof_end(bits == 32 ? PROF_SPMV32 : PROF_SPMV16,
                      ((bits == 32 ? 4.0 : 2.0) + aidx) * A->nnz + 12.0 * n + 4.0);
             if (learned) {
-               launch_pdl(mx_update<false>, gq, kRedBlock, nquads, rr.p, q.p, jac, S.p,
-                          partials.p, counter.p, inner_tol, tol, scale, max_inner, mode);
-               learned_direction(0, 0, 1);
+               launch_pdl(mx_update<false>, gq, kRedBlock, nquads, rr.p, q.p, jac, S.p, pq,
+                          rpart, cur);
+               learned_direction(0, 0, 1, cur + 1, 1, st);
             }
             else {
-               launch_pdl(mx_update<true>, gq, kRedBlock, nquads, rr.p, q.p, dinv.p, S.p,
-                          partials.p, counter.p, inner_tol, tol, scale, max_inner, mode);
-               launch_pdl(mx_direction, gq, kRedBlock, nquads, rr.p, dinv.p, p.p, d.p, 1, S.p);
+               launch_pdl(mx_update<true>, gq, kRedBlock, nquads, rr.p, q.p, dinv.p, S.p, pq,
+                          rpart, cur);
+               launch_pdl(mx_direction, gq, kRedBlock, nquads, rr.p, dinv.p, p.p, d.p, 1, S.p,
+                          rpart, cur + 1, 1, st);
             }
          }
          OFG_LAUNCH_CHECK();
