@@ -498,24 +498,36 @@ void gmres_solve(ofg_prec* P, const double* b, double* x, int m, int max_it, dou
    while (!h.done) {
       gm_start<<<g, kRedBlock, 0, stream()>>>(n, r.p, V.p, s.p, m, S.p);
       count_launch();
-      for (int i = 0; i < m; ++i) {
-         double* vi = V.p + (size_t)i * n;
-         spmv_sell(A, vi, w.p, &S.p->stop);
-         precond_inplace(w.p, &S.p->stop);
-         for (int k = 0; k <= i; ++k) {
-            gm_mgs<<<g, kRedBlock, 0, stream()>>>(
-               n, w.p, k > 0 ? V.p + (size_t)(k - 1) * n : nullptr,
-               k > 0 ? H.p + (size_t)(k - 1) * ld + i : nullptr, V.p + (size_t)k * n,
-               H.p + (size_t)k * ld + i, rs.partials.p, rs.counter.p, S.p);
+      // the cycle's iterations go out in batches of 4, 8, 16, ... with one
+      // read of the state after each: once gm_givens has stopped the cycle,
+      // the kernels of its remaining iterations (which would all return at
+      // once) are not launched
+      int i = 0;
+      for (int batch = 4; i < m; batch *= 2) {
+         const int end = std::min(m, i + batch);
+         for (; i < end; ++i) {
+            double* vi = V.p + (size_t)i * n;
+            spmv_sell(A, vi, w.p, &S.p->stop);
+            precond_inplace(w.p, &S.p->stop);
+            for (int k = 0; k <= i; ++k) {
+               gm_mgs<<<g, kRedBlock, 0, stream()>>>(
+                  n, w.p, k > 0 ? V.p + (size_t)(k - 1) * n : nullptr,
+                  k > 0 ? H.p + (size_t)(k - 1) * ld + i : nullptr, V.p + (size_t)k * n,
+                  H.p + (size_t)k * ld + i, rs.partials.p, rs.counter.p, S.p);
+            }
+            gm_mgs_last<<<g, kRedBlock, 0, stream()>>>(n, w.p, vi, H.p + (size_t)i * ld + i,
+                                                       H.p + (size_t)(i + 1) * ld + i, rs.partials.p,
+                                                       rs.counter.p, S.p);
+            gm_scale<<<g, kRedBlock, 0, stream()>>>(n, w.p, V.p + (size_t)(i + 1) * n,
+                                                    H.p + (size_t)(i + 1) * ld + i, S.p);
+            gm_givens<<<1, 32, 0, stream()>>>(H.p, s.p, cs.p, sn.p, i, m, S.p, tol, max_it);
+            count_launch(i + 5);
+            OFG_LAUNCH_CHECK();
          }
-         gm_mgs_last<<<g, kRedBlock, 0, stream()>>>(n, w.p, vi, H.p + (size_t)i * ld + i,
-                                                    H.p + (size_t)(i + 1) * ld + i, rs.partials.p,
-                                                    rs.counter.p, S.p);
-         gm_scale<<<g, kRedBlock, 0, stream()>>>(n, w.p, V.p + (size_t)(i + 1) * n,
-                                                 H.p + (size_t)(i + 1) * ld + i, S.p);
-         gm_givens<<<1, 32, 0, stream()>>>(H.p, s.p, cs.p, sn.p, i, m, S.p, tol, max_it);
-         count_launch(i + 5);
-         OFG_LAUNCH_CHECK();
+         if (i < m) {
+            S.download(&h, 1);
+            if (h.stop) break;
+         }
       }
       S.download(&h, 1);
       if (P->type != OFG_IDENT && P->type != OFG_DIAG) check_status(P);
