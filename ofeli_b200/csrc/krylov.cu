@@ -235,16 +235,26 @@ __global__ void gm_start(int64_t n, const double* __restrict__ r, double* v0, do
 }
 
 // Modified Gram-Schmidt step k of column i: w -= h_{k-1} v_{k-1} (k > 0),
-// then h_k = (w, v_k).
+// then h_k = (w, v_k).  The chain gm_mgs(0..i), gm_mgs_last, gm_scale
+// finishes each dot product in the next kernel: a kernel leaves its
+// per-block partials in `pout`; the next one sums them (pin) in every block,
+// in the order of a last-block reduction, and its block 0 stores the
+// Hessenberg entry.
 __global__ void __launch_bounds__(kRedBlock, 8) gm_mgs(int64_t n, double* w,
                                                     const double* __restrict__ vprev,
-                                                    const double* hprev,
-                                                    const double* __restrict__ vk, double* hk,
-                                                    double* partials, unsigned* counter,
+                                                    double* hprev,
+                                                    const double* __restrict__ vk,
+                                                    const double* __restrict__ pin, double* pout,
                                                     const GMState* S)
 {
    if (S->stop) return;
-   const double h = hprev ? *hprev : 0.0;
+   double h = 0.0;
+   if (hprev) {
+      double tot[1];
+      partials_total<1>(pin, gridDim.x, tot);
+      h = tot[0];
+      if (blockIdx.x == 0 && threadIdx.x == 0) *hprev = h;
+   }
    double v[1] = {0.0};
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
@@ -255,19 +265,21 @@ __global__ void __launch_bounds__(kRedBlock, 8) gm_mgs(int64_t n, double* w,
       }
       v[0] += wi * vk[i];
    }
-   double t[1];
-   if (grid_reduce<1>(v, partials, counter, t)) *hk = t[0];
+   block_partials<1>(v, pout);
 }
 
-// last projection w -= h_i v_i and H(i+1,i) = ||w||
+// last projection w -= h_i v_i (h_i = H(i,i) from the partials of
+// gm_mgs(i)); ||w||^2 left as partials for gm_scale
 __global__ void __launch_bounds__(kRedBlock, 8) gm_mgs_last(int64_t n, double* w,
-                                                         const double* __restrict__ vi,
-                                                         const double* hi, double* hnext,
-                                                         double* partials, unsigned* counter,
-                                                         const GMState* S)
+                                                         const double* __restrict__ vi, double* hi,
+                                                         const double* __restrict__ pin,
+                                                         double* pout, const GMState* S)
 {
    if (S->stop) return;
-   const double h = *hi;
+   double tot[1];
+   partials_total<1>(pin, gridDim.x, tot);
+   const double h = tot[0];
+   if (blockIdx.x == 0 && threadIdx.x == 0) *hi = h;
    double v[1] = {0.0};
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
@@ -275,15 +287,21 @@ __global__ void __launch_bounds__(kRedBlock, 8) gm_mgs_last(int64_t n, double* w
       w[i] = wi;
       v[0] += wi * wi;
    }
-   double t[1];
-   if (grid_reduce<1>(v, partials, counter, t)) *hnext = sqrt(t[0]);
+   block_partials<1>(v, pout);
 }
 
-__global__ void gm_scale(int64_t n, const double* __restrict__ w, double* vnext, const double* h,
-                         const GMState* S)
+// H(i+1,i) = ||w|| from the partials of gm_mgs_last; v_{i+1} = w / H(i+1,i)
+__global__ void __launch_bounds__(kRedBlock, 8) gm_scale(int64_t n, const double* __restrict__ w,
+                                                      double* vnext, double* h,
+                                                      const double* __restrict__ pin,
+                                                      const GMState* S)
 {
    if (S->stop) return;
-   const double sc = 1.0 / *h;
+   double tot[1];
+   partials_total<1>(pin, gridDim.x, tot);
+   const double hn = sqrt(tot[0]);
+   if (blockIdx.x == 0 && threadIdx.x == 0) *h = hn;
+   const double sc = 1.0 / hn;
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
       vnext[i] = sc * w[i];
@@ -479,6 +497,9 @@ void gmres_solve(ofg_prec* P, const double* b, double* x, int m, int max_it, dou
    DBuf<GMState> S(1);
    RedScratch rs(n);
    const unsigned g = red_grid(n);
+   // the two partial buffers the Gram-Schmidt chain alternates between
+   DBuf<double> gp(2 * (size_t)g);
+   double* const gpb[2] = {gp.p, gp.p + g};
    const int ld = m + 1;
    auto precond_inplace = [&](double* v, const int* skip) {
       if (P->type == OFG_IDENT) return;
@@ -509,17 +530,19 @@ void gmres_solve(ofg_prec* P, const double* b, double* x, int m, int max_it, dou
             double* vi = V.p + (size_t)i * n;
             spmv_sell(A, vi, w.p, &S.p->stop);
             precond_inplace(w.p, &S.p->stop);
+            // gm_mgs(k) writes gpb[k & 1]; H(k-1,i) is stored by gm_mgs(k),
+            // H(i,i) by gm_mgs_last, H(i+1,i) by gm_scale
             for (int k = 0; k <= i; ++k) {
                gm_mgs<<<g, kRedBlock, 0, stream()>>>(
                   n, w.p, k > 0 ? V.p + (size_t)(k - 1) * n : nullptr,
                   k > 0 ? H.p + (size_t)(k - 1) * ld + i : nullptr, V.p + (size_t)k * n,
-                  H.p + (size_t)k * ld + i, rs.partials.p, rs.counter.p, S.p);
+                  gpb[(k + 1) & 1], gpb[k & 1], S.p);
             }
             gm_mgs_last<<<g, kRedBlock, 0, stream()>>>(n, w.p, vi, H.p + (size_t)i * ld + i,
-                                                       H.p + (size_t)(i + 1) * ld + i, rs.partials.p,
-                                                       rs.counter.p, S.p);
+                                                       gpb[i & 1], gpb[(i + 1) & 1], S.p);
             gm_scale<<<g, kRedBlock, 0, stream()>>>(n, w.p, V.p + (size_t)(i + 1) * n,
-                                                    H.p + (size_t)(i + 1) * ld + i, S.p);
+                                                    H.p + (size_t)(i + 1) * ld + i,
+                                                    gpb[(i + 1) & 1], S.p);
             gm_givens<<<1, 32, 0, stream()>>>(H.p, s.p, cs.p, sn.p, i, m, S.p, tol, max_it);
             count_launch(i + 5);
             OFG_LAUNCH_CHECK();
