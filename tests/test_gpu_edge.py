@@ -191,3 +191,49 @@ def test_nan_rhs_returns_like_oracle(cuda, solver):
     x2 = np.zeros(n)
     b2 = np.nan_to_num(b)
     assert F.CG(A, F.Prec(A, F.DIAG_PREC), b2, x2, 200, 1e-10) > 0
+
+
+@pytest.mark.parametrize("bits,mode", [(0, 0), (16, 0), (32, 0), (32, 1)])
+def test_mixed_precision_on_one_slice(cuda, bits, mode):
+    """A 4 x 3-cell system (6 unknowns: one SELL slice, one block per
+    kernel): the reductions carried from one kernel to the next run with a
+    single producer block; the FP64 target is met and the solution is the
+    oracle's FP64 one."""
+    rp, ci, a, b = small_system(4, 3, seed=8)
+    xref, _ = O.cg(rp, ci, a, b, O.DIAG, 1000, 1e-14)
+    A = F.SpMatrix(rp, ci, a)
+    x = np.zeros(A.n)
+    outer, inner, res = F.solve_mixed(A, b, x, prec=F.DIAG_PREC, inner_bits=bits, toler=1e-10,
+                                      mode=mode)
+    assert A.n == 6 and res <= 1e-10 and F.residual(A, b, x) <= 1e-10
+    assert rel_err(x, xref) <= 1e-9
+
+
+def test_learned_solve_on_one_slice(cuda):
+    """The learned flexible CG (untrained network: M is Jacobi) on the same
+    6-unknown system."""
+    rp, ci, a, b = small_system(4, 3, seed=8)
+    xref, _ = O.cg(rp, ci, a, b, O.DIAG, 1000, 1e-14)
+    A = F.SpMatrix(rp, ci, a)
+    P = F.Prec(A, F.LEARNED_PREC, net=F.LearnedNet(4))
+    x = np.zeros(A.n)
+    outer, inner, res, fell_back = F.fcg_learned(P, b, x, toler=1e-10)
+    assert res <= 1e-10 and not fell_back
+    assert rel_err(x, xref) <= 1e-9
+
+
+@pytest.mark.parametrize("m", [1, 3, 4, 5, 8, 30])
+def test_gmres_restart_lengths_around_launch_batches(cuda, m):
+    """A GMRES cycle launches its iterations in batches of 4, 8, 16, ... and
+    stops launching once the device-side test has stopped the cycle: restart
+    lengths below, at and across the batch sizes give the oracle's iteration
+    count and solution."""
+    rp, ci, a, b = small_system(24, 17, seed=6)
+    x0, it0 = O.gmres(rp, ci, a, b, O.DIAG, m, 5000, 1e-10)
+    A = F.SpMatrix(rp, ci, a)
+    x = np.zeros(A.n)
+    it = F.GMRes(A, F.Prec(A, F.DIAG_PREC), b, x, m, 5000, 1e-10)
+    # the parity band of the other Krylov tests; both solutions are at
+    # preconditioned residual 1e-10 of a 368-unknown Laplacian
+    assert abs(it - it0) <= 2
+    assert rel_err(x, x0) <= 1e-8
