@@ -73,6 +73,12 @@ def test_mixed_solve_full_size(big):
     # both solutions meet the same residual bound; they agree to the
     # conditioning-limited accuracy of that bound
     assert rel_err(x, x64) <= 1e-5
+    # every value of this matrix is exact in BF16, so the automatic value
+    # format streams BF16 values and the solve is bit for bit the FP32 one
+    xa = np.zeros(A.n)
+    assert F.solve_mixed(A, big["b"], xa, prec=F.DIAG_PREC, inner_bits=0,
+                         toler=1e-10) == (outer, inner, res)
+    assert np.array_equal(xa, x)
 
 
 def test_kuhn_129_pattern_and_values(cuda):
