@@ -32,6 +32,15 @@ struct ofg_matrix {
    // in 16 bits (idx16 = 1; 0 = does not fit; -1 = not built yet)
    ofg::DBuf<int16_t> sell_d16;
    int idx16 = -1;
+   // slices whose 32 rows have the same 16-bit offset at every position k
+   // (structured meshes in natural order): sell_uni[s] = start of the
+   // slice's w offsets in sell_utab, -1 for a slice that keeps per-entry
+   // offsets; uni_nnz = nonzeros in the uniform slices (built once, with the
+   // 16-bit offsets)
+   ofg::DBuf<int32_t> sell_uni;
+   ofg::DBuf<int16_t> sell_utab;
+   int64_t uni_nnz = 0, utab_len = 0;
+   bool uni_ready = false;
    bool sell_ready = false;
    uint64_t sell_version = 0, sell32_version = 0, sellbf_version = 0;
    int max_row = 0;
@@ -125,6 +134,8 @@ void ensure_sell32(ofg_matrix* A);
 void ensure_sell_bf16(ofg_matrix* A);
 // builds the 16-bit column offsets once per pattern; true when they fit
 bool ensure_sell_d16(ofg_matrix* A);
+// after ensure_sell_d16 returned true
+void ensure_sell_uniform(ofg_matrix* A);
 void spmv_csr(const ofg_matrix* A, const double* x, double* y, bool add);
 void spmv_sell(const ofg_matrix* A, const double* x, double* y, const int* skip = nullptr);
 void matrix_touch(ofg_matrix* A);

@@ -11,6 +11,9 @@
 //     two covering the mean row length), used where no SELL copy exists.
 #include <cuda_bf16.h>
 
+#include <cstdint>
+#include <vector>
+
 #include "internal.cuh"
 
 namespace ofg {
@@ -178,6 +181,48 @@ __global__ void sell_offsets16(int64_t nslices, const int32_t* sp, const int32_t
       if (d > 32767 || d < -32768) atomicOr(wide, 1);
       d16[idx] = (int16_t)d;
    }
+}
+
+// one warp per slice: the slice's width w when all 32 rows have the same
+// 16-bit offset at every position k, else -1; counts the nonzeros of the
+// uniform slices
+__global__ void sell_uniform_scan(int64_t nslices, const int32_t* __restrict__ sp,
+                                  const int16_t* __restrict__ d16,
+                                  const int32_t* __restrict__ ssrc, int32_t* width,
+                                  unsigned long long* uni_nnz)
+{
+   const int64_t s = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+   const int lane = threadIdx.x & 31;
+   if (s >= nslices) return;  // the whole warp shares s
+   const int64_t beg = sp[s];
+   const int w = (int)((sp[s + 1] - beg) >> 5);
+   bool uni = true;
+   int real = 0;
+   for (int k = 0; k < w; ++k) {
+      const int64_t idx = beg + (int64_t)k * 32 + lane;
+      const int16_t d = d16[idx];
+      const bool same = __all_sync(0xffffffffu, d == __shfl_sync(0xffffffffu, d, 0));
+      uni = uni && same;
+      real += ssrc[idx] >= 0 ? 1 : 0;
+   }
+#pragma unroll
+   for (int o = 16; o > 0; o >>= 1) real += __shfl_xor_sync(0xffffffffu, real, o);
+   if (lane == 0) {
+      width[s] = uni ? w : -1;
+      if (uni) atomicAdd(uni_nnz, (unsigned long long)real);
+   }
+}
+
+// the uniform slices' offsets, one per position k
+__global__ void sell_uniform_fill(int64_t nslices, const int32_t* __restrict__ sp,
+                                  const int16_t* __restrict__ d16,
+                                  const int32_t* __restrict__ uni, int16_t* tab)
+{
+   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   if (s >= nslices || uni[s] < 0) return;
+   const int64_t beg = sp[s];
+   const int w = (int)((sp[s + 1] - beg) >> 5);
+   for (int k = 0; k < w; ++k) tab[uni[s] + k] = d16[beg + (int64_t)k * 32];
 }
 
 // ------------------------------------------------------------------ SpMV --
@@ -491,6 +536,47 @@ bool ensure_sell_d16(ofg_matrix* A)
       if (!A->idx16) A->sell_d16.release();
    }
    return A->idx16 == 1;
+}
+
+void ensure_sell_uniform(ofg_matrix* A)
+{
+   if (A->uni_ready) return;
+   OFG_REQUIRE(A->idx16 == 1, OFG_ERR_ARG, "slice-uniform offsets need the 16-bit offsets");
+   const int64_t ns = A->nslices;
+   A->sell_uni.alloc(ns > 0 ? ns : 1);
+   std::vector<int32_t> w((size_t)ns);
+   unsigned long long hn = 0;
+   if (ns > 0) {
+      DBuf<unsigned long long> cnt(1);
+      cnt.zero();
+      sell_uniform_scan<<<(unsigned)((ns * 32 + 255) / 256), 256, 0, stream()>>>(
+         ns, A->sell_ptr.p, A->sell_d16.p, A->sell_src.p, A->sell_uni.p, cnt.p);
+      count_launch();
+      OFG_LAUNCH_CHECK();
+      A->sell_uni.download(w.data(), (size_t)ns);
+      cnt.download(&hn, 1);
+   }
+   // table positions: uniform slices in order, w offsets each
+   int64_t pos = 0;
+   for (int64_t s = 0; s < ns; ++s) {
+      if (w[(size_t)s] < 0) continue;
+      const int32_t ws = w[(size_t)s];
+      w[(size_t)s] = (int32_t)pos;
+      pos += ws;
+   }
+   OFG_REQUIRE(pos <= INT32_MAX, OFG_ERR_SIZE, "offset table too large");
+   A->utab_len = pos;
+   A->uni_nnz = (int64_t)hn;
+   A->sell_utab.alloc(pos > 0 ? pos : 1);
+   if (ns > 0) {
+      A->sell_uni.upload(w.data(), (size_t)ns);
+      sell_uniform_fill<<<(unsigned)((ns + 255) / 256), 256, 0, stream()>>>(
+         ns, A->sell_ptr.p, A->sell_d16.p, A->sell_uni.p, A->sell_utab.p);
+      count_launch();
+      OFG_LAUNCH_CHECK();
+   }
+   OFG_CUDA(cudaStreamSynchronize(stream()));
+   A->uni_ready = true;
 }
 
 void spmv_csr(const ofg_matrix* A, const double* x, double* y, bool add)

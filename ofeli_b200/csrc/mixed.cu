@@ -177,15 +177,36 @@ __device__ __forceinline__ bool decide_pause(MixState* S, double rr2, int it, co
    return stop;
 }
 
+// x[c .. c+3] with 16-byte loads: the aligned quad holding x[c] and, unless
+// c is a multiple of 4, the next one, shifted by c mod 4.  The rows of a
+// slice-uniform slice gather consecutive elements, so a thread's four
+// gathers become one or two vector loads (8 lanes of a slice cover 32
+// consecutive elements).  The second load may read up to 4 elements past
+// the last row: the gathered vectors carry 8 elements of slack.
+__device__ __forceinline__ float4 quad_at(const float* __restrict__ x, int c)
+{
+   const float4* x4 = reinterpret_cast<const float4*>(x);
+   const float4 a = __ldg(x4 + (c >> 2));
+   const int m = c & 3;
+   if (m == 0) return a;
+   const float4 b = __ldg(x4 + (c >> 2) + 1);
+   if (m == 1) return make_float4(a.y, a.z, a.w, b.x);
+   if (m == 2) return make_float4(a.z, a.w, b.x, b.y);
+   return make_float4(a.w, b.x, b.y, b.z);
+}
+
 // q = A p over four rows per thread; (p, q) left as per-block partials for
-// mx_update
-template <class T, class I>
+// mx_update.  UNI: slices with uniform offsets (suni[s] >= 0) read one
+// offset per position from stab and gather p with vector loads.
+template <class T, class I, bool UNI = false>
 __global__ void __launch_bounds__(kRedBlock, 8) mx_spmv(int64_t nquads, const int32_t* __restrict__ sp,
                                                      const I* __restrict__ scol,
                                                      const T* __restrict__ sval,
                                                      const float* __restrict__ p,
                                                      float* __restrict__ q, const MixState* S,
-                                                     double* pq, int* worked)
+                                                     double* pq, int* worked,
+                                                     const int32_t* __restrict__ suni = nullptr,
+                                                     const int16_t* __restrict__ stab = nullptr)
 {
    pdl_wait();
    pdl_release();
@@ -199,16 +220,40 @@ __global__ void __launch_bounds__(kRedBlock, 8) mx_spmv(int64_t nquads, const in
       const int lane0 = (int)(r0 & 31);
       const int32_t beg = sp[s], w = (sp[s + 1] - beg) >> 5;
       float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-      const I* cp = scol + beg + lane0;
       const T* vp = sval + beg + lane0;
+      const int32_t u = UNI ? suni[s] : -1;
+      if (u >= 0) {
+         const int16_t* tp = stab + u;
+#pragma unroll 1
+         for (int32_t k = 0; k < w; ++k) {
+            const float4 a = load_vals(vp + k * 32);
+            const float4 x = quad_at(p, (int)r0 + tp[k]);
+            acc.x += a.x * x.x;
+            acc.y += a.y * x.y;
+            acc.z += a.z * x.z;
+            acc.w += a.w * x.w;
+         }
+      }
+      else {
+         const I* cp = scol + beg + lane0;
+         auto step = [&](int32_t k) {
+            const int4 c = load_cols(cp + k * 32, r0);
+            const float4 a = load_vals(vp + k * 32);
+            acc.x += a.x * __ldg(p + c.x);
+            acc.y += a.y * __ldg(p + c.y);
+            acc.z += a.z * __ldg(p + c.z);
+            acc.w += a.w * __ldg(p + c.w);
+         };
+         // with uniform slices this path is the rare one: kept rolled so
+         // that it does not set the kernel's register count
+         if (UNI) {
+#pragma unroll 1
+            for (int32_t k = 0; k < w; ++k) step(k);
+         }
+         else {
 #pragma unroll 8
-      for (int32_t k = 0; k < w; ++k) {
-         const int4 c = load_cols(cp + k * 32, r0);
-         const float4 a = load_vals(vp + k * 32);
-         acc.x += a.x * __ldg(p + c.x);
-         acc.y += a.y * __ldg(p + c.y);
-         acc.z += a.z * __ldg(p + c.z);
-         acc.w += a.w * __ldg(p + c.w);
+            for (int32_t k = 0; k < w; ++k) step(k);
+         }
       }
       *reinterpret_cast<float4*>(q + r0) = acc;
       const float4 pr = *reinterpret_cast<const float4*>(p + r0);
@@ -316,39 +361,64 @@ __global__ void __launch_bounds__(kRedBlock, 8) mx_direction(int64_t nquads,
 // slices as A, with BF16 values (the preconditioner's own precision; the
 // flexible CG absorbs it) and 16-bit column offsets where they fit; a
 // thread owns four consecutive rows.
-template <class V, class I>
+template <class V, class I, bool UNI>
 __device__ __forceinline__ float4 sell_quad(const int32_t* __restrict__ sp,
                                             const I* __restrict__ scol,
                                             const V* __restrict__ sval,
-                                            const float* __restrict__ x, int64_t r0)
+                                            const float* __restrict__ x, int64_t r0,
+                                            const int32_t* __restrict__ suni,
+                                            const int16_t* __restrict__ stab)
 {
    const int64_t s = r0 >> 5;
    const int lane0 = (int)(r0 & 31);
    const int32_t beg = sp[s], w = (sp[s + 1] - beg) >> 5;
    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-   const I* cp = scol + beg + lane0;
    const V* vp = sval + beg + lane0;
-#pragma unroll 4
-   for (int32_t k = 0; k < w; ++k) {
+   const int32_t u = UNI ? suni[s] : -1;
+   if (u >= 0) {
+      const int16_t* tp = stab + u;
+#pragma unroll 1
+      for (int32_t k = 0; k < w; ++k) {
+         const float4 a = load_vals(vp + k * 32);
+         const float4 xv = quad_at(x, (int)r0 + tp[k]);
+         acc.x += a.x * xv.x;
+         acc.y += a.y * xv.y;
+         acc.z += a.z * xv.z;
+         acc.w += a.w * xv.w;
+      }
+      return acc;
+   }
+   const I* cp = scol + beg + lane0;
+   auto step = [&](int32_t k) {
       const int4 c = load_cols(cp + k * 32, r0);
       const float4 a = load_vals(vp + k * 32);
       acc.x += a.x * __ldg(x + c.x);
       acc.y += a.y * __ldg(x + c.y);
       acc.z += a.z * __ldg(x + c.z);
       acc.w += a.w * __ldg(x + c.w);
+   };
+   if (UNI) {
+#pragma unroll 1
+      for (int32_t k = 0; k < w; ++k) step(k);
+   }
+   else {
+#pragma unroll 4
+      for (int32_t k = 0; k < w; ++k) step(k);
    }
    return acc;
 }
 
 // After iteration `it` (decide): the stop decision from mx_update's
 // partials; then t = G r
-template <class V, class I>
+template <class V, class I, bool UNI = false>
 __global__ void __launch_bounds__(kRedBlock, 8) lg_lower(int64_t nquads, const int32_t* __restrict__ sp,
                                                       const I* __restrict__ scol,
                                                       const V* __restrict__ sval,
                                                       const float* __restrict__ r, float* t,
                                                       MixState* S, const double* __restrict__ rpart,
-                                                      int it, int decide, StopRule st, int* worked)
+                                                      int it, int decide, StopRule st, int* worked,
+                                                      const int32_t* __restrict__ suni = nullptr,
+                                                      const int16_t* __restrict__ stab = nullptr)
 {
    pdl_wait();
    pdl_release();
@@ -361,18 +431,21 @@ __global__ void __launch_bounds__(kRedBlock, 8) lg_lower(int64_t nquads, const i
    prof_mark(worked);
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nquads; i += stride)
-      *reinterpret_cast<float4*>(t + i * 4) = sell_quad(sp, scol, sval, r, i * 4);
+      *reinterpret_cast<float4*>(t + i * 4) =
+         sell_quad<V, I, UNI>(sp, scol, sval, r, i * 4, suni, stab);
 }
 
 // z = G^T t; (r, z) and (q, z) left as partials for lg_direction
-template <class V, class I>
+template <class V, class I, bool UNI = false>
 __global__ void __launch_bounds__(kRedBlock, 8) lg_upper(int64_t nquads, const int32_t* __restrict__ sp,
                                                       const I* __restrict__ scol,
                                                       const V* __restrict__ sval,
                                                       const float* __restrict__ t, float* z,
                                                       const float* __restrict__ r,
                                                       const float* __restrict__ q, const MixState* S,
-                                                      double* cpart, int* worked)
+                                                      double* cpart, int* worked,
+                                                      const int32_t* __restrict__ suni = nullptr,
+                                                      const int16_t* __restrict__ stab = nullptr)
 {
    pdl_wait();
    pdl_release();
@@ -381,7 +454,7 @@ __global__ void __launch_bounds__(kRedBlock, 8) lg_upper(int64_t nquads, const i
    double v[2] = {0.0, 0.0};
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nquads; i += stride) {
-      const float4 zi = sell_quad(sp, scol, sval, t, i * 4);
+      const float4 zi = sell_quad<V, I, UNI>(sp, scol, sval, t, i * 4, suni, stab);
       *reinterpret_cast<float4*>(z + i * 4) = zi;
       const float4 ri = *reinterpret_cast<const float4*>(r + i * 4);
       const float4 qi = *reinterpret_cast<const float4*>(q + i * 4);
@@ -476,6 +549,15 @@ __global__ void inv_diag32(int64_t n, int64_t npad, const int32_t* dpos, const d
    }
 }
 
+// The uniform-slice kernels keep their per-entry path rolled (registers), so
+// they pay off only when nearly every entry sits in a uniform slice: with
+// 95 % (2-D square in natural order) a step took 16 % less time, with 72 %
+// (3-D Kuhn cube, whose grid lines of 127 rows cut many slices) 13 % more.
+bool mostly_uniform(const ofg_matrix* M)
+{
+   return M->utab_len > 0 && M->uni_nnz >= 0.9 * (double)M->nnz;
+}
+
 }  // namespace
 
 void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const double* b, double* x,
@@ -501,12 +583,27 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
       g16 = ensure_sell_d16(LP->gl) && ensure_sell_d16(LP->gu);
       OFG_REQUIRE(LP->gl->nslices == A->nslices && LP->gu->nslices == A->nslices, OFG_ERR_ARG,
                   "learned factor does not match the matrix");
+      if (g16) {
+         ensure_sell_uniform(LP->gl);
+         ensure_sell_uniform(LP->gu);
+      }
    }
+   const bool luni = g16 && mostly_uniform(LP->gl), uuni = g16 && mostly_uniform(LP->gu);
    const int64_t npad = A->nslices * 32, nquads = npad / 4;
    // 16-bit column offsets when every |column - row| fits (banded orderings,
    // structured meshes): 2 bytes less per entry streamed by every SpMV
    const bool a16 = ensure_sell_d16(A);
-   const double aidx = a16 ? 2.0 : 4.0;
+   // slices whose rows share their offsets read one offset per position and
+   // gather p with vector loads
+   if (a16) ensure_sell_uniform(A);
+   const bool auni = a16 && mostly_uniform(A);
+   // index bytes streamed per product: 2 per entry outside the uniform
+   // slices, the uniform slices' table
+   auto index_bytes = [](const ofg_matrix* M, bool d16, bool uni) {
+      if (!d16) return 4.0 * M->nnz;
+      if (!uni) return 2.0 * M->nnz;
+      return 2.0 * (M->nnz - M->uni_nnz) + 2.0 * M->utab_len;
+   };
    // bad[0]: zero diagonal entry; bad[1]: a value of A is not exact in BF16
    DBuf<int> bad(2);
    bad.zero();
@@ -527,8 +624,9 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
       count_launch();
    }
    const int64_t nv = npad > 0 ? npad : 4;
-   DBuf<float> dinv(nv), rr(nv), p(nv), q(nv), d(nv);
-   DBuf<float> tz(learned ? nv : 1), zz(learned ? nv : 1);
+   // p, r and t are gathered: 8 elements of slack for quad_at
+   DBuf<float> dinv(nv), rr(nv + 8), p(nv + 8), q(nv), d(nv);
+   DBuf<float> tz(learned ? nv + 8 : 1), zz(learned ? nv : 1);
    DBuf<double> r(n > 0 ? n : 1), q64(n > 0 ? n : 1);
    DBuf<MixState> S(1);
    p.zero();
@@ -572,28 +670,41 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
    // algorithmic bytes of the two factor products: BF16 value + column
    // index (2 or 4 bytes) per entry, the gathered input and the output (and
    // r, q for the reduction of the second)
-   const double gidx = g16 ? 2.0 : 4.0;
+   const double gl_bytes = learned ? 2.0 * LP->gl->nnz + index_bytes(LP->gl, g16, luni) : 0.0;
+   const double gu_bytes = learned ? 2.0 * LP->gu->nnz + index_bytes(LP->gu, g16, uuni) : 0.0;
    auto learned_direction = [&](int fr, int fresh, int upd_d, int it, int decide,
                                 const StopRule& st) {
       using bf = __nv_bfloat16;
       const bf* vl = reinterpret_cast<const bf*>(learned ? LP->gl->sell_valbf.p : nullptr);
       const bf* vu = reinterpret_cast<const bf*>(learned ? LP->gu->sell_valbf.p : nullptr);
       int* worked = prof_begin();
-      if (g16)
+      if (luni)
+         launch_pdl(lg_lower<bf, int16_t, true>, gq, kRedBlock, nquads, LP->gl->sell_ptr.p,
+                    LP->gl->sell_d16.p, vl, rr.p, tz.p, S.p, rpart, it, decide, st, worked,
+                    LP->gl->sell_uni.p, LP->gl->sell_utab.p);
+      else if (g16)
          launch_pdl(lg_lower<bf, int16_t>, gq, kRedBlock, nquads, LP->gl->sell_ptr.p,
-                    LP->gl->sell_d16.p, vl, rr.p, tz.p, S.p, rpart, it, decide, st, worked);
+                    LP->gl->sell_d16.p, vl, rr.p, tz.p, S.p, rpart, it, decide, st, worked,
+                    nullptr, nullptr);
       else
          launch_pdl(lg_lower<bf, int32_t>, gq, kRedBlock, nquads, LP->gl->sell_ptr.p,
-                    LP->gl->sell_col.p, vl, rr.p, tz.p, S.p, rpart, it, decide, st, worked);
-      prof_end(PROF_LEARNED_APPLY, (2.0 + gidx) * LP->gl->nnz + 8.0 * n);
+                    LP->gl->sell_col.p, vl, rr.p, tz.p, S.p, rpart, it, decide, st, worked,
+                    nullptr, nullptr);
+      prof_end(PROF_LEARNED_APPLY, gl_bytes + 8.0 * n);
       worked = prof_begin();
-      if (g16)
+      if (uuni)
+         launch_pdl(lg_upper<bf, int16_t, true>, gq, kRedBlock, nquads, LP->gu->sell_ptr.p,
+                    LP->gu->sell_d16.p, vu, tz.p, zz.p, rr.p, q.p, S.p, cpart, worked,
+                    LP->gu->sell_uni.p, LP->gu->sell_utab.p);
+      else if (g16)
          launch_pdl(lg_upper<bf, int16_t>, gq, kRedBlock, nquads, LP->gu->sell_ptr.p,
-                    LP->gu->sell_d16.p, vu, tz.p, zz.p, rr.p, q.p, S.p, cpart, worked);
+                    LP->gu->sell_d16.p, vu, tz.p, zz.p, rr.p, q.p, S.p, cpart, worked, nullptr,
+                    nullptr);
       else
          launch_pdl(lg_upper<bf, int32_t>, gq, kRedBlock, nquads, LP->gu->sell_ptr.p,
-                    LP->gu->sell_col.p, vu, tz.p, zz.p, rr.p, q.p, S.p, cpart, worked);
-      prof_end(PROF_LEARNED_APPLY, (2.0 + gidx) * LP->gu->nnz + 16.0 * n);
+                    LP->gu->sell_col.p, vu, tz.p, zz.p, rr.p, q.p, S.p, cpart, worked, nullptr,
+                    nullptr);
+      prof_end(PROF_LEARNED_APPLY, gu_bytes + 16.0 * n);
       launch_pdl(lg_direction, gq, kRedBlock, nquads, zz.p, p.p, d.p, upd_d, S.p, cpart, it, fr,
                  fresh);
    };
@@ -641,22 +752,35 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
             // launch: each one's blocks start while the previous one drains
             // its reduction tail
             int* worked = prof_begin();
-            if (bits == 32 && a16)
+            const int32_t* su = A->sell_uni.p;
+            const int16_t* st16 = A->sell_utab.p;
+            if (bits == 32 && auni)
+               launch_pdl(mx_spmv<float, int16_t, true>, gq, kRedBlock, nquads, A->sell_ptr.p,
+                          A->sell_d16.p, A->sell_val32.p, p.p, q.p, S.p, pq, worked, su, st16);
+            else if (bits == 32 && a16)
                launch_pdl(mx_spmv<float, int16_t>, gq, kRedBlock, nquads, A->sell_ptr.p,
-                          A->sell_d16.p, A->sell_val32.p, p.p, q.p, S.p, pq, worked);
+                          A->sell_d16.p, A->sell_val32.p, p.p, q.p, S.p, pq, worked, nullptr,
+                          nullptr);
             else if (bits == 32)
                launch_pdl(mx_spmv<float, int32_t>, gq, kRedBlock, nquads, A->sell_ptr.p,
-                          A->sell_col.p, A->sell_val32.p, p.p, q.p, S.p, pq, worked);
+                          A->sell_col.p, A->sell_val32.p, p.p, q.p, S.p, pq, worked, nullptr,
+                          nullptr);
+            else if (auni)
+               launch_pdl(mx_spmv<__nv_bfloat16, int16_t, true>, gq, kRedBlock, nquads,
+                          A->sell_ptr.p, A->sell_d16.p, v16.p, p.p, q.p, S.p, pq, worked, su,
+                          st16);
             else if (a16)
                launch_pdl(mx_spmv<__nv_bfloat16, int16_t>, gq, kRedBlock, nquads, A->sell_ptr.p,
-                          A->sell_d16.p, v16.p, p.p, q.p, S.p, pq, worked);
+                          A->sell_d16.p, v16.p, p.p, q.p, S.p, pq, worked, nullptr, nullptr);
             else
                launch_pdl(mx_spmv<__nv_bfloat16, int32_t>, gq, kRedBlock, nquads, A->sell_ptr.p,
-                          A->sell_col.p, v16.p, p.p, q.p, S.p, pq, worked);
-            // algorithmic bytes: value (4 or 2) + column index (4, or 2 as a
-            // 16-bit offset) per entry, p gathered, q written, p read for the dot
+                          A->sell_col.p, v16.p, p.p, q.p, S.p, pq, worked, nullptr, nullptr);
+            // algorithmic bytes: value (4 or 2 bytes) and column index (4, 2
+            // as a 16-bit offset, or a uniform slice's table) per entry, p
+            // gathered, q written, p read for the dot
             prof_end(bits == 32 ? PROF_SPMV32 : PROF_SPMV16,
-                     ((bits == 32 ? 4.0 : 2.0) + aidx) * A->nnz + 12.0 * n + 4.0);
+                     (bits == 32 ? 4.0 : 2.0) * A->nnz + index_bytes(A, a16, auni) + 12.0 * n +
+                        4.0);
             if (learned) {
                launch_pdl(mx_update<false>, gq, kRedBlock, nquads, rr.p, q.p, jac, S.p, pq,
                           rpart, cur);

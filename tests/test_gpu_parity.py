@@ -336,6 +336,47 @@ def test_mixed_precision_automatic_value_format(cuda, exact, p2d65):
         assert np.array_equal(auto[0], bf16[0]) and auto[1:4] == bf16[1:4]
 
 
+def test_mixed_precision_uniform_slices_bit_identical(cuda):
+    """Slices whose 32 rows share their column offsets (about 94 % of the
+    entries of the 1025x1025 Laplacian in natural order) are streamed with
+    one offset per slice position and vector gathers.  The same matrix with
+    an explicit zero added to every 16th row (column row + 2) has no uniform
+    slice and takes the per-entry path; adding exact zeros changes no sum,
+    so both solves are bit for bit the same.  The profile's bytes per SpMV
+    show which format each one streamed."""
+    from ofeli_b200 import capi
+    xy, elem, code = O.mesh2d(1024, 1024)
+    dof, n = O.number_equations(code)
+    rp, ci = O.node_graph(elem, 3, dof, n)
+    f = fields.uniform_pm1(17, code.size)
+    a, b = O.assemble(2, xy, elem, dof, code, n, rp, ci, f=f, bc=np.zeros(code.size))
+    rows = np.arange(0, n - 2, 16)
+    cols = rows + 3  # 1-based column row + 2, absent from the 7-point pattern
+    pos = np.array([rp[r] + np.count_nonzero(ci[rp[r]:rp[r + 1]] < c) for r, c in zip(rows, cols)])
+    cnt = np.zeros(n, np.int64)
+    cnt[rows] = 1
+    rp2 = rp + np.concatenate([[0], np.cumsum(cnt)])
+    ci2, a2 = np.insert(ci, pos, cols), np.insert(a, pos, 0.0)
+    out = []
+    for r_, c_, v_ in ((rp, ci, a), (rp2, ci2, a2)):
+        A = F.SpMatrix(r_.astype(np.int64), c_.astype(np.int64), v_)
+        x = np.zeros(n)
+        capi.profile_enable(1)
+        try:
+            res = F.solve_mixed(A, b, x, prec=F.DIAG_PREC, inner_bits=0, toler=1e-10)
+            launches, _, nbytes = capi.profile_read("spmv16")
+        finally:
+            capi.profile_enable(0)
+        out.append((res, x, nbytes / launches, A.nnz))
+    (res1, x1, b1, nnz1), (res2, x2, b2, nnz2) = out
+    assert res1[2] <= 1e-10 and res1 == res2 and np.array_equal(x1, x2)
+    assert nnz2 == nnz1 + rows.size
+    assert b2 == 4.0 * nnz2 + 12.0 * n + 4.0  # BF16 value + 16-bit offset per entry
+    # BF16 values, and index bytes of at most 0.2 per entry: at least 90 % of
+    # the entries take their offset from the slice table
+    assert b1 <= 2.2 * nnz1 + 12.0 * n + 4.0
+
+
 @pytest.mark.parametrize("prec", ["DIAG", "ILU"])
 def test_bicgstab_matches_reference(cuda, prec):
     """BiCGStab on the 65x65 system against OFELI's own run (golden
