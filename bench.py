@@ -487,7 +487,11 @@ def run_ours(args):
     cnt, tot_ms, tot_bytes = prof[fam]
     avg_us = tot_ms / max(cnt, 1) * 1e3
     achieved = (tot_bytes / max(cnt, 1)) / (avg_us * 1e-6) / 1e9 if cnt else None
-    traffic = ncu_traffic("mx_spmv_f32" if bits == 32 else "mx_spmv_bf16")
+    # slices with uniform column offsets stream one offset per slice position
+    # (the bytes per launch fall below value + 16-bit offset per entry)
+    uniform = cnt and tot_bytes / cnt < ((4.0 if bits == 32 else 2.0) + 2.0) * A.nnz + 12.0 * n
+    traffic = ncu_traffic(("mx_spmv_f32" if bits == 32 else "mx_spmv_bf16") +
+                          ("_uniform" if uniform else ""))
     if args.workload != "poisson2d":
         traffic = None  # the committed capture is of the 2-D matrix
     cpu = None
@@ -518,9 +522,10 @@ def run_ours(args):
         "gpu_launches": launches,
         "e2e": {"value": world * args.steps / (e2e_ms / 1e3), "unit": UNIT,
                 "h2d_bytes_per_step": 8 * nn, "d2h_bytes_per_step": 8 * nn},
-        "roofline": {"kernel": "mx_spmv<float> (SELL-32 SpMV inside the FP32 CG)"
-                     if bits == 32 else "mx_spmv<bf16> (SELL-32 SpMV inside the FP32 CG, "
-                     "bf16 values)",
+        "roofline": {"kernel": ("mx_spmv<float> (SELL-32 SpMV inside the FP32 CG"
+                                if bits == 32 else "mx_spmv<bf16> (SELL-32 SpMV inside the FP32 "
+                                "CG, bf16 values") +
+                     (", uniform-slice column offsets)" if uniform else ")"),
                      "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                      "peak_source": peak_kind, "launches_timed": cnt,
