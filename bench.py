@@ -6,7 +6,7 @@ boundary.
 One step = Equation::build() (element assembly into the CSR matrix and RHS
 from the source term resident in HBM) + the solve to an FP64 true relative
 residual ||b - A x|| / ||b|| <= 1e-10 + insertBC.  The chosen solver is the
-learned + mixed-precision one: FP64 refinement around a flexible CG in FP32
+learned + mixed-precision one: FP64 refinement around a preconditioned CG in FP32
 whose preconditioner M = G^T G is predicted by the library's network from the
 assembled matrix inside every step (the network is trained once before the
 timed region, on small problems, by the library's own kernels); `--prec
@@ -515,7 +515,7 @@ def run_ours(args):
         "config": {"workload": "%s (%d unknowns, %d nonzeros), assembly + solve to FP64 "
                                "true rel. residual <= 1e-10" % (workload, n, A.nnz),
                    "solver": "FP64 refinement around FP32 Jacobi-PCG (direction kept)"
-                   if PL is None else "FP64 refinement around FP32 flexible CG with the learned "
+                   if PL is None else "FP64 refinement around FP32 CG with the learned "
                    "preconditioner M = G^T G (network run per assembled matrix, inside the step)",
                    "seed": SEED, "inputs_larger_than_l2": True,
                    "refinements_per_solve": outer, "inner_iterations_per_solve": inner},

@@ -351,9 +351,11 @@ int ofg_learned_gemm_check(ofg_learned* L, int layer, int64_t rows, const uint16
  * after A's values change).  Usable with ofg_cg, ofg_gmres, ofg_prec_apply;
  * the network must outlive it. */
 int ofg_prec_create_learned(ofg_learned* L, ofg_matrix* A, ofg_prec** out);
-/* Flexible CG with the learned preconditioner, in FP32 (inner_bits 32) or
- * with BF16 matrix values (16, or 0 for BF16 only when lossless, as in
- * ofg_solve_mixed), inside FP64 iterative refinement; the
+/* Preconditioned CG with the learned preconditioner M = G^T G (one fixed
+ * linear operator within a solve: beta = rho_k / rho_{k-1}; the name keeps
+ * the "f" of the flexible Polak-Ribiere form it first had), in FP32
+ * (inner_bits 32) or with BF16 matrix values (16, or 0 for BF16 only when
+ * lossless, as in ofg_solve_mixed), inside FP64 iterative refinement; the
  * arguments and results are those of ofg_solve_mixed.  When the learned
  * iteration stagnates (residual not halved in 500 iterations, not finite, or
  * three refinements without a 10% gain) the solve continues with the plain

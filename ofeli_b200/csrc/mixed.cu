@@ -358,9 +358,9 @@ __global__ void __launch_bounds__(kRedBlock, 8) mx_direction(int64_t nquads,
 
 // ---- learned preconditioner M = G^T G inside the FP32 iteration --------
 // G (lower rows) and G^T (upper rows) are SELL-32 matrices on the same
-// slices as A, with BF16 values (the preconditioner's own precision; the
-// flexible CG absorbs it) and 16-bit column offsets where they fit; a
-// thread owns four consecutive rows.
+// slices as A, with BF16 values (the preconditioner's own precision: M is
+// still one fixed symmetric positive definite operator) and 16-bit column
+// offsets where they fit; a thread owns four consecutive rows.
 template <class V, class I, bool UNI>
 __device__ __forceinline__ float4 sell_quad(const int32_t* __restrict__ sp,
                                             const I* __restrict__ scol,
@@ -435,14 +435,13 @@ __global__ void __launch_bounds__(kRedBlock, 8) lg_lower(int64_t nquads, const i
          sell_quad<V, I, UNI>(sp, scol, sval, r, i * 4, suni, stab);
 }
 
-// z = G^T t; (r, z) and (q, z) left as partials for lg_direction
+// z = G^T t; (r, z) left as partials for lg_direction
 template <class V, class I, bool UNI = false>
 __global__ void __launch_bounds__(kRedBlock, 8) lg_upper(int64_t nquads, const int32_t* __restrict__ sp,
                                                       const I* __restrict__ scol,
                                                       const V* __restrict__ sval,
                                                       const float* __restrict__ t, float* z,
-                                                      const float* __restrict__ r,
-                                                      const float* __restrict__ q, const MixState* S,
+                                                      const float* __restrict__ r, const MixState* S,
                                                       double* cpart, int* worked,
                                                       const int32_t* __restrict__ suni = nullptr,
                                                       const int16_t* __restrict__ stab = nullptr)
@@ -451,36 +450,36 @@ __global__ void __launch_bounds__(kRedBlock, 8) lg_upper(int64_t nquads, const i
    pdl_release();
    if (S->pause) return;
    prof_mark(worked);
-   double v[2] = {0.0, 0.0};
+   double v[1] = {0.0};
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nquads; i += stride) {
       const float4 zi = sell_quad<V, I, UNI>(sp, scol, sval, t, i * 4, suni, stab);
       *reinterpret_cast<float4*>(z + i * 4) = zi;
       const float4 ri = *reinterpret_cast<const float4*>(r + i * 4);
-      const float4 qi = *reinterpret_cast<const float4*>(q + i * 4);
       v[0] += (double)ri.x * zi.x + (double)ri.y * zi.y + (double)ri.z * zi.z + (double)ri.w * zi.w;
-      v[1] += (double)qi.x * zi.x + (double)qi.y * zi.y + (double)qi.z * zi.z + (double)qi.w * zi.w;
    }
-   block_partials<2>(v, cpart);
+   block_partials<1>(v, cpart);
 }
 
-// rho_it = (r, z) from lg_upper's partials; beta of the new direction:
-// flexible (Polak-Ribiere) -alpha (z, q) / rho_{it-1}, or rho_it / rho_{it-1}
-// right after a refinement replaced r (fr = 1); then (d += alpha p;)
-// p = z + beta p (p = z on a fresh start)
+// rho_it = (r, z) from lg_upper's partials and beta = rho_it / rho_{it-1};
+// then (d += alpha p;) p = z + beta p (p = z on a fresh start).  M = G^T G
+// is one fixed linear operator within a solve, so the PCG beta applies (the
+// flexible Polak-Ribiere form, -alpha (z, q) / rho_{it-1}, took 4566 instead
+// of 3994 iterations at 2049^2 in FP32); right after a refinement replaced
+// r the same beta keeps the direction.
 __global__ void __launch_bounds__(kRedBlock, 8) lg_direction(int64_t nquads,
                                                           const float* __restrict__ z, float* p,
                                                           float* d, int upd_d, MixState* S,
                                                           const double* __restrict__ cpart, int it,
-                                                          int fr, int fresh)
+                                                          int fresh)
 {
    pdl_wait();
    pdl_release();
    if (S->pause) return;
-   double tot[2];
-   partials_total<2>(cpart, gridDim.x, tot);
+   double tot[1];
+   partials_total<1>(cpart, gridDim.x, tot);
    const double old = S->rho[(it + 1) & 1];
-   const double bd = fr ? tot[0] / old : -S->alpha * tot[1] / old;
+   const double bd = tot[0] / old;
    if (blockIdx.x == 0 && threadIdx.x == 0) {
       S->rho[it & 1] = tot[0];
       S->beta = bd;
@@ -652,8 +651,8 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
    const float* jac = learned ? nullptr : dinv.p;
    const unsigned gq = grid_for(nquads, kRedBlock, 8);
    // per-block partials of the reductions that the next kernel finishes:
-   // (p, q) of the SpMV, ||r||^2 and (r, D r) of the update, (r, z) and
-   // (q, z) of the product with G^T
+   // (p, q) of the SpMV, ||r||^2 and (r, D r) of the update, (r, z) of the
+   // product with G^T
    DBuf<double> red(5 * (size_t)gq + 1);
    double* const pq = red.p;
    double* const rpart = red.p + gq;
@@ -672,8 +671,7 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
    // r, q for the reduction of the second)
    const double gl_bytes = learned ? 2.0 * LP->gl->nnz + index_bytes(LP->gl, g16, luni) : 0.0;
    const double gu_bytes = learned ? 2.0 * LP->gu->nnz + index_bytes(LP->gu, g16, uuni) : 0.0;
-   auto learned_direction = [&](int fr, int fresh, int upd_d, int it, int decide,
-                                const StopRule& st) {
+   auto learned_direction = [&](int fresh, int upd_d, int it, int decide, const StopRule& st) {
       using bf = __nv_bfloat16;
       const bf* vl = reinterpret_cast<const bf*>(learned ? LP->gl->sell_valbf.p : nullptr);
       const bf* vu = reinterpret_cast<const bf*>(learned ? LP->gu->sell_valbf.p : nullptr);
@@ -694,19 +692,18 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
       worked = prof_begin();
       if (uuni)
          launch_pdl(lg_upper<bf, int16_t, true>, gq, kRedBlock, nquads, LP->gu->sell_ptr.p,
-                    LP->gu->sell_d16.p, vu, tz.p, zz.p, rr.p, q.p, S.p, cpart, worked,
+                    LP->gu->sell_d16.p, vu, tz.p, zz.p, rr.p, S.p, cpart, worked,
                     LP->gu->sell_uni.p, LP->gu->sell_utab.p);
       else if (g16)
          launch_pdl(lg_upper<bf, int16_t>, gq, kRedBlock, nquads, LP->gu->sell_ptr.p,
-                    LP->gu->sell_d16.p, vu, tz.p, zz.p, rr.p, q.p, S.p, cpart, worked, nullptr,
+                    LP->gu->sell_d16.p, vu, tz.p, zz.p, rr.p, S.p, cpart, worked, nullptr,
                     nullptr);
       else
          launch_pdl(lg_upper<bf, int32_t>, gq, kRedBlock, nquads, LP->gu->sell_ptr.p,
-                    LP->gu->sell_col.p, vu, tz.p, zz.p, rr.p, q.p, S.p, cpart, worked, nullptr,
+                    LP->gu->sell_col.p, vu, tz.p, zz.p, rr.p, S.p, cpart, worked, nullptr,
                     nullptr);
-      prof_end(PROF_LEARNED_APPLY, gu_bytes + 16.0 * n);
-      launch_pdl(lg_direction, gq, kRedBlock, nquads, zz.p, p.p, d.p, upd_d, S.p, cpart, it, fr,
-                 fresh);
+      prof_end(PROF_LEARNED_APPLY, gu_bytes + 12.0 * n);
+      launch_pdl(lg_direction, gq, kRedBlock, nquads, zz.p, p.p, d.p, upd_d, S.p, cpart, it, fresh);
    };
    MixState h{};
    true_residual(1);
@@ -732,7 +729,7 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
                                                        counter.p);
       count_launch();
       const StopRule st{inner_tol, tol, scale, max_inner, mode};
-      if (learned) learned_direction(fresh ? 0 : 1, fresh ? 1 : 0, 0, h.it, 0, st);
+      if (learned) learned_direction(fresh ? 1 : 0, 0, h.it, 0, st);
       else if (!fresh) {
          mx_direction<<<gq, kRedBlock, 0, stream()>>>(nquads, rr.p, dinv.p, p.p, d.p, 0, S.p, rpart,
                                                       h.it, 0, st);
@@ -784,7 +781,7 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
             if (learned) {
                launch_pdl(mx_update<false>, gq, kRedBlock, nquads, rr.p, q.p, jac, S.p, pq,
                           rpart, cur);
-               learned_direction(0, 0, 1, cur + 1, 1, st);
+               learned_direction(0, 1, cur + 1, 1, st);
             }
             else {
                launch_pdl(mx_update<true>, gq, kRedBlock, nquads, rr.p, q.p, dinv.p, S.p, pq,
@@ -864,8 +861,9 @@ extern "C" int ofg_solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int
    });
 }
 
-// Flexible CG with the learned preconditioner in FP32 inside FP64 iterative
-// refinement (mode 0); falls back to the plain Jacobi iteration when the
+// CG with the learned preconditioner in FP32 inside FP64 iterative
+// refinement (mode 0; the name keeps the "f" of the flexible form it first
+// had); falls back to the plain Jacobi iteration when the
 // learned iteration stagnates (*fell_back = 1).  Convergence is declared on
 // the FP64 true residual only.
 extern "C" int ofg_fcg_learned(ofg_prec* P, int inner_bits, const double* b, double* x,

@@ -541,8 +541,8 @@ class LearnedNet:
 
 def fcg_learned(P, b, x, inner_bits=32, toler=1e-10, max_outer=200, max_inner=1000000,
                 inner_tol=0.05):
-    """Flexible CG with the learned preconditioner in FP32 inside FP64
-    refinement, falling back to the plain Jacobi iteration on stagnation
+    """CG with the learned preconditioner (M = G^T G, one fixed linear
+    operator within a solve) in FP32 inside FP64 refinement, falling back to the plain Jacobi iteration on stagnation
     (inner_bits as in solve_mixed).  Returns (refinement steps, inner iterations, FP64 true relative residual,
     fell_back)."""
     b = _f64(b, P.A.n)

@@ -210,7 +210,7 @@ def test_mixed_precision_on_one_slice(cuda, bits, mode):
 
 
 def test_learned_solve_on_one_slice(cuda):
-    """The learned flexible CG (untrained network: M is Jacobi) on the same
+    """The learned-preconditioner CG (untrained network: M is Jacobi) on the same
     6-unknown system."""
     rp, ci, a, b = small_system(4, 3, seed=8)
     xref, _ = O.cg(rp, ci, a, b, O.DIAG, 1000, 1e-14)

@@ -1,8 +1,8 @@
 """The learned preconditioner on the GPU (ofeli_b200/csrc/learned.cu) against
 its CPU oracle (oracle/learned_oracle.py): initial parameters, the
 tensor-core layer product, loss and gradient of both objectives, training,
-the gain over the method without it (Jacobi), the mixed-precision flexible
-CG and its fallback on stagnation."""
+the gain over the method without it (Jacobi), the mixed-precision CG with
+the learned preconditioner and its fallback on stagnation."""
 import ctypes
 
 import numpy as np
@@ -155,7 +155,7 @@ def test_trained_network_gains_over_jacobi(trained):
     assert rel_err(xl, xd) <= 1e-8
 
 
-def test_flexible_cg_learned_mixed_precision(trained):
+def test_learned_cg_mixed_precision(trained):
     net = trained[0]
     A, b, _ = kuhn_problem(24, 98)
     P = F.Prec(A, F.LEARNED_PREC, net=net)
