@@ -15,9 +15,11 @@
 // A d = r / ||r|| from d = 0 to `inner_tol` and adds ||r|| d.
 //
 // FP64 is used only for b - A x, the refinement update x += ..., and the
-// accumulation of every Krylov dot product.  One FP32 CG iteration streams
-// 8*nnz + 56*n bytes (6*nnz + 56*n with BF16 values) against 12*nnz + 112*n
-// in FP64.
+// accumulation of every Krylov dot product.  One Jacobi-preconditioned
+// FP32 CG iteration streams (v + c)*nnz + 52*n bytes -- v = 4 (FP32) or 2
+// (BF16) value bytes, c = 4 (int32 column), 2 (16-bit offset) or nearly 0
+// (slices with uniform offsets) -- against 12*nnz + 108*n for a fused FP64
+// iteration.
 //
 // The FP32 vectors are padded to the SELL row count (a multiple of 32) with
 // zeros, so every inner kernel moves 16-byte vectors: a thread owns four
