@@ -60,8 +60,10 @@ typedef struct ofg_mesh_file ofg_mesh_file;
 const char* ofg_last_error(void);
 const char* ofg_version(void);
 /* Selects the device of the calling thread and creates its stream
- * (optional: the first call on a device does the same).  No counterpart in
- * OFELI, which has no device. */
+ * (optional: the first call on a device does the same), and loads the code
+ * and the fixed scratch array of ofg_cg_diag_noalloc on that device, so
+ * that its later calls take no device memory.  No counterpart in OFELI,
+ * which has no device. */
 int ofg_init(int device);
 /* Waits for the library's work and frees its process-wide buffers (the mesh
  * reader's pinned staging buffer); handles stay valid. */
@@ -300,8 +302,11 @@ int ofg_residual(const ofg_matrix* A, const double* b, const double* x, double* 
  * inside the library, held by every GPU that loads it until the process
  * exits.  Limit: n <= 131072 rows (larger systems are rejected with
  * OFG_ERR_SIZE).  Calls that overlap on the GPU share that array and race;
- * serialise them.  The first call on a device looks the array up
- * (cudaGetSymbolAddress) and should come before any stream capture. */
+ * serialise them.  CUDA loads device code and arrays lazily, which takes
+ * device memory: call ofg_init(device) for each device before the phase
+ * that must not allocate (and before any stream capture); it loads this
+ * solver's code and places the array.  A zero, missing or NaN diagonal
+ * entry returns OFG_ERR_PIVOT with x unchanged. */
 int ofg_cg_diag_noalloc(int64_t n, const int32_t* row_ptr, const int32_t* col, const double* val,
                         const double* b, double* x, int max_it, double toler, int* result,
                         double* res);

@@ -63,6 +63,8 @@ cudaStream_t stream();
 void meshio_release_staging();
 int num_sms();
 void count_launch(int n = 1);
+// loads the no-allocation solver's code and scratch array on the current device
+void noalloc_prepare();
 
 #define OFG_LAUNCH_CHECK() OFG_CUDA(cudaGetLastError())
 

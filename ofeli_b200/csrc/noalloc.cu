@@ -16,12 +16,18 @@
 // host threads on one device) race and must be serialised by the caller.
 // The array keeps the last call's contents; the parts that must start at
 // zero (the reduction arrival counter) are cleared on every call.
-// The first call on a device looks up the array's device address with
-// cudaGetSymbolAddress (once per device, that device current); make that
-// first call before any stream capture.
+//
+// CUDA loads a library's device code and its __device__ arrays lazily, on
+// first use, and that load takes device memory.  ofg_init(device) therefore
+// does it up front for this file: it looks up the array's address (which
+// places the array on the device) and queries every kernel here (which loads
+// its code), with that device current.  A caller that must not allocate
+// calls ofg_init for each device it uses before that phase begins, and
+// before any stream capture.  Every call looks the address up again (a
+// host-side table lookup once the code is loaded), so a context that was
+// reset and rebuilt gets the array's new address.
 #include <algorithm>
 #include <cmath>
-#include <mutex>
 
 #include "internal.cuh"
 #include "reduce.cuh"
@@ -47,23 +53,13 @@ constexpr size_t kScratchBytes = kStateOff + 256;
 
 __device__ __align__(256) unsigned char g_cg_scratch[kScratchBytes];
 
-unsigned char* g_scratch_addr[64] = {};
-std::mutex g_scratch_mu;
-
-// device address of g_cg_scratch on the current device (host-side, the
-// symbol itself is only a stand-in for the device array)
+// device address of g_cg_scratch on the current device (in host code the
+// symbol is only a stand-in for the device array, never a device address)
 unsigned char* scratch_address()
 {
-   int dev = 0;
-   OFG_CUDA(cudaGetDevice(&dev));
-   OFG_REQUIRE(dev >= 0 && dev < 64, OFG_ERR_ARG, "device index out of range");
-   std::lock_guard<std::mutex> lk(g_scratch_mu);
-   if (!g_scratch_addr[dev]) {
-      void* p = nullptr;
-      OFG_CUDA(cudaGetSymbolAddress(&p, g_cg_scratch));
-      g_scratch_addr[dev] = static_cast<unsigned char*>(p);
-   }
-   return g_scratch_addr[dev];
+   void* p = nullptr;
+   OFG_CUDA(cudaGetSymbolAddress(&p, g_cg_scratch));
+   return static_cast<unsigned char*>(p);
 }
 
 // 8 lanes per row on CSR; lane 0 of each group owns the row's result
@@ -100,7 +96,7 @@ __global__ void __launch_bounds__(kRedBlock) na_init(int64_t n, const int32_t* r
       double d = 0.0;
       for (int32_t k = rp[row]; k < rp[row + 1]; ++k)
          if (col[k] == (int32_t)row) d = val[k];
-      if (d == 0.0) bad = 1;
+      if (!(fabs(d) > 0.0)) bad = 1;  // zero, missing or NaN
       const double di = 1.0 / d, bi = b[row], ri = bi - ax;
       dinv[row] = di;
       r[row] = ri;
@@ -189,6 +185,19 @@ __global__ void __launch_bounds__(kRedBlock) na_update(int64_t n, double* x, con
 }
 
 }  // namespace
+
+// Loads this file's device code and places g_cg_scratch on the current
+// device, so that later calls of ofg_cg_diag_noalloc take no device memory.
+void noalloc_prepare()
+{
+   scratch_address();
+   cudaFuncAttributes fa;
+   OFG_CUDA(cudaFuncGetAttributes(&fa, na_init));
+   OFG_CUDA(cudaFuncGetAttributes(&fa, na_direction));
+   OFG_CUDA(cudaFuncGetAttributes(&fa, na_spmv));
+   OFG_CUDA(cudaFuncGetAttributes(&fa, na_update));
+}
+
 }  // namespace ofg
 
 using namespace ofg;

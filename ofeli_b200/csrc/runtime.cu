@@ -195,6 +195,7 @@ int ofg_init(int device)
       OFG_REQUIRE(device >= 0, OFG_ERR_ARG, "device must be >= 0");
       OFG_CUDA(cudaSetDevice(device));
       OFG_CUDA(cudaStreamSynchronize(ofg::stream()));
+      ofg::noalloc_prepare();
    });
 }
 

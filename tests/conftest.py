@@ -9,6 +9,9 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 GOLDEN = os.path.join(ROOT, "tests", "golden")
+# the reference OFELI sources, read only by the tests that compare against its
+# shipped mesh files (skipped where the sources are absent)
+REFERENCE = os.environ.get("OFELI_REFERENCE", "/root/reference")
 
 
 def pytest_configure(config):

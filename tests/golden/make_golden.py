@@ -269,9 +269,86 @@ def case_meshio():
     save("meshio", arrays, meta)
 
 
+def _sample_pins(x, stride):
+    return {"x_norm2": float(np.linalg.norm(x)), "x_sum": float(x.sum()),
+            "x_sample_stride": stride}, {"x_sample": x[::stride].copy()}
+
+
+def pins_p2d_2049():
+    """The benchmark's 2-D problem at full size (2049x2049 nodes, f seed
+    1234, u = 0 on the boundary): OFELI's CG + ILU to 1e-10, run to
+    convergence (about 11 minutes of one core at -O2)."""
+    nx = 2048
+    f = fields.uniform_pm1(1234, (nx + 1) ** 2)
+    info, out = O.run_reference(["p2d", nx, nx, "CG", "ILU", 1e-10, 100000], {"f": f})
+    meta, arrays = _sample_pins(out["x"], 4096)
+    meta.update(nx=nx, seed_f=1234, solver="CG", prec="ILU", tol=1e-10, iters=info["iters"],
+                n=info["n"], nnz=info["nnz"], norm_u=info["norm_u"],
+                t_solve_cpu_o2_s=info["t_solve"], t_assembly_cpu_o2_s=info["t_assembly"],
+                t_graph_cpu_o2_s=info["t_graph"])
+    save("p2d_2049_pins", arrays, meta)
+
+
+def pins_p3d_129():
+    """The benchmark's 3-D problem at full size (Kuhn cube 129^3 nodes,
+    12.6M tetrahedra; k = exp(g), g the seeded Gaussian field of sigma 1.5
+    and correlation length 0.1 synthesised on a 256^3 lattice, seed 1234;
+    f seed 1234; u = 0 on the faces): OFELI's CG + ILU and CG + DIAG to
+    1e-10, run to convergence."""
+    M = 128
+    xyz, elem, code = O.mesh3d(M)
+    k = fields.lognormal_k(1234, centroids(xyz, elem, 3), 1.5, 0.1, grid=256)
+    f = fields.uniform_pm1(1234, code.size)
+    del xyz, elem
+    meta = {"M": M, "seed_k": 1234, "seed_f": 1234, "sigma": 1.5, "corr": 0.1, "grid": 256,
+            "tol": 1e-10, "runs": {}}
+    arrays = {}
+    for prec in ("ILU", "DIAG"):
+        info, out = O.run_reference(["p3d", M, "CG", prec, 1e-10, 100000], {"f": f, "k": k})
+        m, a = _sample_pins(out["x"], 2048)
+        m.update(iters=info["iters"], norm_u=info["norm_u"], t_solve_cpu_o2_s=info["t_solve"],
+                 t_assembly_cpu_o2_s=info["t_assembly"], t_graph_cpu_o2_s=info["t_graph"])
+        meta["runs"][prec] = m
+        arrays["x_sample_" + prec] = a["x_sample"]
+        meta["n"], meta["nnz"] = info["n"], info["nnz"]
+        del out
+    save("p3d_129_pins", arrays, meta)
+
+
+def pins_cd2d_1025():
+    """The benchmark's transient problem at full size (DC2DT3 on 1025x1025
+    nodes, eps 1e-3, v = (-(y-0.5), x-0.5), Gaussian bump at (0.3, 0.5) of
+    width 0.05, u = 0 on the boundary, backward Euler dt 1e-3): the first
+    three steps with OFELI's GMRES(30) + ILU, warm-started, to 1e-10."""
+    nx, steps, dt, eps = 1024, 3, 1e-3, 1e-3
+    xy, elem, code = O.mesh2d(nx, nx)
+    P = xy.reshape(-1, 2)
+    u0 = np.exp(-((P[:, 0] - 0.3) ** 2 + (P[:, 1] - 0.5) ** 2) / (2 * 0.05 ** 2))
+    u0[code > 0] = 0.0
+    v = np.stack([-(P[:, 1] - 0.5), P[:, 0] - 0.5], axis=1).reshape(-1)
+    info, out = O.run_reference(["cd2d", nx, nx, steps, dt, eps, "GMRES30", "ILU", 1e-10, 2000],
+                                {"u0": u0, "v": v})
+    meta, arrays = _sample_pins(out["x"], 1024)
+    meta.update(nx=nx, steps=steps, dt=dt, eps=eps, tol=1e-10, m=30, n=info["n"],
+                nnz=info["nnz"], iters=[int(i) for i in out["iters"]],
+                u_norm2=float(np.linalg.norm(out["u"])), t_graph_cpu_o2_s=info["t_graph"],
+                t_assembly_cpu_o2_s=info["t_assembly"], t_prec_cpu_o2_s=info["t_prec"],
+                t_solve_cpu_o2_s=info["t_solve"])
+    save("cd2d_1025_pins", arrays, meta)
+
+
+FULLSIZE = {"p2d_2049": pins_p2d_2049, "p3d_129": pins_p3d_129, "cd2d_1025": pins_cd2d_1025}
+
+
 if __name__ == "__main__":
     if not O.have_reference("o2"):
         raise SystemExit("build the reference first: make -C oracle ref")
+    if len(sys.argv) > 1:
+        # full-size pins, each minutes to tens of minutes of one core:
+        #   python tests/golden/make_golden.py p3d_129 cd2d_1025 [p2d_2049]
+        for name in sys.argv[1:]:
+            FULLSIZE[name]()
+        raise SystemExit(0)
     case_p2d_65()
     case_p2d_jitter()
     case_p2d_ragged()

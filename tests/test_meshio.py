@@ -14,15 +14,15 @@ import tempfile
 import numpy as np
 import pytest
 
-from conftest import GOLDEN, load_golden
+from conftest import GOLDEN, REFERENCE, load_golden
 from ofeli_b200 import ofeli as F
 from ofeli_b200 import problems
 from oracle import mesh_oracle as MO
 from oracle import oracle as O
 
 FILES = ("ring", "codes", "tet")
-REF_DEMOS = sorted(glob.glob("/root/reference/demos/**/*.m", recursive=True)
-                   + ["/root/reference/util/cmesh/disk.m"])
+REF_DEMOS = sorted(glob.glob(os.path.join(REFERENCE, "demos/**/*.m"), recursive=True)
+                   + glob.glob(os.path.join(REFERENCE, "util/cmesh/disk.m")))
 
 
 @pytest.fixture(scope="module")
@@ -87,9 +87,9 @@ def test_codes_quirks(golden):
 
 
 @pytest.mark.skipif(not (REF_DEMOS and O.have_reference("o2") and
-                         os.path.isdir("/root/reference/demos")),
+                         os.path.isdir(os.path.join(REFERENCE, "demos"))),
                     reason="needs the reference sources and oracle/_ref")
-@pytest.mark.parametrize("path", REF_DEMOS, ids=lambda p: os.path.relpath(p, "/root/reference"))
+@pytest.mark.parametrize("path", REF_DEMOS, ids=lambda p: os.path.relpath(p, REFERENCE))
 def test_reference_demo_meshes(path):
     """Every mesh file the reference ships: Mesh::get's arrays and Mesh::put's
     bytes (harness run here) against the library and the oracle."""
