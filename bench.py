@@ -49,6 +49,11 @@ TOL = 1e-10
 # many iterations (run to convergence with the reference built from its
 # sources, tol 1e-10); used to extrapolate the bounded CPU samples.
 REF_ITERS_2049_ILU = 2030
+# the same for the 3-D problem (Kuhn cube 129^3, lognormal k, seed 1234):
+# 257 CG + ILU iterations; OFELI's own times at -O2 on one core of the
+# container that ran it (graph, assembly, solve)
+REF_ITERS_129_ILU = 257
+REF_TIMES_129_ILU = {"graph_s": 43.9, "assembly_s": 9.13, "solve_s": 56.2}
 
 
 def parse():
@@ -74,9 +79,14 @@ def parse():
                          "cost (strong scaling) instead of one replica of it per rank")
     ap.add_argument("--batch-bits", type=int, default=32, choices=[32, 64],
                     help="batch2d: inner CG precision (32: FP32 CG inside FP64 refinement)")
-    ap.add_argument("--tprec", default="DIAG", choices=["ILU", "DIAG"],
-                    help="transient2d: GMRES(30) preconditioner of the timed steps (the plain "
-                         "ILU form is timed beside it)")
+    ap.add_argument("--tprec", default="LEARNED", choices=["ILU", "DIAG", "MIXED", "LEARNED"],
+                    help="transient2d: solver of the timed steps -- ILU / DIAG: FP64 GMRES(30) "
+                         "(OFELI's GMRes) with that preconditioner; MIXED / LEARNED: the "
+                         "mixed-precision flexible GMRES(30) (FP32 products, FP64 Gram-Schmidt "
+                         "and refinement, converged on the FP64 true residual) with the diagonal "
+                         "or the learned preconditioner (the plain ILU form is timed beside it)")
+    ap.add_argument("--t-inner-tol", type=float, default=1e-5,
+                    help="transient2d MIXED / LEARNED: residual reduction of one FGMRES cycle")
     ap.add_argument("--m3d", type=int, default=128, help="kuhn3d cells per side")
     ap.add_argument("--mf-n", type=int, default=1024,
                     help="meshfile2d: circles and nodes per circle of the annulus (the workload "
@@ -89,6 +99,8 @@ def parse():
                          "trained first on small problems of the workload's dimension, outside "
                          "the timed region, and runs inside every step)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 CG+D-ILU solve")
+    ap.add_argument("--no-3d", action="store_true",
+                    help="poisson2d: skip the 3-D problem the default run also measures")
     ap.add_argument("--cpu-iters", type=int, default=10, help="CG iterations per CPU sample")
     return ap.parse_args()
 
@@ -272,26 +284,18 @@ def run_reference(args):
 
 
 # --------------------------------------------------------------- our arm ----
-def run_ours(args):
+def measure(args, wl, R, work_stream, dev, world, rank, with_cpu=True):
+    """One workload (poisson2d or kuhn3d) through the chosen solver: warm-up,
+    the timed device-resident steps, the kernel profile, the end-to-end
+    steps, the plain FP64 CG + D-ILU solve and the error against it.
+    Returns the JSON line (rank 0) or None."""
     import torch
     from ofeli_b200 import capi, fields
     from ofeli_b200 import ofeli as F
-
-    from ofeli_b200 import ranks
-    world, rank, local = ranks.env()
-    if not torch.cuda.is_available():
-        raise SystemExit("bench.py needs a CUDA device")
-    torch.cuda.set_device(local)
-    R = ranks.Ranks("nccl", torch.device("cuda", local))
-    L = capi.lib()
-    # one stream for torch and the library: ordering without extra syncs
-    work_stream = torch.cuda.Stream(device=torch.device("cuda", local))
-    torch.cuda.set_stream(work_stream)
-    capi.call("ofg_set_stream", ctypes.c_void_p(work_stream.cuda_stream))
+    local = dev.index
     nx = args.nx
-    dev = torch.device("cuda", local)
     k_dev = None
-    if args.workload == "kuhn3d":
+    if wl == "kuhn3d":
         M = args.m3d
         mesh = F.Mesh.kuhn(M)
         coords, elem, _, _ = mesh.arrays()
@@ -317,7 +321,7 @@ def run_ours(args):
     PL, train_info, fell_back = None, None, []
     if args.prec == "learned":
         from ofeli_b200 import learned as LN
-        net, train_info = LN.train_default(dim=3 if args.workload == "kuhn3d" else 2)
+        net, train_info = LN.train_default(dim=3 if wl == "kuhn3d" else 2)
         capi.call("ofg_assemble_p1", mesh._h, A._h, P(k_dev), P(f_dev), None, P(b_dev))
         PL = F.Prec(A, F.LEARNED_PREC, net=net)
 
@@ -443,9 +447,10 @@ def run_ours(args):
     u_ref = u_dev.cpu().numpy()
     if not np.allclose(u_pin.numpy(), u_ref, rtol=0, atol=1e-12 * np.abs(u_ref).max()):
         raise SystemExit("end-to-end result differs from the device-resident one")
+    x_chosen = x_dev.cpu().numpy()
 
     # ------------------------------------------------ plain FP64 CG + D-ILU
-    plain = None
+    plain, err_vs_fp64 = None, None
     if not args.no_plain and rank == 0:
         capi.call("ofg_assemble_p1", mesh._h, A._h, P(k_dev), P(f_dev), None, P(b_dev))
         Pc = F.Prec(A, F.ILU_PREC)
@@ -458,6 +463,11 @@ def run_ours(args):
         plain = {"solver": "CG + ILU (OFELI's diagonal ILU), FP64, natural order",
                  "iterations": it, "solve_s": t_plain,
                  "true_rel_residual": F.residual(A, b_dev, x_dev)}
+        x_plain = x_dev.cpu().numpy()
+        err_vs_fp64 = {"value": float(np.linalg.norm(x_chosen - x_plain) /
+                                      np.linalg.norm(x_plain)),
+                       "what": "||x - x_fp64|| / ||x_fp64||, x_fp64 = the plain FP64 CG + ILU "
+                               "solution (true rel. residual <= 1e-10)"}
         del Pc
     # SpMV FP64 bandwidth (the plain path's kernel), live CUDA events
     xs = torch.rand(n, dtype=torch.float64, device=dev)
@@ -477,8 +487,7 @@ def run_ours(args):
     spmv64_bytes = 12.0 * A.nnz + 20.0 * n + 4.0
 
     if rank != 0:
-        R.close()
-        return 0
+        return None
 
     peak, peak_kind = measured_peaks()
     # the value format the solves streamed (inner_bits 0 decides per matrix)
@@ -492,18 +501,21 @@ def run_ours(args):
     uniform = cnt and tot_bytes / cnt < ((4.0 if bits == 32 else 2.0) + 2.0) * A.nnz + 12.0 * n
     traffic = ncu_traffic(("mx_spmv_f32" if bits == 32 else "mx_spmv_bf16") +
                           ("_uniform" if uniform else ""))
-    if args.workload != "poisson2d":
+    if wl != "poisson2d":
         traffic = None  # the committed capture is of the 2-D matrix
     cpu = None
-    if world == 1 and args.workload == "poisson2d":
+    if world == 1 and wl == "poisson2d":
         cpu = cpu_baseline_port(nx, args.cpu_iters)
-    elif world == 1 and plain:
-        cpu = cpu_baseline_port3d(args.m3d, args.cpu_iters, plain["iterations"])
+    elif world == 1 and plain and with_cpu:
+        # extrapolated to the iteration count OFELI itself needs on this
+        # problem (run to convergence with the reference, committed pin)
+        cpu = cpu_baseline_port3d(args.m3d, args.cpu_iters,
+                                  REF_ITERS_129_ILU if args.m3d == 128 else plain["iterations"])
     outer = sum(s[0] for s in stats) / len(stats)
     inner = sum(s[1] for s in stats) / len(stats)
     value = world * args.steps / (ms / 1e3)
     line = {
-        "metric": METRIC if args.workload == "poisson2d" else METRIC_3D, "value": value,
+        "metric": METRIC if wl == "poisson2d" else METRIC_3D, "value": value,
         "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
@@ -533,6 +545,7 @@ def run_ours(args):
                      "bytes_per_launch": tot_bytes / max(cnt, 1)},
         "spmv_fp64": {"us": spmv64_us, "GB/s": spmv64_bytes / (spmv64_us * 1e-6) / 1e9,
                       "frac_of_peak": spmv64_bytes / (spmv64_us * 1e-6) / 1e9 / peak},
+        "err_vs_fp64": err_vs_fp64,
         "plain": plain,
         "learned": learned,
         "cpu_baseline": cpu,
@@ -540,7 +553,50 @@ def run_ours(args):
     }
     if plain:
         line["plain"]["solves_per_s"] = 1.0 / plain["solve_s"]
-    print(json.dumps(line))
+    return line
+
+
+def run_ours(args):
+    import torch
+    from ofeli_b200 import capi, fields
+    from ofeli_b200 import ofeli as F
+
+    from ofeli_b200 import ranks
+    world, rank, local = ranks.env()
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    torch.cuda.set_device(local)
+    R = ranks.Ranks("nccl", torch.device("cuda", local))
+    L = capi.lib()
+    # one stream for torch and the library: ordering without extra syncs
+    work_stream = torch.cuda.Stream(device=torch.device("cuda", local))
+    torch.cuda.set_stream(work_stream)
+    capi.call("ofg_set_stream", ctypes.c_void_p(work_stream.cuda_stream))
+    dev = torch.device("cuda", local)
+    line = measure(args, args.workload, R, work_stream, dev, world, rank)
+    if args.workload == "poisson2d" and not args.no_3d:
+        # the 3-D variable-coefficient problem, in the same run: the chosen
+        # form against the plain GPU CG + ILU, and its error against FP64
+        import gc
+        gc.collect()
+        torch.cuda.empty_cache()
+        l3 = measure(args, "kuhn3d", R, work_stream, dev, world, rank, with_cpu=False)
+        if line is not None:
+            pl = l3["plain"] or {}
+            line["kuhn3d"] = {
+                "workload": l3["config"]["workload"], "metric": l3["metric"],
+                "value": l3["value"], "unit": l3["unit"], "ms_per_step": l3["ms_per_step"],
+                "e2e": l3["e2e"], "solver": l3["config"]["solver"],
+                "inner_iterations_per_solve": l3["config"]["inner_iterations_per_solve"],
+                "refinements_per_solve": l3["config"]["refinements_per_solve"],
+                "plain_ilu_cg": pl, "ofeli_ilu_cg_iterations": REF_ITERS_129_ILU,
+                "ofeli_o2_measured_s": REF_TIMES_129_ILU,
+                "ratio_vs_plain_gpu": (pl["solve_s"] * 1e3 / l3["ms_per_step"]) if pl else None,
+                "err_vs_fp64": l3["err_vs_fp64"], "roofline": l3["roofline"],
+                "gpu_launches": l3["gpu_launches"], "learned": l3["learned"],
+                "clocks": l3["clocks"]}
+    if line is not None:
+        print(json.dumps(line))
     R.close()
     return 0
 
@@ -844,21 +900,44 @@ def run_transient(args):
     u0, v = transient_fields(xy, code)
     A = F.SpMatrix(mesh)
     n, nn = A.n, mesh.nn
-    prec = F.ILU_PREC if args.tprec == "ILU" else F.DIAG_PREC
+    mixed = args.tprec in ("MIXED", "LEARNED")
+    prec = {"ILU": F.ILU_PREC, "DIAG": F.DIAG_PREC, "MIXED": F.DIAG_PREC,
+            "LEARNED": F.LEARNED_PREC}[args.tprec]
+    net, train_info = None, None
+    if args.tprec == "LEARNED":
+        # trained before the timed region on smaller convection-diffusion
+        # matrices with the workload's proportions (the library's kernels)
+        from ofeli_b200 import learned as LN
+        net, train_info = LN.train_transient()
     u_dev = torch.from_numpy(u0).to(dev)
     v_dev = torch.from_numpy(v).to(dev)
     b_dev = torch.zeros(n, dtype=torch.float64, device=dev)
     x_dev = torch.zeros(n, dtype=torch.float64, device=dev)
     Pc = None
     its = []
+    cycles = []
+    true_res = []
 
     def step(u_in, u_out):
         nonlocal Pc
         capi.call("ofg_assemble_cd2d", mesh._h, A._h, T_EPS, P_(v_dev), T_DT, P_(u_in), None,
                   P_(b_dev))
         if Pc is None:
-            Pc = F.Prec(A, prec)
-        it = F.GMRes(A, Pc, b_dev, x_dev, T_M, 2000, T_TOL)  # refactorises: values changed
+            Pc = F.Prec(A, prec, net=net)
+            if prec == F.LEARNED_PREC:
+                # the matrix is the same at every step: the factor is computed
+                # once, on the first step's matrix, and kept
+                Pc.freeze()
+        if mixed:
+            o, it, res, fb = F.fgmres_mixed(Pc, b_dev, x_dev, m=T_M, toler=T_TOL,
+                                            inner_tol=args.t_inner_tol)
+            if res > T_TOL or fb:
+                raise SystemExit("a mixed FGMRES step missed the target: res %.3g fell_back %s"
+                                 % (res, fb))
+            cycles.append(o)
+            true_res.append(res)
+        else:
+            it = F.GMRes(A, Pc, b_dev, x_dev, T_M, 2000, T_TOL)  # refactorises: values changed
         capi.call("ofg_insert_bc", mesh._h, P_(x_dev), None, P_(u_out))
         its.append(it)
         return it
@@ -890,13 +969,16 @@ def run_transient(args):
         raise SystemExit("a GMRES solve did not converge: %s" % its)
     res = F.residual(A, b_dev, x_dev)
     timed_its = list(its)
+    timed_cycles = list(cycles)
     # kernel families timed with CUDA events over two more steps (every 2nd
     # launch), kept out of the timed steps
     capi.profile_enable(2)
     for _ in range(2):
         step(u_dev, u_dev)
     torch.cuda.synchronize()
-    prof = {k: capi.profile_read(k) for k in ("sweep", "spmv64", "assembly")}
+    families = ("sweep", "spmv64", "spmv32", "spmv16", "learned_apply", "gram_schmidt",
+                "assembly")
+    prof = {k: capi.profile_read(k) for k in families}
     capi.profile_enable(0)
 
     # end to end: the state u lives on the host (pinned) and goes up and
@@ -913,11 +995,24 @@ def run_transient(args):
     g1.record(work_stream)
     torch.cuda.synchronize()
     e2e_ms = R.max(max(g0.elapsed_time(g1), (time.perf_counter() - t0) * 1e3))
+    # the error of the timed form against the FP64 steps of OFELI's method:
+    # 11 steps of each from the same initial state
+    def trajectory(nsteps):
+        u_dev.copy_(torch.from_numpy(u0).to(dev))
+        x_dev.zero_()
+        for _ in range(nsteps):
+            step(u_dev, u_dev)
+        torch.cuda.synchronize()
+        return u_dev.cpu().numpy()
+
+    u_timed = trajectory(11) if rank == 0 and not args.no_plain else None
     # the plain form (OFELI's GMRES(30) + ILU) over 10 steps from the same
-    # initial state
-    plain = None
-    if rank == 0 and not args.no_plain and args.tprec != "ILU":
-        prec, Pc = F.ILU_PREC, None
+    # initial state, and FP64 GMRES(30) + DIAG likewise
+    plain, fp64_diag, err = None, None, None
+
+    def time_fp64(p):
+        nonlocal prec, Pc, mixed
+        prec, Pc, mixed = p, None, False
         u_dev.copy_(torch.from_numpy(u0).to(dev))
         x_dev.zero_()
         del its[:]
@@ -928,20 +1023,43 @@ def run_transient(args):
             step(u_dev, u_dev)
         torch.cuda.synchronize()
         t_pl = (time.perf_counter() - t0) / 10
-        plain = {"solver": "GMRES(30) + ILU (OFELI's diagonal ILU), FP64, warm start",
-                 "ms_per_step": t_pl * 1e3, "steps_per_s": 1.0 / t_pl,
-                 "gmres_iterations_per_step": statistics.mean(its[1:]),
-                 "true_rel_residual": F.residual(A, b_dev, x_dev)}
+        return {"ms_per_step": t_pl * 1e3, "steps_per_s": 1.0 / t_pl,
+                "gmres_iterations_per_step": statistics.mean(its[1:]),
+                "true_rel_residual": F.residual(A, b_dev, x_dev)}, u_dev.cpu().numpy()
+
+    if rank == 0 and not args.no_plain:
+        if args.tprec != "ILU":
+            plain, u_ilu = time_fp64(F.ILU_PREC)
+            plain["solver"] = "GMRES(30) + ILU (OFELI's diagonal ILU), FP64, warm start"
+            err = float(np.linalg.norm(u_timed - u_ilu) / np.linalg.norm(u_ilu))
+        if args.tprec != "DIAG":
+            fp64_diag, _ = time_fp64(F.DIAG_PREC)
+            fp64_diag["solver"] = "GMRES(30) + DIAG, FP64, warm start (OFELI's GMRes order)"
     if rank != 0:
         R.close()
         return 0
     cpu = cpu_baseline_transient() if world == 1 else None
     peak, peak_kind = measured_peaks()
-    fam = max(("sweep", "spmv64"), key=lambda k: prof[k][1])
+    fam = max((k for k in families if k != "assembly"), key=lambda k: prof[k][1])
     cnt, tot_ms, tot_bytes = prof[fam]
     avg_us = tot_ms / max(cnt, 1) * 1e3
     achieved = (tot_bytes / max(cnt, 1)) / (avg_us * 1e-6) / 1e9 if cnt else None
-    shares = {k: round(prof[k][1], 3) for k in prof}
+    shares = {k: round(prof[k][1], 3) for k in prof if prof[k][0]}
+    kernel_names = {"sweep": "solve_sweep (D-ILU triangular sweeps)",
+                    "spmv64": "spmv_sell_kernel (FP64 SELL-32 SpMV)",
+                    "spmv32": "fg_product (FP32 SELL-32 product with A)",
+                    "spmv16": "fg_product (BF16-value SELL-32 product with A)",
+                    "learned_apply": "fg_product (products with G and G^T, BF16 values)",
+                    "gram_schmidt": "fg_dots / fg_orth1 / fg_orth2 (FP64 classical "
+                                    "Gram-Schmidt, twice)"}
+    solver = {"ILU": "FP64 GMRES(30) + ILU (OFELI's GMRes, left preconditioned, MGS)",
+              "DIAG": "FP64 GMRES(30) + DIAG (OFELI's GMRes, left preconditioned, MGS)",
+              "MIXED": "mixed-precision flexible GMRES(30) + DIAG: FP32 products, FP64 CGS2 "
+                       "and refinement, converged on the FP64 true residual",
+              "LEARNED": "mixed-precision flexible GMRES(30) + learned M = G^T G (factor "
+                         "computed on the first step's matrix and kept): FP32 products, BF16 "
+                         "factor values, FP64 CGS2 and refinement, converged on the FP64 true "
+                         "residual"}[args.tprec]
     line = {
         "metric": METRIC_TRANSIENT, "value": world * args.steps / (ms / 1e3), "unit": "steps/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -952,20 +1070,27 @@ def run_transient(args):
                                "bump (0.3, 0.5) width 0.05, u = 0 on the boundary, backward Euler "
                                "dt 1e-3; per step build() + Prec + GMRES(30) warm-started to "
                                "OFELI's preconditioned residual 1e-10 + insertBC" % (n, A.nnz),
-                   "preconditioner": args.tprec,
+                   "preconditioner": args.tprec, "solver": solver,
                    "gmres_iterations_per_step": statistics.mean(timed_its),
+                   "refinement_cycles_per_step": (statistics.mean(timed_cycles)
+                                                  if timed_cycles else None),
+                   "inner_tol": args.t_inner_tol if mixed else None,
                    "last_true_rel_residual": res, "inputs_larger_than_l2": True},
+        "err_vs_fp64": {"value": err, "what": "||u - u_ref|| / ||u_ref|| after 11 steps from u0, "
+                                              "u_ref = FP64 GMRES(30) + ILU (OFELI's method)"}
+        if err is not None else None,
+        "learned": train_info,
         "gpu_launches": launches,
         "e2e": {"value": world * args.steps / (e2e_ms / 1e3), "unit": "steps/s",
                 "h2d_bytes_per_step": 8 * nn, "d2h_bytes_per_step": 8 * nn},
-        "roofline": {"kernel": "solve_sweep (D-ILU triangular sweeps)" if fam == "sweep"
-                     else "spmv_sell_kernel (FP64 SELL-32 SpMV)",
+        "roofline": {"kernel": kernel_names[fam],
                      "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if achieved else None, "traffic": None,
                      "peak_source": peak_kind, "launches_timed": cnt, "avg_launch_us": avg_us,
                      "bytes_per_launch": tot_bytes / max(cnt, 1),
                      "family_ms_sampled": shares},
         "plain": plain,
+        "fp64_gmres_diag": fp64_diag,
         "cpu_baseline": cpu,
         "clocks": clk,
     }

@@ -243,6 +243,12 @@ int ofg_prec_create(ofg_matrix* A, int type, ofg_prec** out);
 int ofg_prec_destroy(ofg_prec* P);
 /* Recompute the factorisation after the values of A changed. */
 int ofg_prec_update(ofg_prec* P);
+/* on != 0: the solvers keep P as it was set up even after the values of
+ * its matrix changed (no refresh; ofg_prec_update still refreshes), e.g. a
+ * learned factor computed once for a time-stepping scheme whose matrix is
+ * the same at every step.  No counterpart in OFELI, whose Prec refactorises
+ * when it is rebuilt. */
+int ofg_prec_freeze(ofg_prec* P, int on);
 /* Prec::solve(b, x) (Prec_impl.h:227-255). */
 int ofg_prec_apply(ofg_prec* P, const double* b, double* x);
 /* Prec::getPivot for all rows (inverse pivots for DIAG/DILU/ILU). */
@@ -369,6 +375,25 @@ int ofg_prec_create_learned(ofg_learned* L, ofg_matrix* A, ofg_prec** out);
 int ofg_fcg_learned(ofg_prec* P, int inner_bits, const double* b, double* x, int max_outer,
                     int max_inner, double inner_tol, double toler, int* outer, int* inner,
                     double* true_res, int* fell_back);
+
+/* Flexible GMRES(m), right preconditioned, in mixed precision inside FP64
+ * iterative refinement: the chosen form for nonsymmetric systems (the
+ * transient convection-diffusion steps).  Replaces GMRes(A, P, b, x, m,
+ * max_it, toler) (include/solvers/GMRes.h:148-241), which is FP64, left
+ * preconditioned, with modified Gram-Schmidt.  Per Arnoldi step: z_j =
+ * M^{-1} v_j in FP32 (P: DIAG, IDENT, or LEARNED with BF16 factor values),
+ * the product A z_j in FP32 (FP32 values, or BF16 values per inner_bits as
+ * in ofg_solve_mixed), classical Gram-Schmidt applied twice in FP64, Givens
+ * rotations; a cycle stops when its residual estimate fell by inner_tol,
+ * predicts the target, or after m steps (1 <= m <= 64).  x (initial guess
+ * in, solution out) += Z y.  Converged only when the FP64 true relative
+ * residual ||b - A x|| / ||b|| <= toler.  *outer = cycles, *inner = Arnoldi
+ * steps, *true_res = final FP64 relative residual; with LEARNED, when two
+ * cycles in a row fail to halve the residual (or it is not finite) the
+ * remaining cycles use the diagonal preconditioner and *fell_back = 1. */
+int ofg_fgmres_mixed(ofg_prec* P, int inner_bits, const double* b, double* x, int m,
+                     int max_outer, int max_inner, double inner_tol, double toler, int* outer,
+                     int* inner, double* true_res, int* fell_back);
 
 /* ------------------------------------------------------ batched problems --
  * No counterpart in OFELI (its equivalent is a loop of build() + CG per

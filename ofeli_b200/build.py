@@ -14,7 +14,7 @@ CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libofeli_gpu.so")
 SOURCES = ["runtime.cu", "matrix.cu", "mesh.cu", "assembly.cu", "prec.cu", "krylov.cu", "mixed.cu",
-           "noalloc.cu", "learned.cu", "batch.cu", "bicgstab.cu",
+           "noalloc.cu", "learned.cu", "batch.cu", "bicgstab.cu", "fgmres.cu",
            "meshio.cu", "entries.cu"]
 # per-source flags: the element arithmetic is kept free of fused multiply-adds
 # so that assembled values round exactly as OFELI's (separate multiply and add)

@@ -99,6 +99,9 @@ SIGNATURES = {
     "ofg_learned_gemm_check": (_i32, [_p, _i32, _i64, _p, _p, _p]),
     "ofg_prec_create_learned": (_i32, [_p, _p, _pp]),
     "ofg_fcg_learned": (_i32, [_p, _i32, _p, _p, _i32, _i32, _d, _d, _pi32, _pi32, _pd, _pi32]),
+    "ofg_fgmres_mixed": (_i32, [_p, _i32, _p, _p, _i32, _i32, _i32, _d, _d, _pi32, _pi32, _pd,
+                                _pi32]),
+    "ofg_prec_freeze": (_i32, [_p, _i32]),
     "ofg_batch_create": (_i32, [_i32, _p, _pp]),
     "ofg_batch_destroy": (_i32, [_p]),
     "ofg_batch_info": (_i32, [_p, _pi32, _pi64, _pi64, _pi64, _pi64]),

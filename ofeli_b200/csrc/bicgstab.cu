@@ -211,7 +211,7 @@ void bicgstab_solve(ofg_prec* P, const double* b, double* x, int max_it, double 
    ofg_matrix* A = P->A;
    const int64_t n = A->n;
    ensure_sell(A);
-   if (P->version != A->version) prec_setup(P);
+   if (prec_stale(P)) prec_setup(P);
    DBuf<double> r(n), rr(n), p(n), pp(n), s(n), ss(n), t(n), v(n);
    DBuf<BiState> S(1);
    const unsigned g = grid_for(n, kRedBlock, 8), ge = grid_for(n, 256);

@@ -74,7 +74,7 @@ void noalloc_prepare();
 // nullptr when profiling is off; prof_end(kind, algorithmic bytes) after the
 // launch.  Launches that found their stop flag set are not counted.
 enum { PROF_SPMV64 = 0, PROF_SPMV32 = 1, PROF_SPMV16 = 2, PROF_SWEEP = 3, PROF_ASSEMBLY = 4,
-       PROF_NET_GEMM = 5, PROF_LEARNED_APPLY = 6, kProfKinds = 7 };
+       PROF_NET_GEMM = 5, PROF_LEARNED_APPLY = 6, PROF_ORTH = 7, kProfKinds = 8 };
 bool prof_on();
 int* prof_begin();
 void prof_end(int kind, double bytes);

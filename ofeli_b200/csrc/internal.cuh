@@ -110,6 +110,9 @@ struct ofg_prec {
    ofg::DBuf<int32_t> tpos;  // D-ILU: transposed position of each lower entry
    ofg::DBuf<double> dot;    // (r, z) of the last backward sweep that was asked for it
    int grid = 0;             // blocks of the persistent sweep launch
+   // frozen: the solvers keep the preconditioner as it was set up even after
+   // the matrix values changed (ofg_prec_freeze; refreshed by ofg_prec_update)
+   bool frozen = false;
    // LEARNED: the network that predicts the factor G, and G (lower rows) and
    // G^T (upper rows) as matrices of their own; M = G^T G
    ofg_learned* net = nullptr;
@@ -149,6 +152,9 @@ void scan_exclusive_i64(const int64_t* d_in, int64_t* d_out, int64_t n);
 
 // prec.cu
 void prec_setup(ofg_prec* P);
+// true when the solvers must set the preconditioner up again before use: the
+// matrix values changed since, and the preconditioner is not frozen
+inline bool prec_stale(const ofg_prec* P) { return !P->frozen && P->version != P->A->version; }
 // z = M^{-1} r on device buffers (r and z may alias).  With rz != nullptr
 // the sweep preconditioners also leave (r, z) in *rz (device scalar).  With
 // skip != nullptr every launch is a no-op while *skip != 0.

@@ -472,7 +472,7 @@ void cg_solve(ofg_prec* P, const double* b, double* x, int max_it, double tol, i
               double* res, double* hist)
 {
    ensure_sell(P->A);
-   if (P->version != P->A->version) prec_setup(P);
+   if (prec_stale(P)) prec_setup(P);
    switch (P->type) {
       case OFG_IDENT: cg_run<PT_IDENT>(P, b, x, max_it, tol, result, res, hist); break;
       case OFG_DIAG: cg_run<PT_DIAG>(P, b, x, max_it, tol, result, res, hist); break;
@@ -485,7 +485,7 @@ void gmres_solve(ofg_prec* P, const double* b, double* x, int m, int max_it, dou
 {
    ofg_matrix* A = P->A;
    ensure_sell(A);
-   if (P->version != A->version) prec_setup(P);
+   if (prec_stale(P)) prec_setup(P);
    const int64_t n = A->n;
    OFG_REQUIRE(m >= 1, OFG_ERR_ARG, "restart length must be >= 1");
    DBuf<double> r(n), w(n), q(n), V((size_t)(m + 1) * n);

@@ -32,6 +32,7 @@
 
 #include "internal.cuh"
 #include "reduce.cuh"
+#include "sellq.cuh"
 
 namespace ofg {
 namespace {
@@ -126,32 +127,6 @@ __global__ void __launch_bounds__(kRedBlock, 8) mx_load_residual(int64_t n, int6
    }
 }
 
-__device__ __forceinline__ float4 load_vals(const float* p) { return *reinterpret_cast<const float4*>(p); }
-
-__device__ __forceinline__ float4 load_vals(const __nv_bfloat16* p)
-{
-   const uint2 u = *reinterpret_cast<const uint2*>(p);
-   const __nv_bfloat162 a = *reinterpret_cast<const __nv_bfloat162*>(&u.x);
-   const __nv_bfloat162 b = *reinterpret_cast<const __nv_bfloat162*>(&u.y);
-   const float2 fa = __bfloat1622float2(a), fb = __bfloat1622float2(b);
-   return make_float4(fa.x, fa.y, fb.x, fb.y);
-}
-
-// the columns of four adjacent SELL entries: absolute int32 columns, or
-// 16-bit offsets from the rows r0 .. r0+3 (6 instead of 8 bytes per entry
-// with FP32 values, 4 with BF16 values)
-__device__ __forceinline__ int4 load_cols(const int32_t* p, int64_t)
-{
-   return *reinterpret_cast<const int4*>(p);
-}
-
-__device__ __forceinline__ int4 load_cols(const int16_t* p, int64_t r0)
-{
-   const short4 d = *reinterpret_cast<const short4*>(p);
-   const int r = (int)r0;
-   return make_int4(r + d.x, r + 1 + d.y, r + 2 + d.z, r + 3 + d.w);
-}
-
 // When the host must refine (mode 0) or stop the inner solve (mode 1).
 struct StopRule {
    double delta, tol, scale;
@@ -179,29 +154,11 @@ __device__ __forceinline__ bool decide_pause(MixState* S, double rr2, int it, co
    return stop;
 }
 
-// x[c .. c+3] with 16-byte loads: the aligned quad holding x[c] and, unless
-// c is a multiple of 4, the next one, shifted by c mod 4.  The rows of a
-// slice-uniform slice gather consecutive elements, so a thread's four
-// gathers become one or two vector loads (8 lanes of a slice cover 32
-// consecutive elements).  The second load may read up to 4 elements past
-// the last row: the gathered vectors carry 8 elements of slack.
-__device__ __forceinline__ float4 quad_at(const float* __restrict__ x, int c)
-{
-   const float4* x4 = reinterpret_cast<const float4*>(x);
-   const float4 a = __ldg(x4 + (c >> 2));
-   const int m = c & 3;
-   if (m == 0) return a;
-   const float4 b = __ldg(x4 + (c >> 2) + 1);
-   if (m == 1) return make_float4(a.y, a.z, a.w, b.x);
-   if (m == 2) return make_float4(a.z, a.w, b.x, b.y);
-   return make_float4(a.w, b.x, b.y, b.z);
-}
-
 // q = A p over four rows per thread; (p, q) left as per-block partials for
 // mx_update.  UNI: slices with uniform offsets (suni[s] >= 0) read one
 // offset per position from stab and gather p with vector loads.
 template <class T, class I, bool UNI = false>
-__global__ void __launch_bounds__(kRedBlock, 8) mx_spmv(int64_t nquads, const int32_t* __restrict__ sp,
+__global__ void __launch_bounds__(kRedBlock, kQuadBlocks) mx_spmv(int64_t nquads, const int32_t* __restrict__ sp,
                                                      const I* __restrict__ scol,
                                                      const T* __restrict__ sval,
                                                      const float* __restrict__ p,
@@ -225,16 +182,7 @@ __global__ void __launch_bounds__(kRedBlock, 8) mx_spmv(int64_t nquads, const in
       const T* vp = sval + beg + lane0;
       const int32_t u = UNI ? suni[s] : -1;
       if (u >= 0) {
-         const int16_t* tp = stab + u;
-#pragma unroll 1
-         for (int32_t k = 0; k < w; ++k) {
-            const float4 a = load_vals(vp + k * 32);
-            const float4 x = quad_at(p, (int)r0 + tp[k]);
-            acc.x += a.x * x.x;
-            acc.y += a.y * x.y;
-            acc.z += a.z * x.z;
-            acc.w += a.w * x.w;
-         }
+         acc = uniform_quad(vp, stab + u, w, p, (int)r0);
       }
       else {
          const I* cp = scol + beg + lane0;
@@ -358,62 +306,10 @@ __global__ void __launch_bounds__(kRedBlock, 8) mx_direction(int64_t nquads,
    }
 }
 
-// ---- learned preconditioner M = G^T G inside the FP32 iteration --------
-// G (lower rows) and G^T (upper rows) are SELL-32 matrices on the same
-// slices as A, with BF16 values (the preconditioner's own precision: M is
-// still one fixed symmetric positive definite operator) and 16-bit column
-// offsets where they fit; a thread owns four consecutive rows.
-template <class V, class I, bool UNI>
-__device__ __forceinline__ float4 sell_quad(const int32_t* __restrict__ sp,
-                                            const I* __restrict__ scol,
-                                            const V* __restrict__ sval,
-                                            const float* __restrict__ x, int64_t r0,
-                                            const int32_t* __restrict__ suni,
-                                            const int16_t* __restrict__ stab)
-{
-   const int64_t s = r0 >> 5;
-   const int lane0 = (int)(r0 & 31);
-   const int32_t beg = sp[s], w = (sp[s + 1] - beg) >> 5;
-   float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-   const V* vp = sval + beg + lane0;
-   const int32_t u = UNI ? suni[s] : -1;
-   if (u >= 0) {
-      const int16_t* tp = stab + u;
-#pragma unroll 1
-      for (int32_t k = 0; k < w; ++k) {
-         const float4 a = load_vals(vp + k * 32);
-         const float4 xv = quad_at(x, (int)r0 + tp[k]);
-         acc.x += a.x * xv.x;
-         acc.y += a.y * xv.y;
-         acc.z += a.z * xv.z;
-         acc.w += a.w * xv.w;
-      }
-      return acc;
-   }
-   const I* cp = scol + beg + lane0;
-   auto step = [&](int32_t k) {
-      const int4 c = load_cols(cp + k * 32, r0);
-      const float4 a = load_vals(vp + k * 32);
-      acc.x += a.x * __ldg(x + c.x);
-      acc.y += a.y * __ldg(x + c.y);
-      acc.z += a.z * __ldg(x + c.z);
-      acc.w += a.w * __ldg(x + c.w);
-   };
-   if (UNI) {
-#pragma unroll 1
-      for (int32_t k = 0; k < w; ++k) step(k);
-   }
-   else {
-#pragma unroll 4
-      for (int32_t k = 0; k < w; ++k) step(k);
-   }
-   return acc;
-}
-
 // After iteration `it` (decide): the stop decision from mx_update's
 // partials; then t = G r
 template <class V, class I, bool UNI = false>
-__global__ void __launch_bounds__(kRedBlock, 8) lg_lower(int64_t nquads, const int32_t* __restrict__ sp,
+__global__ void __launch_bounds__(kRedBlock, kQuadBlocks) lg_lower(int64_t nquads, const int32_t* __restrict__ sp,
                                                       const I* __restrict__ scol,
                                                       const V* __restrict__ sval,
                                                       const float* __restrict__ r, float* t,
@@ -439,7 +335,7 @@ __global__ void __launch_bounds__(kRedBlock, 8) lg_lower(int64_t nquads, const i
 
 // z = G^T t; (r, z) left as partials for lg_direction
 template <class V, class I, bool UNI = false>
-__global__ void __launch_bounds__(kRedBlock, 8) lg_upper(int64_t nquads, const int32_t* __restrict__ sp,
+__global__ void __launch_bounds__(kRedBlock, kQuadBlocks) lg_upper(int64_t nquads, const int32_t* __restrict__ sp,
                                                       const I* __restrict__ scol,
                                                       const V* __restrict__ sval,
                                                       const float* __restrict__ t, float* z,
@@ -578,7 +474,7 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
    OFG_REQUIRE(A->dpos_complete, OFG_ERR_PIVOT, "a row has no diagonal entry");
    bool g16 = false;
    if (learned) {
-      if (LP->version != A->version) prec_setup(LP);
+      if (prec_stale(LP)) prec_setup(LP);
       ensure_sell_bf16(LP->gl);
       ensure_sell_bf16(LP->gu);
       g16 = ensure_sell_d16(LP->gl) && ensure_sell_d16(LP->gu);
@@ -651,7 +547,7 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
       }
    }
    const float* jac = learned ? nullptr : dinv.p;
-   const unsigned gq = grid_for(nquads, kRedBlock, 8);
+   const unsigned gq = grid_for(nquads, kRedBlock, kQuadBlocks);
    // per-block partials of the reductions that the next kernel finishes:
    // (p, q) of the SpMV, ||r||^2 and (r, D r) of the update, (r, z) of the
    // product with G^T

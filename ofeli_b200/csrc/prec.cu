@@ -945,11 +945,19 @@ int ofg_prec_update(ofg_prec* P)
    });
 }
 
+int ofg_prec_freeze(ofg_prec* P, int on)
+{
+   return guarded("ofg_prec_freeze", [&] {
+      OFG_REQUIRE(P, OFG_ERR_ARG, "null preconditioner");
+      P->frozen = on != 0;
+   });
+}
+
 int ofg_prec_apply(ofg_prec* P, const double* b, double* x)
 {
    return guarded("ofg_prec_apply", [&] {
       OFG_REQUIRE(P && b && x, OFG_ERR_ARG, "null argument");
-      if (P->version != P->A->version) prec_setup(P);
+      if (prec_stale(P)) prec_setup(P);
       const int64_t n = P->A->n;
       In<double> db(b, n);
       InOut<double> dx(x, n, false);

@@ -151,8 +151,9 @@ void prof_collect()
    g_pending.clear();
 }
 
-static const char* kProfNames[kProfKinds] = {"spmv64", "spmv32",       "spmv16",       "sweep",
-                                             "assembly", "network_gemm", "learned_apply"};
+static const char* kProfNames[kProfKinds] = {"spmv64",   "spmv32",       "spmv16",
+                                             "sweep",    "assembly",     "network_gemm",
+                                             "learned_apply", "gram_schmidt"};
 
 bool is_device_ptr(const void* p)
 {

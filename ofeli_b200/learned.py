@@ -81,3 +81,49 @@ def train_default(seed=7, M=20, nproblems=4, rounds=8, dim=3):
             "problems": what, "pairs_per_problem": 64, "loss_first": hist[0],
             "loss_last": hist[-1], "objective": "Kaporin number of M A on the pairs"}
     return net, info
+
+
+def cd2d_problem(nx, seed, eps=1e-3, dt=1e-3, nx_target=1024):
+    """A DC2DT3 backward-Euler matrix on nx x nx cells whose mass, diffusion
+    and convection terms stand in the proportions they have on nx_target
+    cells with (eps, dt): all three scale with h when eps and dt do, so
+    eps and dt are multiplied by nx_target / nx.  The velocity field is a
+    rotation about a seeded centre near (0.5, 0.5) with a seeded speed in
+    [0.5, 1.5].  Returns (A, mesh)."""
+    rng = np.random.default_rng(seed)
+    c = 0.5 + 0.1 * rng.uniform(-1, 1, 2)
+    w = rng.uniform(0.5, 1.5)
+    s = nx_target / float(nx)
+    mesh = F.Mesh(0.0, 1.0, 0.0, 1.0, nx, nx, 1, 1, 1, 1)
+    xy, _, code, _ = mesh.arrays()
+    P = xy.reshape(-1, 2)
+    v = np.stack([-w * (P[:, 1] - c[1]), w * (P[:, 0] - c[0])], axis=1).reshape(-1)
+    eq = F.DC2DT3(mesh, np.zeros(mesh.nn), v, eps * s, dt * s)
+    eq.setDirichlet(np.zeros(mesh.nn))
+    A, _ = eq.build()
+    return A, mesh
+
+
+def train_transient(seed=7, sizes=(128, 256), nproblems=4, rounds=8, npairs=64, steps=10):
+    """The network of the transient benchmark's chosen form: trained on
+    `nproblems` convection-diffusion matrices (cd2d_problem, seeds 200, 201,
+    ..., sizes taken in turn) with the Kaporin objective on operator pairs
+    (make_pairs_operator).  Returns (net, info)."""
+    t0 = time.perf_counter()
+    net = F.LearnedNet(seed)
+    data, keep = [], []
+    for q in range(nproblems):
+        A, mesh = cd2d_problem(sizes[q % len(sizes)], 200 + q)
+        R, E = F.LearnedNet.make_pairs_operator(A, npairs, seed=2000 + q)
+        data.append((A, R, E))
+        keep.append(mesh)
+    hist = []
+    for _ in range(rounds):
+        for A, R, E in data:
+            hist.append(float(net.train(A, R, E, steps=steps, batch=16).mean()))
+    info = {"train_s": time.perf_counter() - t0, "adam_steps": rounds * nproblems * steps,
+            "problems": "%d DC2DT3 backward-Euler matrices, %s cells, eps and dt scaled to the "
+                        "1024^2-cell proportions, seeded rotations" % (nproblems, list(sizes)),
+            "pairs_per_problem": npairs, "loss_first": hist[0], "loss_last": hist[-1],
+            "objective": "Kaporin number of M A_sym on operator pairs r = A e"}
+    return net, info

@@ -371,6 +371,13 @@ class Prec:
         else:
             _call("ofg_prec_update", self._h)
 
+    def freeze(self, on=True):
+        """Keep this preconditioner as it is while the matrix values change
+        (the solvers then skip their refresh; setMatrix() still refreshes).
+        The learned factor of a time-stepping scheme whose matrix stays the
+        same from step to step is computed once this way."""
+        _call("ofg_prec_freeze", self._h, 1 if on else 0)
+
     def solve(self, b, x=None):
         b = _f64(b, self.A.n)
         if x is None:
@@ -514,6 +521,22 @@ class LearnedNet:
             E[p] = xs - x0
         return R, E
 
+    @staticmethod
+    def make_pairs_operator(A, npairs, seed=0):
+        """Residual / error pairs without a solve: e_p white noise and
+        r_p = A e_p, the spectrally flat errors the Kaporin objective wants
+        (what make_pairs' random starting guesses give, up to the solve's
+        tolerance).  Works for nonsymmetric A, where the objective fits
+        G^T G to the symmetric part.  Returns R, E as (npairs, n) float32."""
+        n = A.n
+        R = np.zeros((npairs, n), np.float32)
+        E = np.zeros((npairs, n), np.float32)
+        for p in range(npairs):
+            e = fields.normal(seed * 1000003 + p, n)
+            R[p] = A.Mult(e)
+            E[p] = e
+        return R, E
+
     def train(self, A, R, E, steps, batch=16, lr=1e-3):
         """Adam steps on residual / error pairs (rows of R and E); returns the
         per-step batch losses."""
@@ -549,6 +572,24 @@ def fcg_learned(P, b, x, inner_bits=32, toler=1e-10, max_outer=200, max_inner=10
     o, i, r, fb = ctypes.c_int(), ctypes.c_int(), ctypes.c_double(), ctypes.c_int()
     _call("ofg_fcg_learned", P._h, inner_bits, _ptr(b), _ptr(x), max_outer, max_inner, inner_tol,
           toler, ctypes.byref(o), ctypes.byref(i), ctypes.byref(r), ctypes.byref(fb))
+    return o.value, i.value, r.value, bool(fb.value)
+
+
+def fgmres_mixed(P, b, x, m=30, inner_bits=0, toler=1e-10, inner_tol=1e-5, max_outer=50,
+                 max_inner=100000):
+    """Flexible GMRES(m), right preconditioned by P (DIAG, IDENT or the learned
+    M = G^T G), with an FP32 matrix-vector product and preconditioner inside
+    FP64 iterative refinement, FP64 classical Gram-Schmidt applied twice; x
+    is the initial guess (warm start) and receives the solution.  Converged
+    on the FP64 true residual ||b - A x|| / ||b|| <= toler.  inner_bits: 32
+    (FP32 values), 16 (BF16 values) or 0 (BF16 only when every value is
+    exact).  Returns (cycles, Arnoldi steps, true relative residual,
+    fell_back): fell_back is True when the learned preconditioner stopped
+    reducing the residual and the last cycles used the diagonal one."""
+    b = _f64(b, P.A.n)
+    o, i, r, fb = ctypes.c_int(), ctypes.c_int(), ctypes.c_double(), ctypes.c_int()
+    _call("ofg_fgmres_mixed", P._h, inner_bits, _ptr(b), _ptr(x), m, max_outer, max_inner,
+          inner_tol, toler, ctypes.byref(o), ctypes.byref(i), ctypes.byref(r), ctypes.byref(fb))
     return o.value, i.value, r.value, bool(fb.value)
 
 
@@ -802,3 +843,23 @@ class DC2DT3:
             it = GMRes(self._A, Prec(self._A, prec), self._b, self.x, m, max_it, toler)
         _call("ofg_insert_bc", self.mesh._h, _ptr(self.x), _ptr(self._bc), _ptr(self.u))
         return it
+
+    def step_mixed(self, prec=DIAG_PREC, net=None, m=30, toler=1e-10, inner_tol=1e-5,
+                   inner_bits=0):
+        """One time step with the chosen form: flexible GMRES(m) in mixed
+        precision (fgmres_mixed), warm-started from the previous step,
+        converged on the FP64 true residual.  prec: DIAG_PREC, or
+        LEARNED_PREC with `net`, whose factor is computed on the first
+        step's matrix and kept (frozen) for the later steps: with a fixed
+        time step the matrix is the same at every step.  Returns (cycles,
+        Arnoldi steps, FP64 true relative residual, fell_back)."""
+        self.build()
+        P = getattr(self, "_mixed_prec", None)
+        if P is None or P.type != prec:
+            P = self._mixed_prec = Prec(self._A, prec, net=net)
+            if prec == LEARNED_PREC:
+                P.freeze()
+        out = fgmres_mixed(P, self._b, self.x, m=m, inner_bits=inner_bits, toler=toler,
+                           inner_tol=inner_tol)
+        _call("ofg_insert_bc", self.mesh._h, _ptr(self.x), _ptr(self._bc), _ptr(self.u))
+        return out
