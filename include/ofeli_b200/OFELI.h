@@ -628,8 +628,11 @@ class DC2DT3 {
    }
    SpMatrix<real_t>& getMatrix() { return _A; }
    Vect<real_t>& getRHS() { return _b; }
+   // Equa::getLinearSolver(): the solver of TimeStepping's implicit steps
+   LinearSolver& getLinearSolver() { return _ls; }
 
  private:
+   friend class TimeStepping;
    Mesh* _mesh;
    Vect<real_t>* _u;
    const Vect<real_t>* _v;
@@ -638,6 +641,71 @@ class DC2DT3 {
    SpMatrix<real_t> _A;
    const Vect<real_t>* _bc = nullptr;
    Vect<real_t> _b, _x;
+   LinearSolver _ls;
+};
+
+// TimeStepping (src/solvers/TimeStepping.cpp) for a DC2DT3 equation under
+// its first-order schemes.  Backward Euler and Crank-Nicolson: build() of
+// the scheme's system and the equation's LinearSolver (the solver and
+// preconditioner of setLinearSolver, GMRES restarting every n/5 steps,
+// warm-started from the previous step); forward Euler: x = b / D with D the
+// assembled diagonal (ofg_matrix_diag_solve).  As OFELI's set() tests the
+// scheme against HEUN and NEWMARK with bitwise ANDs, forward Euler (1) and
+// Crank-Nicolson (3) make two sub-steps per runOneTimeStep (NEWMARK = 5).
+class TimeStepping {
+ public:
+   TimeStepping(TimeScheme s, real_t time_step, real_t final_time = 1.0)
+      : _s(s), _dt(time_step), _final(final_time)
+   {
+      if (s != FORWARD_EULER && s != BACKWARD_EULER && s != CRANK_NICOLSON)
+         throw OFELIException("In TimeStepping::set(...): scheme outside the GPU path");
+      _nb_ssteps = ((int)s & 4) || ((int)s & 5) ? 2 : 1;  // HEUN = 4, NEWMARK = 5
+   }
+   void setPDE(DC2DT3& eq)
+   {
+      _eq = &eq;
+      eq._dt = _dt;
+      eq.setTransient(_s);
+   }
+   void setInitial(Vect<real_t>& u) { *_eq->_u = u; }
+   void setBC(const Vect<real_t>& bc) { _eq->setDirichlet(bc); }
+   void setLinearSolver(Iteration s = GMRES_SOLVER, Preconditioner p = DIAG_PREC)
+   {
+      _it = s, _p = p;
+   }
+   real_t runOneTimeStep()
+   {
+      if (!_eq) throw OFELIException("TimeStepping: no equation (setPDE)");
+      DC2DT3& eq = *_eq;
+      for (int k = 0; k < _nb_ssteps; ++k) {
+         eq.build();
+         if (_s == FORWARD_EULER)
+            ofg_check(ofg_matrix_diag_solve(eq._A.handle(), eq._b.data(), eq._x.data()),
+                      "TimeStepping::solveForwardEuler");
+         else {
+            eq._ls.setMatrix(eq._A);
+            eq._ls.setRHS(eq._b);
+            eq._ls.setSolution(eq._x);
+            eq._ls.solve(_it, _p);
+         }
+         ofg_check(ofg_insert_bc(eq._mesh->handle(), eq._x.data(),
+                                 eq._bc ? eq._bc->data() : nullptr, eq._u->data()),
+                   "TimeStepping::insertBC");
+      }
+      return _dt;
+   }
+   void run()
+   {
+      for (real_t t = 0; t < _final - 0.5 * _dt; t += _dt) runOneTimeStep();
+   }
+
+ private:
+   TimeScheme _s;
+   real_t _dt, _final;
+   int _nb_ssteps = 1;
+   DC2DT3* _eq = nullptr;
+   Iteration _it = GMRES_SOLVER;
+   Preconditioner _p = DIAG_PREC;
 };
 
 }  // namespace OFELI

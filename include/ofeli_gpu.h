@@ -116,6 +116,11 @@ int ofg_spmv_add(const ofg_matrix* A, const double* x, double* y);
  * order as OFELI's loop intends (SpMatrix_impl.h:760-767; OFELI's loop reads
  * the previous entry's column, see entries.cu). */
 int ofg_spmv_transpose_add(ofg_matrix* A, const double* x, double* y);
+/* x_i = b_i / a_ii for every row (one division each): the explicit step of
+ * TimeStepping's forward Euler scheme, b(i) /= D(i) with D the assembled
+ * diagonal (src/solvers/TimeStepping.cpp:428-441).  OFG_ERR_PIVOT when a
+ * row's diagonal entry is zero or absent. */
+int ofg_matrix_diag_solve(ofg_matrix* A, const double* b, double* x);
 /* SpMatrix::set(i,j,v) (set = 1) / add(i,j,v) (set = 0) for `count` entries,
  * 1-based indices, applied in order (SpMatrix_impl.h:785-802); a pair outside
  * the pattern stops the batch with OFG_ERR_ARG. */

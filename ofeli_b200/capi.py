@@ -40,6 +40,7 @@ SIGNATURES = {
     "ofg_matrix_create": (_i32, [_i64, _i64, _p, _p, _pp]),
     "ofg_matrix_destroy": (_i32, [_p]),
     "ofg_spmv_transpose_add": (_i32, [_p, _p, _p]),
+    "ofg_matrix_diag_solve": (_i32, [_p, _p, _p]),
     "ofg_matrix_edit": (_i32, [_p, _i64, _p, _p, _p, _i32]),
     "ofg_matrix_info": (_i32, [_p, _pi64, _pi64]),
     "ofg_matrix_get_pattern": (_i32, [_p, _p, _p]),

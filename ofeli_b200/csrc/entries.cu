@@ -18,6 +18,11 @@
 // penalties); a pair outside the pattern stops the batch with OFG_ERR_ARG
 // after the entries before it (OFELI's set throws there; its add writes
 // into the previous row's last entry instead).
+//
+// The diagonal solve x_i = b_i / a_ii is the explicit step of TimeStepping's
+// forward Euler scheme (src/solvers/TimeStepping.cpp:428-441: b(i) /=
+// D(i), D the assembled diagonal of the scaled capacity), one correctly
+// rounded division per row.
 #include "internal.cuh"
 
 namespace ofg {
@@ -131,6 +136,20 @@ void ensure_transpose(ofg_matrix* A)
    A->t_ready = true;
 }
 
+// x_i = b_i / a_ii; *bad = lowest row without a nonzero diagonal entry
+__global__ void diag_divide(int64_t n, const int32_t* __restrict__ dpos,
+                            const double* __restrict__ val, const double* __restrict__ b, double* x,
+                            int* bad)
+{
+   int64_t stride = (int64_t)gridDim.x * blockDim.x;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+      const int32_t d = dpos[i];
+      const double a = d >= 0 ? val[d] : 0.0;
+      if (a == 0.0) atomicMin(bad, (int)i);
+      x[i] = b[i] / a;
+   }
+}
+
 }  // namespace
 }  // namespace ofg
 
@@ -181,6 +200,31 @@ int ofg_matrix_edit(ofg_matrix* A, int64_t count, const int64_t* i, const int64_
                                       ") not compatible with sparse storage (entry " +
                                       std::to_string(h) + " of the batch)");
       }
+   });
+}
+
+int ofg_matrix_diag_solve(ofg_matrix* A, const double* b, double* x)
+{
+   return guarded("ofg_matrix_diag_solve", [&] {
+      OFG_REQUIRE(A && b && x, OFG_ERR_ARG, "null argument");
+      const int64_t n = A->n;
+      ensure_dpos(A);
+      In<double> db(b, n);
+      InOut<double> dx(x, n, false);
+      DBuf<int> bad(1);
+      int big = INT32_MAX;
+      bad.upload(&big, 1);
+      if (n) {
+         diag_divide<<<grid_for(n, 256), 256, 0, stream()>>>(n, A->dpos.p, A->val.p, db.d, dx.d,
+                                                            bad.p);
+         count_launch();
+         OFG_LAUNCH_CHECK();
+      }
+      int h = 0;
+      bad.download(&h, 1);
+      OFG_REQUIRE(h == INT32_MAX, OFG_ERR_PIVOT,
+                  "zero or missing diagonal entry in row " + std::to_string(h + 1));
+      dx.finish();
    });
 }
 

@@ -109,7 +109,8 @@ struct ofg_prec {
    ofg::SweepPlan fwd, bwd;
    ofg::DBuf<int32_t> tpos;  // D-ILU: transposed position of each lower entry
    ofg::DBuf<double> dot;    // (r, z) of the last backward sweep that was asked for it
-   int grid = 0;             // blocks of the persistent sweep launch
+   int grid = 0;             // blocks of the persistent factorisation sweep launch
+   int solve_grid = 0;       // blocks of the persistent solve sweep launch
    // frozen: the solvers keep the preconditioner as it was set up even after
    // the matrix values changed (ofg_prec_freeze; refreshed by ofg_prec_update)
    bool frozen = false;

@@ -35,7 +35,9 @@
 // issues, the epilogue reads the accumulators with tcgen05.ld and applies
 // bias / ReLU / residual in registers.  A CUDA-core version of the same
 // product is kept as the checker (ofg_learned_gemm_check).  The weight
-// gradient X^T dZ (a reduction over all rows) runs on CUDA cores.
+// gradient X^T dZ (a reduction over all rows: the rows are the MMA's K)
+// runs on the tensor cores too (wgrad_tc), from the BF16 copy of dZ that
+// the data product uses.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -457,6 +459,136 @@ __global__ void __launch_bounds__(128, 4) gemm_tc(int64_t rows, GemmA a,
    // after a wait that ran out, give the MMAs in flight one more bounded
    // wait before the tensor memory is released
    if (failed) mbar_wait(smem_u32(mbar), phase);
+   __syncthreads();
+   if (warp == 0)
+      asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(N)
+                   : "memory");
+}
+
+// Weight gradient on the tensor cores: part[block] = X^T dz over the
+// block's 128-row tiles, X = [h | agg] (rows x 128, BF16) and dz (rows x 64,
+// BF16).  The reduction runs over the rows, so the rows are the MMA's K:
+// each tile stages X^T (M = 128 features x K = 128 rows) and dz^T (N = 64 x
+// K) in the K-major core-matrix layout of gemm_tc (element (m, k) at
+// (k/8)*(M/8)*128 + m*16 + (k%8)*2 bytes; thread t writes row t of the
+// tile, transposed, two bytes at a time), one thread issues the tile's
+// eight K = 16 MMAs into the block's tensor-memory accumulator (128 lanes x
+// 64 FP32 columns, kept across the block's tiles), and the block writes its
+// 128 x 64 partial at the end.  Waits are bounded as in gemm_tc.
+__global__ void __launch_bounds__(128, 4) wgrad_tc(int64_t rows, GemmA a,
+                                                   const bf16* __restrict__ dz, float* part,
+                                                   int* status, int* worked)
+{
+   constexpr int M = 2 * HID, N = HID;
+   prof_mark(worked);
+   extern __shared__ __align__(1024) unsigned char smem[];
+   unsigned char* sA = smem;                // M x 128 rows: 32 KB
+   unsigned char* sB = smem + M * 128 * 2;  // N x 128 rows: 16 KB
+   uint64_t* mbar = reinterpret_cast<uint64_t*>(sB + N * 128 * 2);
+   uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 1);
+   const int tid = threadIdx.x, warp = tid >> 5;
+   if (tid == 0) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(1) : "memory");
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+   }
+   if (warp == 0) {
+      asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                      smem_u32(tslot)),
+                   "r"(N)
+                   : "memory");
+      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+   }
+   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+   __syncthreads();
+   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+   const uint32_t tmem = *tslot;
+   const uint32_t sa = smem_u32(sA), sb = smem_u32(sB);
+   constexpr uint32_t idesc = instr_desc_bf16_f32<N>();
+   uint32_t phase = 0;
+   bool failed = false, any = false;
+   const int64_t ntiles = (rows + 127) / 128;
+   bf16* pa = reinterpret_cast<bf16*>(sA + (tid >> 3) * (M / 8) * 128 + (tid & 7) * 2);
+   bf16* pb = reinterpret_cast<bf16*>(sB + (tid >> 3) * (N / 8) * 128 + (tid & 7) * 2);
+
+   for (int64_t tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
+      const int64_t r = tile * 128 + tid;  // this thread's row: K index tid of the tile
+#pragma unroll 4
+      for (int c = 0; c < M / 8; ++c) {
+         uint4 v = make_uint4(0, 0, 0, 0);
+         if (r < rows) v = *reinterpret_cast<const uint4*>(a.at(r, c * 8));
+         const bf16* e = reinterpret_cast<const bf16*>(&v);
+#pragma unroll
+         for (int q = 0; q < 8; ++q) pa[(c * 8 + q) * 8] = e[q];  // (m = 8c + q) * 16 bytes
+      }
+#pragma unroll 4
+      for (int c = 0; c < N / 8; ++c) {
+         uint4 v = make_uint4(0, 0, 0, 0);
+         if (r < rows) v = *reinterpret_cast<const uint4*>(dz + r * N + c * 8);
+         const bf16* e = reinterpret_cast<const bf16*>(&v);
+#pragma unroll
+         for (int q = 0; q < 8; ++q) pb[(c * 8 + q) * 8] = e[q];
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncthreads();
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      if (tid == 0) {
+#pragma unroll
+         for (int kk = 0; kk < 8; ++kk) {
+            const uint64_t ad = smem_desc(sa + kk * 2 * (M * 16), M * 16, 128);
+            const uint64_t bd = smem_desc(sb + kk * 2 * (N * 16), N * 16, 128);
+            const uint32_t acc = (any || kk > 0) ? 1u : 0u;
+            asm volatile(
+               "{\n\t.reg .pred p;\n\t"
+               "setp.ne.b32 p, %4, 0;\n\t"
+               "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+               "l"(ad), "l"(bd), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0)
+               : "memory");
+         }
+         asm volatile(
+            "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+               smem_u32(mbar))
+            : "memory");
+      }
+      any = true;
+      // the tile's MMAs must finish before the next tile overwrites the
+      // operands (bounded wait, verdict uniform over the block)
+      if (__syncthreads_or(mbar_wait(smem_u32(mbar), phase) ? 0 : 1)) {
+         failed = true;
+         if (tid == 0) atomicOr(status, 1);
+      }
+      else {
+         phase ^= 1;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+   }
+   // the accumulator: lane m = input feature, column n = output
+   float* out = part + (int64_t)blockIdx.x * M * N + (int64_t)(warp * 32 + (tid & 31)) * N;
+   for (int cb = 0; cb < N; cb += 16) {
+      uint32_t v[16];
+      if (any && !failed) {
+         const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb;
+         asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, "
+            "%10, %11, %12, %13, %14, %15}, [%16];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+              "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+              "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+            : "r"(taddr));
+         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      }
+      else {
+#pragma unroll
+         for (int q = 0; q < 16; ++q) v[q] = 0u;
+      }
+      float4* o = reinterpret_cast<float4*>(out + cb);
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+         o[q] = make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]),
+                            __uint_as_float(v[4 * q + 2]), __uint_as_float(v[4 * q + 3]));
+   }
+   if (failed) mbar_wait(smem_u32(mbar), phase);
+   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
    __syncthreads();
    if (warp == 0)
       asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(N)
@@ -968,9 +1100,10 @@ __global__ void lp_layer_back(int64_t n, const int32_t* rp, const int32_t* col, 
 
 // per-block partials of X^T dz with X = [x0 (k0 columns) | x1] and an
 // implicit all-ones column KIN for the bias gradient: part[b][(KIN+1) x HID]
-template <int KIN, class XT>
+// (KIN = 0: the bias gradient alone)
+template <int KIN, class XT, class ZT>
 __global__ void __launch_bounds__(256) lp_wgrad(int64_t n, const XT* x0, int ld0, int k0,
-                                                const XT* x1, int ld1, const float* dz, float* part)
+                                                const XT* x1, int ld1, const ZT* dz, float* part)
 {
    constexpr int W = (KIN + 1) * HID;
    float acc[(W + 255) / 256];
@@ -983,7 +1116,7 @@ __global__ void __launch_bounds__(256) lp_wgrad(int64_t n, const XT* x0, int ld0
       for (int q = threadIdx.x; q < KIN; q += blockDim.x)
          xs[q] = q < k0 ? to_f(x0[i * ld0 + q]) : to_f(x1[i * ld1 + (q - k0)]);
       if (threadIdx.x == 0) xs[KIN] = 1.f;
-      for (int q = threadIdx.x; q < HID; q += blockDim.x) zs[q] = dz[i * HID + q];
+      for (int q = threadIdx.x; q < HID; q += blockDim.x) zs[q] = to_f(dz[i * HID + q]);
       __syncthreads();
 #pragma unroll
       for (int q = 0; q < (W + 255) / 256; ++q) {
@@ -1066,11 +1199,39 @@ static double learned_backward(ofg_learned* L, ofg_matrix* A, LearnedGraph& G, c
       GemmA a{dz16.p, HID, nullptr, 0, HID};
       run_gemm<HID, 2 * HID>(L, n, a, L->wb.p + (size_t)l * 2 * HID * HID, bf);
       {
+         // weight and bias gradients from the BF16 copy of dz, the operand of
+         // the data product: X^T dz on the tensor cores (or on CUDA cores, the
+         // checker), the column sums of dz on CUDA cores
          constexpr int W = (2 * HID + 1) * HID;
-         DBuf<float> part((size_t)nb * W), tot(W);
-         lp_wgrad<2 * HID, bf16><<<nb, 256, 0, stream()>>>(n, G.hbuf(l), HID, HID, G.aggbuf(l), HID,
-                                                           dz.p, part.p);
-         lp_sum_parts<<<32, 256, 0, stream()>>>(part.p, nb, W, tot.p);
+         DBuf<float> tot(W);
+         if (L->use_tc && n > 0) {
+            const int smem = 2 * HID * 128 * 2 + HID * 128 * 2 + 64;
+            static bool attr_set = false;
+            if (!attr_set) {
+               OFG_CUDA(cudaFuncSetAttribute(wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             smem));
+               attr_set = true;
+            }
+            const unsigned gw =
+               (unsigned)std::min<int64_t>((n + 127) / 128, (int64_t)num_sms() * 4);
+            DBuf<float> pw((size_t)gw * 2 * HID * HID), pb((size_t)nb * HID);
+            int* worked = prof_begin();
+            wgrad_tc<<<gw, 128, smem, stream()>>>(n, GemmA{G.hbuf(l), HID, G.aggbuf(l), HID, HID},
+                                                  dz16.p, pw.p, L->status.p, worked);
+            prof_end(PROF_NET_GEMM, (double)n * (2 * HID * 2 + HID * 2) + 4.0 * gw * 2 * HID * HID);
+            lp_wgrad<0, bf16, bf16><<<nb, 256, 0, stream()>>>(n, nullptr, 0, 0, nullptr, 0, dz16.p,
+                                                              pb.p);
+            lp_sum_parts<<<32, 256, 0, stream()>>>(pw.p, gw, 2 * HID * HID, tot.p);
+            lp_sum_parts<<<1, 64, 0, stream()>>>(pb.p, nb, HID, tot.p + 2 * HID * HID);
+            count_launch(2);
+         }
+         else {
+            DBuf<float> part((size_t)nb * W);
+            lp_wgrad<2 * HID, bf16, bf16><<<nb, 256, 0, stream()>>>(n, G.hbuf(l), HID, HID,
+                                                                   G.aggbuf(l), HID, dz16.p,
+                                                                   part.p);
+            lp_sum_parts<<<32, 256, 0, stream()>>>(part.p, nb, W, tot.p);
+         }
          // rows 0..127 -> W_l, row 128 -> b_l
          OFG_CUDA(cudaMemcpyAsync(L->grads.p + P_W + l * 2 * HID * HID, tot.p,
                                   sizeof(float) * 2 * HID * HID, cudaMemcpyDeviceToDevice, stream()));
@@ -1087,8 +1248,8 @@ static double learned_backward(ofg_learned* L, ofg_matrix* A, LearnedGraph& G, c
    {
       constexpr int W = (NFEAT + 1) * HID;
       DBuf<float> part((size_t)nb * W), tot(W);
-      lp_wgrad<NFEAT, float><<<nb, 256, 0, stream()>>>(n, G.feat.p, NFEAT, NFEAT, G.feat.p, NFEAT,
-                                                       dz.p, part.p);
+      lp_wgrad<NFEAT, float, float><<<nb, 256, 0, stream()>>>(n, G.feat.p, NFEAT, NFEAT, G.feat.p,
+                                                              NFEAT, dz.p, part.p);
       lp_sum_parts<<<4, 256, 0, stream()>>>(part.p, nb, W, tot.p);
       OFG_CUDA(cudaMemcpyAsync(L->grads.p + P_WIN, tot.p, sizeof(float) * NFEAT * HID,
                                cudaMemcpyDeviceToDevice, stream()));

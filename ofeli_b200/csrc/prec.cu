@@ -22,8 +22,10 @@
 // contraction), so its pivots are bit-identical to the reference's.
 //
 // Per application: 12*nnz + 4*n (matrix, once per sweep over its half) +
-// ~40*n bytes of vectors.  Time is set by the dependency chain (about 2 grid
-// lines' worth of segments on a structured 2-D mesh), not by bandwidth.
+// ~40*n bytes of vectors.  Time is set by the dependency chain (one
+// segment step per grid line on a structured 2-D mesh, plus one per segment
+// of a line), not by bandwidth; the solve sweeps hand the values of a strand
+// to the next one through shared memory where both belong to one block.
 #include <algorithm>
 
 #include "internal.cuh"
@@ -423,24 +425,94 @@ __device__ __forceinline__ void load_segment(const SolveArgs& g, int64_t s, int6
    }
 }
 
+// Band hand-off.  A block takes a band of kBandWarps consecutive strands,
+// one warp each.  Besides storing its results to global memory (for the
+// strands of other blocks), a warp keeps the latest kRing of them in a
+// shared-memory ring and publishes how far it got (done_end: the logical
+// row one past its last finished segment) with a CTA-scope release; the
+// next warp of the band takes the values of the previous strand from the
+// ring, with an acquire, instead of waiting for them to travel through L2.
+// The ring is only a faster path: when the producer may already have
+// overwritten a slot (it ran more than kRing - 32 rows ahead), the value is
+// read from global memory, where it was stored first.  The arithmetic is the
+// same either way, so the results are bit for bit those of the global path.
+constexpr int kBandWarps = 16;
+constexpr int kRing = 256;
+constexpr long long kSpinSmemFast = 1 << 14;
+constexpr long long kSpinSmemSlow = 1 << 22;  // x ~0.5 us sleep: a few seconds at most
+
+__device__ __forceinline__ long long ld_acquire_cta(const long long* p)
+{
+   long long v;
+   asm volatile("ld.acquire.cta.shared.s64 %0, [%1];"
+                : "=l"(v)
+                : "r"((unsigned)__cvta_generic_to_shared(p))
+                : "memory");
+   return v;
+}
+
+__device__ __forceinline__ void st_release_cta(long long* p, long long v)
+{
+   asm volatile("st.release.cta.shared.s64 [%0], %1;" ::"r"((unsigned)__cvta_generic_to_shared(p)),
+                "l"(v)
+                : "memory");
+}
+
+// Value of logical row lj of the previous strand of the band (warp w - 1):
+// from the ring once its producer published it, else (waited too long, or
+// possibly overwritten) from global memory with the bounded wait.
+__device__ __noinline__ double ring_value(const double* ring, const long long* done_end,
+                                          long long lj, const double* gsrc, int* status)
+{
+   long long de = ld_acquire_cta(done_end);
+   for (long long it = 0; de <= lj; ++it) {
+      if (it >= kSpinSmemFast + kSpinSmemSlow) {
+         atomicOr(status, 1);
+         return wait_value_slow(gsrc, status);
+      }
+      if (it >= kSpinSmemFast) __nanosleep(500);
+      de = ld_acquire_cta(done_end);
+   }
+   if (de - lj < kRing - 32) {
+      const double v = *(volatile const double*)(ring + (lj % kRing));
+      __threadfence_block();
+      const long long de2 = *(volatile const long long*)done_end;
+      if (de2 - lj < kRing - 32) return v;
+   }
+   return wait_value(gsrc, status);
+}
+
 template <int MODE>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32) solve_sweep(SolveArgs g)
+__global__ void __launch_bounds__(kBandWarps * 32, 1) solve_sweep(SolveArgs g)
 {
    constexpr bool FWD = (MODE == FWD_DILU || MODE == FWD_SSOR);
-   __shared__ double segv[kWarpsPerBlock][32];
+   __shared__ double segv[kBandWarps][32];
+   __shared__ double ring[kBandWarps][kRing];
+   __shared__ long long done_end[kBandWarps];
+   __shared__ long long band_sh;
    const int lane = threadIdx.x & 31;
    const int w = threadIdx.x >> 5;
    const unsigned FULL = 0xffffffffu;
    const int64_t n = g.n;
    if (g.skip && *g.skip) return;
    prof_mark(g.worked);
+   const int64_t nbands = (g.nstrands + kBandWarps - 1) / kBandWarps;
 
    for (;;) {
-      int t = 0;
-      if (lane == 0) t = atomicAdd(&g.ticket[0], 1);
-      t = __shfl_sync(FULL, t, 0);
-      if (t >= g.nstrands) break;
-      const int64_t beg = g.sstart[t], end = g.sstart[t + 1];
+      // every warp finished the previous band: the rings are free
+      __syncthreads();
+      if (threadIdx.x == 0) band_sh = atomicAdd(&g.ticket[0], 1);
+      __syncthreads();
+      const int64_t band = band_sh;
+      if (band >= nbands) break;
+      const int64_t t = band * kBandWarps + w;
+      const bool active = t < g.nstrands;
+      const int64_t beg = active ? g.sstart[t] : 0, end = active ? g.sstart[t + 1] : 0;
+      // the previous strand is this block's warp w - 1 (rows pbeg .. beg-1)
+      const int64_t pbeg = (active && w > 0) ? g.sstart[t - 1] : beg;
+      if (lane == 0) done_end[w] = beg;
+      __syncthreads();
+      if (!active) continue;
       const int64_t sfirst = g.tseg[t], slast = g.tseg[t + 1];
       double carry = 0.0;
       bool have_carry = false;
@@ -452,7 +524,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) solve_sweep(SolveArgs g)
          if (s + 1 < slast) load_segment<FWD>(g, s + 1, s0 + 32, end, lane, nxt);
          const int64_t rho = s0 + lane;
          const bool valid = rho < end;
-         // earlier-row values: all loads issued, then consumed in slot order
+         // earlier-row values of other blocks' strands: all loads issued,
+         // then consumed in slot order
          double z[kSlots];
 #pragma unroll
          for (int k = 0; k < kSlots; ++k) {
@@ -460,7 +533,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) solve_sweep(SolveArgs g)
             const int32_t c = cur.c[k];
             if (c >= 0) {
                const int64_t lj = FWD ? c : n - 1 - c;
-               if (lj < s0 && !(lj == s0 - 1 && have_carry)) z[k] = ld_relaxed(g.out + c);
+               if (lj < pbeg) z[k] = ld_relaxed(g.out + c);
             }
          }
          double sext = 0.0, m1 = 0.0;
@@ -477,6 +550,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) solve_sweep(SolveArgs g)
             }
             double v;
             if (lj == s0 - 1 && have_carry) v = carry;
+            else if (lj >= beg) v = wait_value(g.out + c, g.status);  // own strand, earlier segment
+            else if (lj >= pbeg) v = ring_value(ring[w - 1], &done_end[w - 1], lj, g.out + c, g.status);
             else v = is_sentinel(z[k]) ? wait_value_slow(g.out + c, g.status) : z[k];
             sext += cur.a[k] * v;
          }
@@ -490,7 +565,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) solve_sweep(SolveArgs g)
                else other_intra = true;
                continue;
             }
-            const double v = (lj == s0 - 1 && have_carry) ? carry : wait_value(g.out + c, g.status);
+            double v;
+            if (lj == s0 - 1 && have_carry) v = carry;
+            else if (lj >= pbeg && lj < beg)
+               v = ring_value(ring[w - 1], &done_end[w - 1], lj, g.out + c, g.status);
+            else v = wait_value(g.out + c, g.status);
             sext += a * v;
          }
          const double bi = cur.b, pv = cur.pv;
@@ -550,8 +629,15 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) solve_sweep(SolveArgs g)
          if (valid) {
             const int64_t row = FWD ? rho : n - 1 - rho;
             st_relaxed(g.out + row, zr);
+            ring[w][rho % kRing] = zr;
             if (g.reset) g.reset[row] = sentinel_value();
             if (g.dot_with) dotp += g.dot_with[row] * zr;
+         }
+         // publish the segment to the next warp of the band
+         __syncwarp();
+         if (lane == 0) {
+            __threadfence_block();
+            st_release_cta(&done_end[w], (long long)min(end, s0 + 32));
          }
          const int64_t last = min((int64_t)31, end - 1 - s0);
          carry = __shfl_sync(FULL, zr, (int)last);
@@ -737,11 +823,11 @@ void launch_solve(ofg_prec* P, SweepPlan& plan, SolveArgs g)
 {
    if (!plan.nstrands) return;
    OFG_CUDA(cudaMemsetAsync(plan.ticket.p, 0, 4 * sizeof(int), stream()));
-   int blocks = (int)std::min<int64_t>((plan.nstrands + kWarpsPerBlock - 1) / kWarpsPerBlock,
-                                       (int64_t)P->grid);
+   int blocks = (int)std::min<int64_t>((plan.nstrands + kBandWarps - 1) / kBandWarps,
+                                       (int64_t)P->solve_grid);
    if (blocks < 1) blocks = 1;
    g.worked = prof_begin();
-   solve_sweep<MODE><<<blocks, kWarpsPerBlock * 32, 0, stream()>>>(g);
+   solve_sweep<MODE><<<blocks, kBandWarps * 32, 0, stream()>>>(g);
    // algorithmic bytes: one triangle of the off-diagonal entries (FP64 value
    // + int32 column), the pivots, the input, the output and the reset
    const ofg_matrix* A = P->A;
@@ -832,6 +918,9 @@ void prec_setup(ofg_prec* P)
       OFG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_kernel<FWD_DILU>,
                                                              kWarpsPerBlock * 32, 0));
       P->grid = std::max(1, per_sm) * num_sms();
+      OFG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, solve_sweep<FWD_DILU>,
+                                                             kBandWarps * 32, 0));
+      P->solve_grid = std::max(1, per_sm) * num_sms();
       build_plan(A, true, P->fwd);
       build_plan(A, false, P->bwd);
       P->status.alloc(1);

@@ -57,12 +57,18 @@ def train(net, problems, rounds=8, steps=10, batch=16, lr=1e-3, npairs=64):
     return hist
 
 
-def train_default(seed=7, M=20, nproblems=4, rounds=8, dim=3):
+def train_default(seed=7, M=20, nproblems=None, rounds=None, dim=3):
     """The networks used by the benchmark: trained on `nproblems` problems
-    (seeds 100, 101, ...) -- 3-D: Kuhn cubes of M^3 cells with log-normal
-    conductivities (sigma 1.5, correlation length 0.1); 2-D: squares of
-    (6M + 8)^2 cells, alternately k = 1 and log-normal k (sigma 1).  Returns
+    (seeds 100, 101, ...) with 64 residual / error pairs each -- 3-D: 32
+    Kuhn cubes of M^3 cells, each with its own seeded log-normal
+    conductivity field (sigma 1.5, correlation length 0.1), 2048 pairs in
+    all, each problem visited twice; 2-D: 4 squares of (6M + 8)^2 cells,
+    alternately k = 1 and log-normal k (sigma 1), visited 8 times.  Returns
     (net, info)."""
+    if nproblems is None:
+        nproblems = 32 if dim == 3 else 4
+    if rounds is None:
+        rounds = 2 if dim == 3 else 8
     t0 = time.perf_counter()
     net = F.LearnedNet(seed)
     problems = []
@@ -78,7 +84,8 @@ def train_default(seed=7, M=20, nproblems=4, rounds=8, dim=3):
     what = ("%d Kuhn cubes %d^3 nodes, lognormal k (sigma 1.5)" % (nproblems, M + 1) if dim == 3
             else "%d squares %d^2 nodes, k = 1 and lognormal k (sigma 1)" % (nproblems, 6 * M + 9))
     info = {"train_s": time.perf_counter() - t0, "adam_steps": rounds * nproblems * 10,
-            "problems": what, "pairs_per_problem": 64, "loss_first": hist[0],
+            "problems": what, "pairs_per_problem": 64, "pairs": 64 * nproblems,
+            "loss_first": hist[0],
             "loss_last": hist[-1], "objective": "Kaporin number of M A on the pairs"}
     return net, info
 

@@ -821,6 +821,13 @@ class DC2DT3:
     def setDirichlet(self, bc):
         self._bc = _f64(bc, self.mesh.nn)
 
+    def getLinearSolver(self):
+        """Equa::getLinearSolver(): the solver the time steps of a
+        TimeStepping driver use (its tolerance and iteration cap)."""
+        if getattr(self, "_ls", None) is None:
+            self._ls = LinearSolver()
+        return self._ls
+
     def setTransient(self, scheme):
         """Equa::setTransient: FORWARD_EULER, BACKWARD_EULER or CRANK_NICOLSON."""
         if scheme not in (FORWARD_EULER, BACKWARD_EULER, CRANK_NICOLSON):
@@ -863,3 +870,87 @@ class DC2DT3:
                            inner_tol=inner_tol)
         _call("ofg_insert_bc", self.mesh._h, _ptr(self.x), _ptr(self._bc), _ptr(self.u))
         return out
+
+
+# OFELI's HEUN and NEWMARK values (include/equations/Equa.h:124-137)
+HEUN, NEWMARK = 4, 5
+
+
+class TimeStepping:
+    """OFELI's TimeStepping driver (src/solvers/TimeStepping.cpp) for a DC2DT3
+    equation under its first-order schemes, each step on the device:
+
+    * BACKWARD_EULER: build() of the backward-Euler system, then the
+      equation's LinearSolver (getLinearSolver(): tolerance, iteration cap;
+      the solver and preconditioner of setLinearSolver, GMRES restarting
+      every n/5 steps) from the previous step's solution, insertBC;
+    * CRANK_NICOLSON: the same with the Crank-Nicolson system;
+    * FORWARD_EULER: the explicit step x = b / D, D the assembled diagonal
+      (ofg_matrix_diag_solve), insertBC.
+
+    Each element matrix and right-hand side is the one OFELI's
+    AssembleBackwardEuler / AssembleCrankNicolson / AssembleForwardEuler
+    builds (:635-734), which for a zero source and zero Dirichlet data are
+    the Equa_Therm::build systems of setTransient, bit for bit.  As in
+    OFELI, set() tests the scheme with bitwise ANDs against HEUN and
+    NEWMARK (:141-170): FORWARD_EULER (1) and CRANK_NICOLSON (3) share a bit
+    with NEWMARK (5), so runOneTimeStep makes two sub-steps of time_step for
+    them and one for BACKWARD_EULER."""
+
+    def __init__(self, scheme, time_step, final_time=1.0):
+        if scheme not in (FORWARD_EULER, BACKWARD_EULER, CRANK_NICOLSON):
+            raise OFELIException("In TimeStepping::set(...): only the first-order schemes "
+                                 "(forward and backward Euler, Crank-Nicolson) are on this path")
+        self.scheme, self.time_step, self.final_time = scheme, time_step, final_time
+        self._nb_ssteps = 2 if (scheme & HEUN or scheme & NEWMARK) else 1
+        self._eq = None
+        self._s, self._p = None, None
+        self._step = 0
+
+    def setPDE(self, eq):
+        if not isinstance(eq, DC2DT3):
+            raise OFELIException("TimeStepping drives a DC2DT3 equation on this path")
+        self._eq = eq
+        eq.dt = self.time_step
+        eq.setTransient(self.scheme)
+
+    def setInitial(self, u):
+        self._eq.u = _f64(u, self._eq.mesh.nn).copy()
+
+    def setBC(self, bc):
+        self._eq.setDirichlet(bc)
+
+    def setLinearSolver(self, s=GMRES_SOLVER, p=DIAG_PREC):
+        self._s, self._p = s, p
+
+    def runOneTimeStep(self):
+        """One time step (the scheme's sub-steps); returns the time step."""
+        eq = self._eq
+        if eq is None:
+            raise OFELIException("TimeStepping: no equation (setPDE)")
+        if eq._bc is None:
+            eq.setDirichlet(np.zeros(eq.mesh.nn))
+        self._step += 1
+        ls = eq.getLinearSolver()
+        for _ in range(self._nb_ssteps):
+            A, b = eq.build()
+            if self.scheme == FORWARD_EULER:
+                _call("ofg_matrix_diag_solve", A._h, _ptr(b), _ptr(eq.x))
+            else:
+                ls.setMatrix(A)
+                ls.setRHS(b)
+                ls.setSolution(eq.x)
+                ls.solve(self._s if self._s is not None else GMRES_SOLVER,
+                         self._p if self._p is not None else DIAG_PREC)
+            _call("ofg_insert_bc", eq.mesh._h, _ptr(eq.x), _ptr(eq._bc), _ptr(eq.u))
+        return self.time_step
+
+    def run(self):
+        """Steps until final_time (TimeStepping::run)."""
+        t = 0.0
+        while t < self.final_time - 0.5 * self.time_step:
+            self.runOneTimeStep()
+            t += self.time_step
+
+    def getSolution(self):
+        return self._eq.u

@@ -169,8 +169,10 @@ def loss_and_grad(g, P, R, E, bf16=True, kind=1):
     for l in range(NLAYER - 1, -1, -1):
         dz = dH * (f["z"][l + 1] > 0)
         c = f["cat"][l]
-        grad[P_W + l * 2 * HID * HID:P_W + (l + 1) * 2 * HID * HID] = (c.T @ dz).ravel()
-        grad[P_B + l * HID:P_B + (l + 1) * HID] = dz.sum(0)
+        # the weight and bias gradients, like the data product, take dz in
+        # BF16 (the GPU's tensor-core operand)
+        grad[P_W + l * 2 * HID * HID:P_W + (l + 1) * 2 * HID * HID] = (c.T @ rb(dz)).ravel()
+        grad[P_B + l * HID:P_B + (l + 1) * HID] = rb(dz).sum(0)
         dcat = rb(dz) @ rb(p["W"][l]).T
         dH = dH + dcat[:, :HID] + g.Atil @ dcat[:, HID:]
     dz0 = dH * (f["z"][0] > 0)

@@ -8,6 +8,7 @@
 //   ofeli_ref p2d  NX NY   SOLVER PREC TOL MAXIT INDIR OUTDIR
 //   ofeli_ref p3d  M       SOLVER PREC TOL MAXIT INDIR OUTDIR
 //   ofeli_ref cd2d NX NY   NSTEPS DT EPS SOLVER PREC TOL MAXIT INDIR OUTDIR [BE|FE|CN]
+//   ofeli_ref ts2d NX NY   NSTEPS DT EPS BE|FE|CN SOLVER PREC TOL MAXIT INDIR OUTDIR
 //   ofeli_ref mget FILE INDIR OUTDIR            (Mesh::get, dump, Mesh::put)
 //   ofeli_ref mrect NX NY CX0 CXN CY0 CYN INDIR OUTDIR  (Mesh(rect), dump, put)
 //   ofeli_ref mlap FILE SOLVER PREC TOL MAXIT INDIR OUTDIR
@@ -33,6 +34,8 @@
 //   Equa_Laplace::build, Equa_Therm::build          include/equations/laplace/Equa_Laplace.h:112-133,
 //                                                   include/equations/therm/Equa_Therm.h:162-218
 //   Mesh::get / Mesh::put                           src/mesh/Mesh.cpp:2639-2668, 2731-2806
+//   TimeStepping (setPDE, setInitial, setBC, setLinearSolver, runOneTimeStep)
+//                                                   src/solvers/TimeStepping.cpp:141-250,341-460
 //   Prec<real_t>(A,type), CG(A,P,b,x,..), GMRes(A,P,b,x,m,..)
 //                                                   include/solvers/{Prec.h,CG.h:99-157,GMRes.h:148-241}
 #include "OFELI.h"
@@ -566,6 +569,71 @@ int run_cd2d(int argc, char** argv)
    return 0;
 }
 
+// DC2DT3 steps driven by OFELI's TimeStepping class (src/solvers/
+// TimeStepping.cpp): setPDE, setInitial, setBC (a zero vector: without one,
+// TimeStepping::insertBC assigns the equation-space solution to the nodal
+// field), setLinearSolver, runOneTimeStep per step.  The linear solves are
+// the equation's LinearSolver (GMRES restarts every n/5 steps) with the
+// given tolerance; forward Euler is explicit (lumped diagonal).  Writes the
+// nodal field after every step (u_steps.f64) and the solver's iteration
+// count per step.
+int run_ts2d(int argc, char** argv)
+{
+   if (argc < 14) return 2;
+   size_t nx = std::stoul(argv[2]), ny = std::stoul(argv[3]);
+   int nsteps = std::stoi(argv[4]);
+   double dt = std::stod(argv[5]), eps = std::stod(argv[6]);
+   std::string sc = argv[7], solver = argv[8];
+   Preconditioner prec = parse_prec(argv[9]);
+   double tol = std::stod(argv[10]);
+   int maxit = std::stoi(argv[11]);
+   std::string in = argv[12], out = argv[13];
+   Info info;
+   TimeScheme scheme = sc == "FE" ? FORWARD_EULER : sc == "CN" ? CRANK_NICOLSON : BACKWARD_EULER;
+   Iteration it_kind = solver == "CG" ? CG_SOLVER
+                       : solver == "BICGSTAB" ? BICG_STAB_SOLVER : GMRES_SOLVER;
+
+   Mesh ms(0., 1., 0., 1., nx, ny, 1, 1, 1, 1, TRIANGLE);
+   size_t nn = ms.getNbNodes();
+   std::vector<double> u0 = read_f64(in + "/u0.f64", nn);
+   std::vector<double> vv = read_f64(in + "/v.f64", 2 * nn);
+   Vect<real_t> u(ms), v(2 * nn), bc(ms);
+   for (size_t i = 0; i < nn; ++i) u[i] = u0[i];
+   for (size_t i = 0; i < 2 * nn; ++i) v[i] = vv[i];
+   bc = 0;
+   KDC2DT3 eq(ms, u);
+   eq.eps = eps;
+   eq.setSolver(it_kind, prec);
+   eq.getLinearSolver().setTolerance(tol);
+   eq.getLinearSolver().setMaxIter(maxit);
+   eq.setTerms(PDE_Terms::CAPACITY);
+   eq.setTerms(PDE_Terms::CONVECTION);
+   eq.setInput(EType::VELOCITY, v);
+   TimeStepping ts(scheme, dt, nsteps * dt);
+   ts.setPDE(eq);
+   ts.setInitial(u);
+   ts.setBC(bc);
+   ts.setLinearSolver(it_kind, prec);
+   std::vector<double> steps;
+   std::vector<int> its;
+   double t0 = now_s();
+   for (int s = 0; s < nsteps; ++s) {
+      ts.runOneTimeStep();
+      its.push_back(scheme == FORWARD_EULER ? 0 : eq.getLinearSolver().getNbIter());
+      for (size_t i = 0; i < nn; ++i) steps.push_back(u[i]);
+   }
+   double t_steps = now_s() - t0;
+   write_bin(out + "/u_steps.f64", steps.data(), steps.size());
+   write_bin(out + "/iters.i32", its.data(), its.size());
+   info.seti("nodes", (long long)nn);
+   info.seti("steps", nsteps);
+   info.set("t_steps", t_steps);
+   info.set("norm_u", u.getNorm2());
+   info.sets("scheme", sc);
+   info.write(out);
+   return 0;
+}
+
 // The data a Mesh keeps (coords, codes, 1-based element / side node labels)
 // and Mesh::put of it.
 void dump_mesh(Mesh& ms, const std::string& out, Info& info)
@@ -731,6 +799,7 @@ int main(int argc, char** argv)
       if (mode == "p2d") return run_p2d(argc, argv);
       if (mode == "p3d") return run_p3d(argc, argv);
       if (mode == "cd2d") return run_cd2d(argc, argv);
+      if (mode == "ts2d") return run_ts2d(argc, argv);
       if (mode == "bench2d") return run_bench2d(argc, argv);
       if (mode == "mget") return run_mget(argc, argv);
       if (mode == "mrect") return run_mrect(argc, argv);

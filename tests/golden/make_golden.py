@@ -269,6 +269,28 @@ def case_meshio():
     save("meshio", arrays, meta)
 
 
+def case_ts2d():
+    """OFELI's TimeStepping class driving DC2DT3 on the 17x17-node transient
+    problem of case_cd2d (eps 1e-3, v = (-(y-0.5), x-0.5), Gaussian bump,
+    u = 0 on the boundary): 5 runOneTimeStep calls of dt 1e-3 under forward
+    Euler, backward Euler and Crank-Nicolson, GMRES + ILU to 1e-10 for the
+    implicit schemes; the nodal field after every call."""
+    nx, steps, dt, eps = 16, 5, 1e-3, 1e-3
+    xy, elem, code = O.mesh2d(nx, nx)
+    P = xy.reshape(-1, 2)
+    u0 = np.exp(-((P[:, 0] - 0.3) ** 2 + (P[:, 1] - 0.5) ** 2) / (2 * 0.05 ** 2))
+    u0[code > 0] = 0.0
+    v = np.stack([-(P[:, 1] - 0.5), P[:, 0] - 0.5], axis=1).reshape(-1)
+    arrays, meta = {}, {"nx": nx, "steps": steps, "dt": dt, "eps": eps, "tol": 1e-10,
+                        "solver": "GMRES", "prec": "ILU"}
+    for sc in ("FE", "BE", "CN"):
+        info, out = O.run_reference(["ts2d", nx, nx, steps, dt, eps, sc, "GMRES", "ILU", 1e-10,
+                                     2000], {"u0": u0, "v": v})
+        arrays[sc + "_u_steps"] = out["u_steps"].reshape(steps, -1)
+        arrays[sc + "_iters"] = out["iters"]
+    save("ts2d_17", arrays, meta)
+
+
 def _sample_pins(x, stride):
     return {"x_norm2": float(np.linalg.norm(x)), "x_sum": float(x.sum()),
             "x_sample_stride": stride}, {"x_sample": x[::stride].copy()}
@@ -357,3 +379,4 @@ if __name__ == "__main__":
     case_bicgstab()
     case_meshio()
     case_cd2d_schemes()
+    case_ts2d()

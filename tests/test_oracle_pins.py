@@ -203,3 +203,38 @@ def test_cd2d_schemes_bit_exact(name):
         u = O.insert_bc(code, x)
     assert its == list(g[name + "_iters"])
     assert np.array_equal(u, g[name + "_u"])
+
+
+@pytest.mark.parametrize("name", ["FE", "BE", "CN"])
+def test_timestepping_bit_exact(name):
+    """OFELI's TimeStepping class driving DC2DT3 (src/solvers/TimeStepping.cpp)
+    restated from the Equa_Therm systems: forward Euler is x = b / diag(A),
+    the implicit schemes the equation's LinearSolver (GMRES restarting every
+    n/5 steps, warm start); forward Euler and Crank-Nicolson make two
+    sub-steps per call (the scheme tests of TimeStepping::set).  Every
+    step's field equals the reference's bit for bit."""
+    g, info = load_golden("ts2d_17")
+    nx, dt, eps = info["nx"], info["dt"], info["eps"]
+    scheme = {"FE": 1, "BE": 2, "CN": 3}[name]
+    xy, elem, code = O.mesh2d(nx, nx)
+    P = xy.reshape(-1, 2)
+    u = np.exp(-((P[:, 0] - 0.3) ** 2 + (P[:, 1] - 0.5) ** 2) / (2 * 0.05 ** 2))
+    u[code > 0] = 0.0
+    v = np.stack([-(P[:, 1] - 0.5), P[:, 0] - 0.5], axis=1).reshape(-1)
+    dof, n = O.number_equations(code)
+    rp, ci = O.node_graph(elem, 3, dof, n)
+    dpos = np.array([rp[r] + np.nonzero(ci[rp[r]:rp[r + 1]] - 1 == r)[0][0] for r in range(n)])
+    x = np.zeros(n)
+    substeps = 1 if name == "BE" else 2
+    for s in range(info["steps"]):
+        for _ in range(substeps):
+            a, b = O.assemble_cd2d(xy, elem, dof, code, n, rp, ci, eps, v, dt, u,
+                                   bc=np.zeros(code.size), scheme=scheme)
+            if name == "FE":
+                x = b / a[dpos]
+            else:
+                x, it = O.gmres(rp.astype(np.int64), ci.astype(np.int64), a, b, O.ILU, n // 5,
+                                2000, info["tol"], x0=x)
+                assert it > 0
+            u = O.insert_bc(code, x)
+        assert np.array_equal(u, g[name + "_u_steps"][s])
