@@ -279,8 +279,32 @@ def run_reference(args):
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
             "wall_s": wall}
+    pin = reference_full_run(nx)
+    if pin:
+        line["reference_full_run"] = pin
     print(json.dumps(line))
     return 0
+
+
+def reference_full_run(nx):
+    """OFELI's own CG + ILU on this problem run to convergence (the committed
+    pin, measured where the reference was built: -O2, one core), beside the
+    per-step model: the model's extrapolated solve against that measured
+    one."""
+    if nx != 2048:
+        return None
+    try:
+        z = np.load(os.path.join(HERE, "tests", "golden", "p2d_2049_pins.npz"))
+        info = json.loads(str(z["info"]))
+    except (OSError, KeyError, ValueError):
+        return None
+    return {"source": "tests/golden/p2d_2049_pins.npz", "build": "-O2, 1 thread",
+            "iterations": info["iters"], "graph_s": info["t_graph_cpu_o2_s"],
+            "assembly_s": info["t_assembly_cpu_o2_s"], "solve_s": info["t_solve_cpu_o2_s"],
+            "solve_s_per_iteration": info["t_solve_cpu_o2_s"] / info["iters"],
+            "note": "measured to convergence once; the timed steps above are bounded samples "
+                    "(build + Prec + a few iterations, -Ofast) extrapolated to this "
+                    "iteration count"}
 
 
 # --------------------------------------------------------------- our arm ----

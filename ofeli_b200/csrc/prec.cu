@@ -438,6 +438,23 @@ __device__ __forceinline__ void load_segment(const SolveArgs& g, int64_t s, int6
 // same either way, so the results are bit for bit those of the global path.
 constexpr int kBandWarps = 16;
 constexpr int kRing = 256;
+// A segment step waits for the slot data of the next segment (loaded one
+// segment ahead into registers); left to come from DRAM that wait is a full
+// DRAM latency per step.  The slot data of the segment kPrefetch ahead is
+// therefore pulled into L2 first (one bulk prefetch per array, issued by
+// lane 0: a strand's segments are contiguous in the slot layout), and its
+// right-hand side and pivots likewise, one row per lane.
+constexpr int kPrefetch = 4;
+
+__device__ __forceinline__ void prefetch_l2_bulk(const void* p, uint32_t bytes)
+{
+   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void prefetch_l2(const void* p)
+{
+   asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
 constexpr long long kSpinSmemFast = 1 << 14;
 constexpr long long kSpinSmemSlow = 1 << 22;  // x ~0.5 us sleep: a few seconds at most
 
@@ -521,6 +538,21 @@ __global__ void __launch_bounds__(kBandWarps * 32, 1) solve_sweep(SolveArgs g)
       load_segment<FWD>(g, sfirst, beg, end, lane, cur);
       for (int64_t s = sfirst; s < slast; ++s) {
          const int64_t s0 = beg + 32 * (s - sfirst);
+         if (s + kPrefetch < slast) {
+            const int64_t rp = s0 + 32 * kPrefetch + lane;
+            if (lane == 0) {
+               const int32_t o0 = g.seg_off[s + kPrefetch], o1 = g.seg_off[s + kPrefetch + 1];
+               if (o1 > o0) {
+                  prefetch_l2_bulk(g.sl_col + o0, (uint32_t)(o1 - o0) * 4u);
+                  prefetch_l2_bulk(g.sl_val + o0, (uint32_t)(o1 - o0) * 8u);
+               }
+            }
+            if (rp < end) {
+               const int64_t row = FWD ? rp : n - 1 - rp;
+               prefetch_l2(g.in + row);
+               prefetch_l2(g.piv + row);
+            }
+         }
          if (s + 1 < slast) load_segment<FWD>(g, s + 1, s0 + 32, end, lane, nxt);
          const int64_t rho = s0 + lane;
          const bool valid = rho < end;

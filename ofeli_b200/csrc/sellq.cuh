@@ -73,11 +73,11 @@ __device__ __forceinline__ float4 raw_f4(const uint2 u)
 
 // Positions whose values a thread loads before its first product in a
 // uniform slice (BF16 values; half as many FP32 values).
-constexpr int kHoist = 4;
+constexpr int kHoist = 1;
 // Resident 256-thread blocks per SM of the SELL product kernels (their
 // register budget: 65536 / (256 * kQuadBlocks)), and the grid of the
 // kernel chains they are part of.
-constexpr int kQuadBlocks = 6;
+constexpr int kQuadBlocks = 8;
 
 // The four rows r0 .. r0+3 of a uniform slice: w positions, the offset of
 // position k from tp[k].  The values of kHoist positions are loaded before
