@@ -79,7 +79,7 @@ def parse():
                          "cost (strong scaling) instead of one replica of it per rank")
     ap.add_argument("--batch-bits", type=int, default=32, choices=[32, 64],
                     help="batch2d: inner CG precision (32: FP32 CG inside FP64 refinement)")
-    ap.add_argument("--tprec", default="LEARNED", choices=["ILU", "DIAG", "MIXED", "LEARNED"],
+    ap.add_argument("--tprec", default="MIXED", choices=["ILU", "DIAG", "MIXED", "LEARNED"],
                     help="transient2d: solver of the timed steps -- ILU / DIAG: FP64 GMRES(30) "
                          "(OFELI's GMRes) with that preconditioner; MIXED / LEARNED: the "
                          "mixed-precision flexible GMRES(30) (FP32 products, FP64 Gram-Schmidt "
@@ -1086,11 +1086,11 @@ def run_transient(args):
     u_timed = trajectory(11) if rank == 0 and not args.no_plain else None
     # the plain form (OFELI's GMRES(30) + ILU) over 10 steps from the same
     # initial state, and FP64 GMRES(30) + DIAG likewise
-    plain, fp64_diag, err = None, None, None
+    plain, fp64_diag, err, learned_form = None, None, None, None
 
-    def time_fp64(p):
+    def time_fp64(p, mixed_form=False):
         nonlocal prec, Pc, mixed
-        prec, Pc, mixed = p, None, False
+        prec, Pc, mixed = p, None, mixed_form
         u_dev.copy_(torch.from_numpy(u0).to(dev))
         x_dev.zero_()
         del its[:]
@@ -1113,6 +1113,19 @@ def run_transient(args):
         if args.tprec != "DIAG":
             fp64_diag, _ = time_fp64(F.DIAG_PREC)
             fp64_diag["solver"] = "GMRES(30) + DIAG, FP64, warm start (OFELI's GMRes order)"
+        if args.tprec != "LEARNED":
+            # the learned preconditioner in the same mixed FGMRES (trained
+            # here, outside any timed region; factor computed on the first
+            # step's matrix and kept)
+            from ofeli_b200 import learned as LN
+            net, tinfo = LN.train_transient()
+            learned_form, u_l = time_fp64(F.LEARNED_PREC, mixed_form=True)
+            learned_form["solver"] = ("mixed-precision flexible GMRES(30) + learned M = G^T G, "
+                                      "converged on the FP64 true residual")
+            learned_form["training"] = tinfo
+            learned_form["err_vs_fp64_ilu"] = (float(np.linalg.norm(u_l - u_ilu) /
+                                                     np.linalg.norm(u_ilu))
+                                               if plain else None)
     if rank != 0:
         R.close()
         return 0
@@ -1169,6 +1182,7 @@ def run_transient(args):
                      "family_ms_sampled": shares},
         "plain": plain,
         "fp64_gmres_diag": fp64_diag,
+        "learned_fgmres": learned_form,
         "cpu_baseline": cpu,
         "clocks": clk,
     }

@@ -85,6 +85,7 @@ struct SweepPlan {
    // stored column-major (slot k of lane l at seg_off[s] + 32 k + l), in
    // the CSR's column order
    int64_t nseg = 0;
+   int wmax = 0;              // slots of the widest segment
    DBuf<int32_t> tseg;        // first segment of each strand, nstrands+1
    DBuf<int32_t> seg_off;     // nseg+1
    DBuf<int32_t> sl_col;      // physical column, -1 for padding

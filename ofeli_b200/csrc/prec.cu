@@ -370,7 +370,8 @@ __global__ void transpose_positions(int64_t n, const int32_t* rp, const int32_t*
 // layout.  Per segment a lane holds one row: its dependency slots (column,
 // value) arrive as coalesced lines, the next segment's slots, b and pivot
 // are fetched while the current segment waits for its earlier-row values.
-constexpr int kSlots = 8;  // slots held in registers; wider rows take a slow loop
+// A lane holds 4 or 8 slots in registers (the plan's widest segment); rows
+// wider than 8 take a slow loop.
 
 struct SolveArgs {
    int64_t n;
@@ -393,55 +394,31 @@ struct SolveArgs {
    int* worked;
 };
 
-struct SegRegs {
-   int32_t off, w;
-   int32_t c[kSlots];
-   double a[kSlots];
-   double b, pv;
-};
-
-template <bool FWD>
-__device__ __forceinline__ void load_segment(const SolveArgs& g, int64_t s, int64_t s0, int64_t end,
-                                             int lane, SegRegs& R)
-{
-   R.off = g.seg_off[s];
-   R.w = (g.seg_off[s + 1] - R.off) >> 5;
-#pragma unroll
-   for (int k = 0; k < kSlots; ++k) {
-      R.c[k] = -1;
-      R.a[k] = 0.0;
-      if (k < R.w) {
-         R.c[k] = g.sl_col[R.off + k * 32 + lane];
-         R.a[k] = g.sl_val[R.off + k * 32 + lane];
-      }
-   }
-   const int64_t rho = s0 + lane;
-   R.b = 0.0;
-   R.pv = 1.0;
-   if (rho < end) {
-      const int64_t row = FWD ? rho : g.n - 1 - rho;
-      R.b = g.in[row];
-      R.pv = g.piv[row];
-   }
-}
-
 // Band hand-off.  A block takes a band of kBandWarps consecutive strands,
 // one warp each.  Besides storing its results to global memory (for the
 // strands of other blocks), a warp keeps the latest kRing of them in a
 // shared-memory ring and publishes how far it got (done_end: the logical
 // row one past its last finished segment) with a CTA-scope release; the
-// next warp of the band takes the values of the previous strand from the
-// ring, with an acquire, instead of waiting for them to travel through L2.
-// The ring is only a faster path: when the producer may already have
-// overwritten a slot (it ran more than kRing - 32 rows ahead), the value is
-// read from global memory, where it was stored first.  The arithmetic is the
-// same either way, so the results are bit for bit those of the global path.
+// next warp of the band waits once per segment, with an acquire, until the
+// rows of the previous strand that the segment needs are published, and
+// reads them from the ring instead of waiting for them to travel through
+// L2.  The ring is only a faster path: when the producer may have
+// overwritten a slot (it ran more than kRing - 32 rows ahead, checked
+// before and after the reads), the segment takes those values from global
+// memory, where they were stored first.  The arithmetic is the same either
+// way, so the results are bit for bit those of the global path.
+//
+// A segment step is a dependent chain (wait, gather, scan, publish) that
+// one warp executes; the step is kept short: the register slots are sized
+// to the plan's widest segment (NS = 4 or 8), indices are 32-bit, and the
+// previous strand is waited for once per segment.
 constexpr int kBandWarps = 16;
 constexpr int kRing = 256;
+constexpr long long kSpinSmemFast = 1 << 14;
+constexpr long long kSpinSmemSlow = 1 << 22;  // x ~0.5 us sleep: a few seconds at most
 // A segment step waits for the slot data of the next segment (loaded one
-// segment ahead into registers); left to come from DRAM that wait is a full
-// DRAM latency per step.  The slot data of the segment kPrefetch ahead is
-// therefore pulled into L2 first (one bulk prefetch per array, issued by
+// segment ahead into registers); the slot data of the segment kPrefetch
+// ahead is pulled into L2 first (one bulk prefetch per array, issued by
 // lane 0: a strand's segments are contiguous in the slot layout), and its
 // right-hand side and pivots likewise, one row per lane.
 constexpr int kPrefetch = 4;
@@ -455,91 +432,115 @@ __device__ __forceinline__ void prefetch_l2(const void* p)
 {
    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
-constexpr long long kSpinSmemFast = 1 << 14;
-constexpr long long kSpinSmemSlow = 1 << 22;  // x ~0.5 us sleep: a few seconds at most
 
-__device__ __forceinline__ long long ld_acquire_cta(const long long* p)
+__device__ __forceinline__ int ld_acquire_cta(const int* p)
 {
-   long long v;
-   asm volatile("ld.acquire.cta.shared.s64 %0, [%1];"
-                : "=l"(v)
+   int v;
+   asm volatile("ld.acquire.cta.shared.s32 %0, [%1];"
+                : "=r"(v)
                 : "r"((unsigned)__cvta_generic_to_shared(p))
                 : "memory");
    return v;
 }
 
-__device__ __forceinline__ void st_release_cta(long long* p, long long v)
+__device__ __forceinline__ void st_release_cta(int* p, int v)
 {
-   asm volatile("st.release.cta.shared.s64 [%0], %1;" ::"r"((unsigned)__cvta_generic_to_shared(p)),
-                "l"(v)
+   asm volatile("st.release.cta.shared.s32 [%0], %1;" ::"r"((unsigned)__cvta_generic_to_shared(p)),
+                "r"(v)
                 : "memory");
 }
 
-// Value of logical row lj of the previous strand of the band (warp w - 1):
-// from the ring once its producer published it, else (waited too long, or
-// possibly overwritten) from global memory with the bounded wait.
-__device__ __noinline__ double ring_value(const double* ring, const long long* done_end,
-                                          long long lj, const double* gsrc, int* status)
+// waits (bounded) until *done_end > need; returns the value seen, or -1
+// when the wait ran out (status set)
+__device__ __noinline__ int wait_published(const int* done_end, int need, int* status)
 {
-   long long de = ld_acquire_cta(done_end);
-   for (long long it = 0; de <= lj; ++it) {
+   int de = ld_acquire_cta(done_end);
+   for (long long it = 0; de <= need; ++it) {
       if (it >= kSpinSmemFast + kSpinSmemSlow) {
          atomicOr(status, 1);
-         return wait_value_slow(gsrc, status);
+         return -1;
       }
       if (it >= kSpinSmemFast) __nanosleep(500);
       de = ld_acquire_cta(done_end);
    }
-   if (de - lj < kRing - 32) {
-      const double v = *(volatile const double*)(ring + (lj % kRing));
-      __threadfence_block();
-      const long long de2 = *(volatile const long long*)done_end;
-      if (de2 - lj < kRing - 32) return v;
-   }
-   return wait_value(gsrc, status);
+   return de;
 }
 
-template <int MODE>
+template <int NS>
+struct SegRegs {
+   int32_t off, w;
+   int32_t c[NS];
+   double a[NS];
+   double b, pv;
+};
+
+template <bool FWD, int NS>
+__device__ __forceinline__ void load_segment(const SolveArgs& g, int64_t s, int32_t s0, int32_t end,
+                                             int lane, SegRegs<NS>& R)
+{
+   R.off = g.seg_off[s];
+   R.w = (g.seg_off[s + 1] - R.off) >> 5;
+#pragma unroll
+   for (int k = 0; k < NS; ++k) {
+      R.c[k] = -1;
+      R.a[k] = 0.0;
+      if (k < R.w) {
+         R.c[k] = g.sl_col[R.off + k * 32 + lane];
+         R.a[k] = g.sl_val[R.off + k * 32 + lane];
+      }
+   }
+   const int32_t rho = s0 + lane;
+   R.b = 0.0;
+   R.pv = 1.0;
+   if (rho < end) {
+      const int32_t row = FWD ? rho : (int32_t)g.n - 1 - rho;
+      R.b = g.in[row];
+      R.pv = g.piv[row];
+   }
+}
+
+template <int MODE, int NS>
 __global__ void __launch_bounds__(kBandWarps * 32, 1) solve_sweep(SolveArgs g)
 {
    constexpr bool FWD = (MODE == FWD_DILU || MODE == FWD_SSOR);
    __shared__ double segv[kBandWarps][32];
    __shared__ double ring[kBandWarps][kRing];
-   __shared__ long long done_end[kBandWarps];
-   __shared__ long long band_sh;
+   __shared__ int done_end[kBandWarps];
+   __shared__ int band_sh;
    const int lane = threadIdx.x & 31;
    const int w = threadIdx.x >> 5;
    const unsigned FULL = 0xffffffffu;
-   const int64_t n = g.n;
+   const int32_t n = (int32_t)g.n;
    if (g.skip && *g.skip) return;
    prof_mark(g.worked);
-   const int64_t nbands = (g.nstrands + kBandWarps - 1) / kBandWarps;
+   const int nbands = (int)((g.nstrands + kBandWarps - 1) / kBandWarps);
 
    for (;;) {
       // every warp finished the previous band: the rings are free
       __syncthreads();
       if (threadIdx.x == 0) band_sh = atomicAdd(&g.ticket[0], 1);
       __syncthreads();
-      const int64_t band = band_sh;
+      const int band = band_sh;
       if (band >= nbands) break;
-      const int64_t t = band * kBandWarps + w;
+      const int64_t t = (int64_t)band * kBandWarps + w;
       const bool active = t < g.nstrands;
-      const int64_t beg = active ? g.sstart[t] : 0, end = active ? g.sstart[t + 1] : 0;
+      const int32_t beg = active ? g.sstart[t] : 0, end = active ? g.sstart[t + 1] : 0;
       // the previous strand is this block's warp w - 1 (rows pbeg .. beg-1)
-      const int64_t pbeg = (active && w > 0) ? g.sstart[t - 1] : beg;
+      const int32_t pbeg = (active && w > 0) ? g.sstart[t - 1] : beg;
       if (lane == 0) done_end[w] = beg;
       __syncthreads();
       if (!active) continue;
+      const int* prev_done = &done_end[w > 0 ? w - 1 : 0];
       const int64_t sfirst = g.tseg[t], slast = g.tseg[t + 1];
       double carry = 0.0;
       bool have_carry = false;
       double dotp = 0.0;
-      SegRegs cur, nxt;
-      load_segment<FWD>(g, sfirst, beg, end, lane, cur);
+      SegRegs<NS> cur, nxt;
+      load_segment<FWD, NS>(g, sfirst, beg, end, lane, cur);
       for (int64_t s = sfirst; s < slast; ++s) {
-         const int64_t s0 = beg + 32 * (s - sfirst);
+         const int32_t s0 = beg + 32 * (int32_t)(s - sfirst);
          if (s + kPrefetch < slast) {
-            const int64_t rp = s0 + 32 * kPrefetch + lane;
+            const int32_t rp = s0 + 32 * kPrefetch + lane;
             if (lane == 0) {
                const int32_t o0 = g.seg_off[s + kPrefetch], o1 = g.seg_off[s + kPrefetch + 1];
                if (o1 > o0) {
@@ -548,60 +549,86 @@ __global__ void __launch_bounds__(kBandWarps * 32, 1) solve_sweep(SolveArgs g)
                }
             }
             if (rp < end) {
-               const int64_t row = FWD ? rp : n - 1 - rp;
+               const int32_t row = FWD ? rp : n - 1 - rp;
                prefetch_l2(g.in + row);
                prefetch_l2(g.piv + row);
             }
          }
-         if (s + 1 < slast) load_segment<FWD>(g, s + 1, s0 + 32, end, lane, nxt);
-         const int64_t rho = s0 + lane;
+         if (s + 1 < slast) load_segment<FWD, NS>(g, s + 1, s0 + 32, end, lane, nxt);
+         const int32_t rho = s0 + lane;
          const bool valid = rho < end;
-         // earlier-row values of other blocks' strands: all loads issued,
-         // then consumed in slot order
-         double z[kSlots];
+         // logical rows of the slots; other blocks' strands are loaded now
+         // (consumed in slot order below), the previous strand's rows are
+         // waited for once for the whole segment
+         int32_t lj[NS];
+         double z[NS];
+         int need = -1, low = INT32_MAX;
 #pragma unroll
-         for (int k = 0; k < kSlots; ++k) {
-            z[k] = 0.0;
+         for (int k = 0; k < NS; ++k) {
             const int32_t c = cur.c[k];
-            if (c >= 0) {
-               const int64_t lj = FWD ? c : n - 1 - c;
-               if (lj < pbeg) z[k] = ld_relaxed(g.out + c);
+            lj[k] = c < 0 ? -1 : (FWD ? c : n - 1 - c);
+            z[k] = 0.0;
+            if (c >= 0 && lj[k] < pbeg) z[k] = ld_relaxed(g.out + c);
+            if (lj[k] >= pbeg && lj[k] < beg) {
+               need = max(need, lj[k]);
+               low = min(low, lj[k]);
             }
+         }
+         bool from_ring = false;
+         need = __reduce_max_sync(FULL, need);
+         if (need >= 0) {
+            low = __reduce_min_sync(FULL, low);
+            const int de = wait_published(prev_done, need, g.status);
+            from_ring = de > need && de - low < kRing - 32;
          }
          double sext = 0.0, m1 = 0.0;
          bool other_intra = false;
 #pragma unroll
-         for (int k = 0; k < kSlots; ++k) {
+         for (int k = 0; k < NS; ++k) {
             const int32_t c = cur.c[k];
             if (c < 0) continue;
-            const int64_t lj = FWD ? c : n - 1 - c;
-            if (lj >= s0) {
-               if (lj == rho - 1) m1 = cur.a[k];
+            if (lj[k] >= s0) {
+               if (lj[k] == rho - 1) m1 = cur.a[k];
                else other_intra = true;
                continue;
             }
             double v;
-            if (lj == s0 - 1 && have_carry) v = carry;
-            else if (lj >= beg) v = wait_value(g.out + c, g.status);  // own strand, earlier segment
-            else if (lj >= pbeg) v = ring_value(ring[w - 1], &done_end[w - 1], lj, g.out + c, g.status);
+            if (lj[k] == s0 - 1 && have_carry) v = carry;
+            else if (lj[k] >= beg) v = wait_value(g.out + c, g.status);  // own strand, earlier segment
+            else if (lj[k] >= pbeg)
+               v = from_ring ? ring[w - 1][lj[k] & (kRing - 1)] : wait_value(g.out + c, g.status);
             else v = is_sentinel(z[k]) ? wait_value_slow(g.out + c, g.status) : z[k];
             sext += cur.a[k] * v;
          }
-         for (int k = kSlots; k < cur.w; ++k) {  // rows wider than the register slots
+         if (from_ring) {
+            // the ring slots read must still hold those rows
+            __threadfence_block();
+            const int de2 = *(volatile const int*)prev_done;
+            if (de2 - low >= kRing - 32) {
+               sext = 0.0;
+#pragma unroll
+               for (int k = 0; k < NS; ++k) {
+                  const int32_t c = cur.c[k];
+                  if (c < 0 || lj[k] >= s0) continue;
+                  double v;
+                  if (lj[k] == s0 - 1 && have_carry) v = carry;
+                  else if (lj[k] >= pbeg) v = wait_value(g.out + c, g.status);
+                  else v = is_sentinel(z[k]) ? wait_value_slow(g.out + c, g.status) : z[k];
+                  sext += cur.a[k] * v;
+               }
+            }
+         }
+         for (int k = NS; k < cur.w; ++k) {  // rows wider than the register slots
             const int32_t c = g.sl_col[cur.off + k * 32 + lane];
             if (c < 0) continue;
             const double a = g.sl_val[cur.off + k * 32 + lane];
-            const int64_t lj = FWD ? c : n - 1 - c;
-            if (lj >= s0) {
-               if (lj == rho - 1) m1 = a;
+            const int32_t l = FWD ? c : n - 1 - c;
+            if (l >= s0) {
+               if (l == rho - 1) m1 = a;
                else other_intra = true;
                continue;
             }
-            double v;
-            if (lj == s0 - 1 && have_carry) v = carry;
-            else if (lj >= pbeg && lj < beg)
-               v = ring_value(ring[w - 1], &done_end[w - 1], lj, g.out + c, g.status);
-            else v = wait_value(g.out + c, g.status);
+            const double v = (l == s0 - 1 && have_carry) ? carry : wait_value(g.out + c, g.status);
             sext += a * v;
          }
          const double bi = cur.b, pv = cur.pv;
@@ -640,9 +667,9 @@ __global__ void __launch_bounds__(kBandWarps * 32, 1) solve_sweep(SolveArgs g)
                   for (int k = 0; k < cur.w && ready; ++k) {
                      const int32_t c = g.sl_col[cur.off + k * 32 + lane];
                      if (c < 0) continue;
-                     const int64_t lj = FWD ? c : n - 1 - c;
-                     if (lj < s0) continue;
-                     const double v = segv[w][lj - s0];
+                     const int32_t l = FWD ? c : n - 1 - c;
+                     if (l < s0) continue;
+                     const double v = segv[w][l - s0];
                      if (is_sentinel(v)) { ready = false; break; }
                      acc += g.sl_val[cur.off + k * 32 + lane] * v;
                   }
@@ -659,9 +686,9 @@ __global__ void __launch_bounds__(kBandWarps * 32, 1) solve_sweep(SolveArgs g)
             if (!__all_sync(FULL, done) && lane == 0) atomicOr(g.status, 2);
          }
          if (valid) {
-            const int64_t row = FWD ? rho : n - 1 - rho;
+            const int32_t row = FWD ? rho : n - 1 - rho;
             st_relaxed(g.out + row, zr);
-            ring[w][rho % kRing] = zr;
+            ring[w][rho & (kRing - 1)] = zr;
             if (g.reset) g.reset[row] = sentinel_value();
             if (g.dot_with) dotp += g.dot_with[row] * zr;
          }
@@ -669,10 +696,10 @@ __global__ void __launch_bounds__(kBandWarps * 32, 1) solve_sweep(SolveArgs g)
          __syncwarp();
          if (lane == 0) {
             __threadfence_block();
-            st_release_cta(&done_end[w], (long long)min(end, s0 + 32));
+            st_release_cta(&done_end[w], min(end, s0 + 32));
          }
-         const int64_t last = min((int64_t)31, end - 1 - s0);
-         carry = __shfl_sync(FULL, zr, (int)last);
+         const int last = min(31, end - 1 - s0);
+         carry = __shfl_sync(FULL, zr, last);
          have_carry = true;
          if (s + 1 < slast) cur = nxt;
       }
@@ -795,6 +822,9 @@ void build_plan(ofg_matrix* A, bool fwd, SweepPlan& plan)
       tseg[t + 1] = (int32_t)(seg_off.size() - 1);
    }
    const int64_t nslot = seg_off.back();
+   plan.wmax = 0;
+   for (size_t q = 0; q + 1 < seg_off.size(); ++q)
+      plan.wmax = std::max(plan.wmax, (seg_off[q + 1] - seg_off[q]) / 32);
    OFG_REQUIRE(nslot < (int64_t(1) << 31), OFG_ERR_PATTERN, "sweep layout exceeds 2^31 slots");
    std::vector<int32_t> slc(nslot > 0 ? nslot : 1, -1), sls(nslot > 0 ? nslot : 1, -1);
    for (int64_t t = 0, s = 0; t < plan.nstrands; ++t) {
@@ -859,7 +889,9 @@ void launch_solve(ofg_prec* P, SweepPlan& plan, SolveArgs g)
                                        (int64_t)P->solve_grid);
    if (blocks < 1) blocks = 1;
    g.worked = prof_begin();
-   solve_sweep<MODE><<<blocks, kBandWarps * 32, 0, stream()>>>(g);
+   // register slots sized to the plan's widest segment
+   if (plan.wmax <= 4) solve_sweep<MODE, 4><<<blocks, kBandWarps * 32, 0, stream()>>>(g);
+   else solve_sweep<MODE, 8><<<blocks, kBandWarps * 32, 0, stream()>>>(g);
    // algorithmic bytes: one triangle of the off-diagonal entries (FP64 value
    // + int32 column), the pivots, the input, the output and the reset
    const ofg_matrix* A = P->A;
@@ -950,7 +982,7 @@ void prec_setup(ofg_prec* P)
       OFG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_kernel<FWD_DILU>,
                                                              kWarpsPerBlock * 32, 0));
       P->grid = std::max(1, per_sm) * num_sms();
-      OFG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, solve_sweep<FWD_DILU>,
+      OFG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, solve_sweep<FWD_DILU, 8>,
                                                              kBandWarps * 32, 0));
       P->solve_grid = std::max(1, per_sm) * num_sms();
       build_plan(A, true, P->fwd);

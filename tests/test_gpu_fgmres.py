@@ -144,14 +144,18 @@ def test_learned_fgmres_frozen_across_steps(transient_net):
 
 
 def test_learned_fgmres_falls_back(cuda):
-    """A network whose factor is not finite (a NaN parameter, injected on
-    the host): the solve notices the residual is not falling, finishes with
-    the diagonal preconditioner and reports it."""
+    """A network whose factor is not finite (NaN off-diagonal head weights,
+    injected on the host): the solve notices the residual is not finite,
+    finishes with the diagonal preconditioner and reports it.  (A NaN in the
+    diagonal's offset c only drives the diagonal to its floor: a tiny
+    multiple of a valid preconditioner, to which the right-preconditioned
+    FGMRES is indifferent.)"""
+    from oracle import learned_oracle as LO
     g, info = load_golden("cd2d_17")
     A = F.SpMatrix(g["row_ptr"], g["col_ind"], g["a0"])
     net = F.LearnedNet(3)
     p, m1, m2, st = net.get_params()
-    p[-1] = np.nan
+    p[LO.P_U:LO.P_V] = np.nan
     net.set_params(p, m1, m2, st)
     x = np.zeros(A.n)
     cycles, steps, res, fell_back = F.fgmres_mixed(F.Prec(A, F.LEARNED_PREC, net=net), g["b0"], x,
