@@ -439,7 +439,7 @@ def measure(args, wl, R, work_stream, dev, world, rank, with_cpu=True):
         learned = dict(train_info)
         learned.update({
             "network_forward_ms": net_ms,
-            "layer_gemm": {"kernel": "gemm_tc (tcgen05.mma kind::f16, BF16 -> FP32 in TMEM)",
+            "layer_gemm": {"kernel": "gemm_tc_tma (TMA-fed A tiles, two stages; tcgen05.mma kind::f16, BF16 -> FP32 in TMEM)",
                            "launches": g_cnt, "avg_us": g_us,
                            "GB/s": (g_bytes / max(g_cnt, 1)) / (g_us * 1e-6) / 1e9 if g_cnt else None,
                            "TFLOP/s": g_flops / (g_us * 1e-6) / 1e12 if g_cnt else None},

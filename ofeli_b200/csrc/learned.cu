@@ -38,6 +38,8 @@
 // gradient X^T dZ (a reduction over all rows: the rows are the MMA's K)
 // runs on the tensor cores too (wgrad_tc), from the BF16 copy of dZ that
 // the data product uses.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -465,6 +467,201 @@ __global__ void __launch_bounds__(128, 4) gemm_tc(int64_t rows, GemmA a,
                    : "memory");
 }
 
+// The forward layer product [h | agg] W (K = 128, N = 64) with the A tiles
+// brought in by the tensor memory accelerator and two stages in flight.
+// Each 128-row tile of A arrives as sixteen 2-D boxes of {8 elements, 128
+// rows} (one per 8-column chunk of h or agg), so box c lands as chunk c of
+// gemm_tc's K-major core-matrix layout (2048 bytes: row m at m*16).  Per
+// tile k of the block: thread 0 issues the TMA loads of tile k+2 into the
+// stage the MMAs of tile k have just released and the MMAs of tile k+1 (into
+// the other tensor-memory accumulator), then all threads run the epilogue
+// of tile k.  So the loads, the MMAs and the epilogue of three tiles
+// overlap.  Loads complete on a `full` mbarrier per stage (transaction
+// count), MMAs commit to a `done` mbarrier per stage; every wait is bounded,
+// and a block whose wait ran out drains what it issued before it returns.
+// The tensor maps cover this GPU's own buffers only; no multicast.
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y,
+                                            uint32_t mbar)
+{
+   asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, "
+      "%3}], [%4];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(mbar)
+      : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes)
+{
+   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes)
+                : "memory");
+}
+
+template <class Epi>
+__global__ void __launch_bounds__(128, 2) gemm_tc_tma(int64_t rows,
+                                                      const __grid_constant__ CUtensorMap t0,
+                                                      const __grid_constant__ CUtensorMap t1,
+                                                      const bf16* __restrict__ Bt, Epi epi,
+                                                      int* status, int* worked)
+{
+   constexpr int K = 2 * HID, N = HID;
+   constexpr uint32_t kTileBytes = 128 * K * 2;  // 32 KB
+   prof_mark(worked);
+   extern __shared__ __align__(1024) unsigned char smem[];
+   unsigned char* sA = smem;                    // two stages of kTileBytes
+   unsigned char* sB = smem + 2 * kTileBytes;   // N*K*2 bytes
+   uint64_t* bars = reinterpret_cast<uint64_t*>(sB + N * K * 2);  // full[2], done[2]
+   uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 4);
+   __shared__ int fail_sh;
+   const int tid = threadIdx.x, warp = tid >> 5;
+
+   for (int piece = tid; piece < N * K / 8; piece += 128) {
+      const int nr = piece % N, c = piece / N;
+      const uint4 v = *reinterpret_cast<const uint4*>(Bt + (int64_t)nr * K + c * 8);
+      *reinterpret_cast<uint4*>(sB + c * N * 16 + nr * 16) = v;
+   }
+   if (tid == 0) {
+      for (int q = 0; q < 4; ++q)
+         asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bars + q)), "r"(1)
+                      : "memory");
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      fail_sh = 0;
+   }
+   if (warp == 0) {
+      asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                      smem_u32(tslot)),
+                   "r"(2 * N)
+                   : "memory");
+      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+   }
+   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+   __syncthreads();
+   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+   const uint32_t tmem = *tslot;
+   const uint32_t sa = smem_u32(sA), sb = smem_u32(sB);
+   constexpr uint32_t idesc = instr_desc_bf16_f32<N>();
+   const int64_t ntiles = (rows + 127) / 128;
+   const int64_t mine = blockIdx.x < ntiles ? (ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+   auto full = [&](int s) { return smem_u32(bars + s); };
+   auto done = [&](int s) { return smem_u32(bars + 2 + s); };
+   // thread 0 only
+   auto issue_load = [&](int64_t k) {
+      const int s = (int)(k & 1);
+      const int y = (int)((blockIdx.x + k * gridDim.x) * 128);
+      const uint32_t dst = sa + s * kTileBytes;
+      mbar_expect_tx(full(s), kTileBytes);
+#pragma unroll
+      for (int c = 0; c < K / 8; ++c)
+         tma_load_2d(dst + c * 2048, c < 8 ? &t0 : &t1, (c & 7) * 8, y, full(s));
+   };
+   auto issue_mma = [&](int64_t k) {
+      const int s = (int)(k & 1);
+      const uint32_t a0 = sa + s * kTileBytes;
+#pragma unroll
+      for (int kk = 0; kk < K / 16; ++kk) {
+         const uint64_t ad = smem_desc(a0 + kk * 2 * 2048, 2048, 128);
+         const uint64_t bd = smem_desc(sb + kk * 2 * N * 16, N * 16, 128);
+         const uint32_t acc = kk > 0 ? 1u : 0u;
+         asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+               tmem + (uint32_t)(s * N)),
+            "l"(ad), "l"(bd), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0)
+            : "memory");
+      }
+      asm volatile(
+         "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(done(s))
+         : "memory");
+   };
+   // loads issued and waited for, per stage (for the drain after a failure)
+   int64_t loads_issued = 0, loads_waited = 0, mmas_issued = 0, mmas_waited = 0;
+   bool failed = false;
+   if (tid == 0 && mine > 0) {
+      issue_load(0);
+      loads_issued = 1;
+      if (mine > 1) {
+         issue_load(1);
+         loads_issued = 2;
+      }
+      if (mbar_wait(full(0), 0)) {
+         loads_waited = 1;
+         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+         issue_mma(0);
+         mmas_issued = 1;
+      }
+      else {
+         fail_sh = 1;
+      }
+   }
+   __syncthreads();
+   failed = fail_sh != 0;
+   for (int64_t k = 0; k < mine && !failed; ++k) {
+      const int s = (int)(k & 1);
+      // MMAs of tile k finished: its accumulator is ready, its stage free
+      if (__syncthreads_or(mbar_wait(done(s), (uint32_t)((k >> 1) & 1)) ? 0 : 1)) {
+         failed = true;
+         if (tid == 0) atomicOr(status, 1);
+         break;
+      }
+      if (tid == 0) mmas_waited = k + 1;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      if (tid == 0) {
+         if (k + 2 < mine) {
+            issue_load(k + 2);
+            loads_issued = k + 3;
+         }
+         if (k + 1 < mine) {
+            if (mbar_wait(full((int)((k + 1) & 1)), (uint32_t)(((k + 1) >> 1) & 1))) {
+               loads_waited = k + 2;
+               asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+               issue_mma(k + 1);
+               mmas_issued = k + 2;
+            }
+            else {
+               fail_sh = 1;
+               atomicOr(status, 1);
+            }
+         }
+      }
+      // epilogue of tile k from its accumulator
+      const int64_t row = (blockIdx.x + k * gridDim.x) * 128 + warp * 32 + (tid & 31);
+#pragma unroll
+      for (int cb = 0; cb < N; cb += 16) {
+         uint32_t r[16];
+         const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(s * N + cb);
+         asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, "
+            "%10, %11, %12, %13, %14, %15}, [%16];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+              "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+              "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+            : "r"(taddr));
+         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+         float v[16];
+#pragma unroll
+         for (int q = 0; q < 16; ++q) v[q] = __uint_as_float(r[q]);
+         if (row < rows) epi(row, cb, v);
+      }
+      // every thread is done with accumulator s before MMAs reuse it
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncthreads();
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      failed = fail_sh != 0;
+   }
+   // after a wait that ran out: drain what was issued (bounded waits)
+   if (failed && tid == 0) {
+      for (int64_t q = loads_waited; q < loads_issued; ++q)
+         mbar_wait(full((int)(q & 1)), (uint32_t)((q >> 1) & 1));
+      for (int64_t q = mmas_waited; q < mmas_issued; ++q)
+         mbar_wait(done((int)(q & 1)), (uint32_t)((q >> 1) & 1));
+   }
+   __syncthreads();
+   if (warp == 0)
+      asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * N)
+                   : "memory");
+}
+
 // Weight gradient on the tensor cores: part[block] = X^T dz over the
 // block's 128-row tiles, X = [h | agg] (rows x 128, BF16) and dz (rows x 64,
 // BF16).  The reduction runs over the rows, so the rows are the MMA's K:
@@ -800,10 +997,68 @@ static void graph_prepare(ofg_matrix* A, LearnedGraph& G, bool train)
    OFG_LAUNCH_CHECK();
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the
+// library does not link the driver library itself)
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+   if (!fn) {
+      void* p = nullptr;
+      cudaDriverEntryPointQueryResult q;
+      OFG_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+      OFG_REQUIRE(q == cudaDriverEntryPointSuccess && p, OFG_ERR_CUDA,
+                  "cuTensorMapEncodeTiled is not available");
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+   }
+   return fn;
+}
+
+// 2-D map of a rows x 64 BF16 block with row stride ld elements, boxes of
+// {8 elements, 128 rows} (rows past the end read as zeros)
+static CUtensorMap half_map(const bf16* base, int64_t rows, int64_t ld)
+{
+   OFG_REQUIRE(((uintptr_t)base & 15) == 0 && (ld * 2) % 16 == 0, OFG_ERR_ARG,
+               "layer operand not 16-byte aligned");
+   CUtensorMap m;
+   cuuint64_t dims[2] = {(cuuint64_t)HID, (cuuint64_t)rows};
+   cuuint64_t strides[1] = {(cuuint64_t)(ld * 2)};
+   cuuint32_t box[2] = {8, 128};
+   cuuint32_t estr[2] = {1, 1};
+   const CUresult r = tensor_map_encoder()(
+      &m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<bf16*>(base), dims, strides, box, estr,
+      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+   OFG_REQUIRE(r == CUDA_SUCCESS, OFG_ERR_CUDA,
+               "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+   return m;
+}
+
 template <int K, int N, class Epi>
 static void run_gemm(ofg_learned* L, int64_t rows, GemmA a, const bf16* Bt, Epi epi)
 {
    if (rows <= 0) return;
+   if constexpr (K == 2 * HID && N == HID) {
+      if (L->use_tc && a.k0 == HID && rows < (int64_t(1) << 31)) {
+         // the forward product: TMA-fed, two stages in flight
+         constexpr int smem = 2 * 128 * K * 2 + N * K * 2 + 64;
+         static bool attr_set = false;
+         if (!attr_set) {
+            OFG_CUDA(cudaFuncSetAttribute(gemm_tc_tma<Epi>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            attr_set = true;
+         }
+         const CUtensorMap t0 = half_map(a.a0, rows, a.lda0), t1 = half_map(a.a1, rows, a.lda1);
+         const int64_t tiles = (rows + 127) / 128;
+         const unsigned grid = (unsigned)std::min<int64_t>(tiles, (int64_t)num_sms() * 2);
+         int* worked = prof_begin();
+         gemm_tc_tma<Epi><<<grid, 128, smem, stream()>>>(rows, t0, t1, Bt, epi, L->status.p,
+                                                         worked);
+         prof_end(PROF_NET_GEMM, (double)rows * (K * 2 + N * Epi::kBytesPerCol) + (double)N * K * 2);
+         count_launch();
+         OFG_LAUNCH_CHECK();
+         return;
+      }
+   }
    if (L->use_tc) {
       // at least 48 KB of shared memory per block caps residency at four
       // blocks per SM, so the tensor-memory allocations (<= 128 columns
