@@ -671,19 +671,24 @@ def _batch_cpu_worker(jobs, barrier, out):
     out.put((t0, time.time(), work))
 
 
-def cpu_parallel_batch(sizes, w_all, per_core=2):
+def cpu_parallel_batch(sizes, w_all, per_core=4):
     """N = host cores single-threaded oracle-port processes at once, each
-    on its own problems of an evenly spaced sample of the batch
-    (`per_core` per process); the batch extrapolated by the parallel wall
-    time per (nonzeros x iterations) of the sample."""
+    on its own problems of an evenly spaced sample of the batch (`per_core`
+    per process on average, largest first to the least loaded process by
+    the estimated cost nx^3, so that no process idles long); the batch
+    extrapolated by the parallel wall time per (nonzeros x iterations) of
+    the sample."""
     import multiprocessing as mp
     cores = os.cpu_count() or 1
     order = np.argsort(sizes)
     m = min(len(sizes), cores * per_core)
     pick = order[np.linspace(0, len(order) - 1, m).astype(int)]
     jobs = [[] for _ in range(cores)]
-    for q, p in enumerate(pick):
-        jobs[q % cores].append((int(sizes[p]), SEED * 7919 + int(p)))
+    load = [0.0] * cores
+    for p in sorted(pick, key=lambda q: -int(sizes[q])):
+        c = int(np.argmin(load))
+        jobs[c].append((int(sizes[p]), SEED * 7919 + int(p)))
+        load[c] += float(sizes[p]) ** 3
     ctx = mp.get_context("spawn")
     barrier = ctx.Barrier(cores)
     out = ctx.Queue()
