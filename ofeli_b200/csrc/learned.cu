@@ -222,11 +222,13 @@ struct GemmA {
 // Epilogue of a forward layer, 16 columns of one row at a time:
 // z = acc + b; h_new = relu(z) + h_old (BF16); z kept when asked for.
 struct FwdFunctor {
-   static constexpr int kBytesPerCol = 6;  // h_old read, h_new written (BF16); z if kept
    const float* bias;
    const bf16* h_old;
    bf16* z;  // may be null
    bf16* h_new;
+   // h_new written, and z when kept (BF16); h_old, read too, is the first
+   // half of the A operand and counted there
+   int bytes_per_col() const { return z ? 4 : 2; }
    __device__ __forceinline__ void operator()(int64_t row, int c0, const float* v) const
    {
       float ho[16], zz[16], hh[16];
@@ -248,8 +250,8 @@ struct FwdFunctor {
 
 // Epilogue of the backward data product: dcat (FP32, 128 columns).
 struct BwdFunctor {
-   static constexpr int kBytesPerCol = 4;
    float* dcat;
+   int bytes_per_col() const { return 4; }
    __device__ __forceinline__ void operator()(int64_t row, int c0, const float* v) const
    {
       float4* o = reinterpret_cast<float4*>(dcat + row * 2 * HID + c0);
@@ -259,9 +261,9 @@ struct BwdFunctor {
 };
 
 struct StoreFunctor {  // plain FP32 store, for the product check
-   static constexpr int kBytesPerCol = 4;
    float* out;
    int ld;
+   int bytes_per_col() const { return 4; }
    __device__ __forceinline__ void operator()(int64_t row, int c0, const float* v) const
    {
       float4* o = reinterpret_cast<float4*>(out + row * ld + c0);
@@ -1053,7 +1055,7 @@ static void run_gemm(ofg_learned* L, int64_t rows, GemmA a, const bf16* Bt, Epi 
          int* worked = prof_begin();
          gemm_tc_tma<Epi><<<grid, 128, smem, stream()>>>(rows, t0, t1, Bt, epi, L->status.p,
                                                          worked);
-         prof_end(PROF_NET_GEMM, (double)rows * (K * 2 + N * Epi::kBytesPerCol) + (double)N * K * 2);
+         prof_end(PROF_NET_GEMM, (double)rows * (K * 2 + N * epi.bytes_per_col()) + (double)N * K * 2);
          count_launch();
          OFG_LAUNCH_CHECK();
          return;
@@ -1076,7 +1078,7 @@ static void run_gemm(ofg_learned* L, int64_t rows, GemmA a, const bf16* Bt, Epi 
       gemm_tc<K, N, Epi><<<grid, 128, smem, stream()>>>(rows, a, Bt, epi, L->status.p, worked);
       // algorithmic bytes: the A operand, the weights, and the epilogue's
       // own reads and writes per output column
-      prof_end(PROF_NET_GEMM, (double)rows * (K * 2 + N * Epi::kBytesPerCol) + (double)N * K * 2);
+      prof_end(PROF_NET_GEMM, (double)rows * (K * 2 + N * epi.bytes_per_col()) + (double)N * K * 2);
    }
    else {
       gemm_cc<K, N, Epi><<<grid_for(rows * (N / 16), 256), 256, 0, stream()>>>(rows, a, Bt, epi);
