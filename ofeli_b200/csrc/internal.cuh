@@ -91,6 +91,11 @@ struct SweepPlan {
    DBuf<int32_t> sl_col;      // physical column, -1 for padding
    DBuf<int32_t> sl_src;      // CSR index of the value, -1 for padding
    DBuf<double> sl_val;
+   // per segment: the lowest row of the previous strand that this or a
+   // later segment of its strand reads from the band's shared-memory ring
+   // (INT32_MAX: none); the solve sweeps publish it so that the previous
+   // strand's warp never overwrites a ring slot still to be read
+   DBuf<int32_t> seg_keep;
 };
 }  // namespace ofg
 

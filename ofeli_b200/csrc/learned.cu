@@ -47,6 +47,7 @@
 #include <vector>
 
 #include "internal.cuh"
+#include "mbar.cuh"
 #include "reduce.cuh"
 
 typedef __nv_bfloat16 bf16;
@@ -322,30 +323,6 @@ __host__ __device__ constexpr uint32_t instr_desc_bf16_f32()
    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((128u >> 4) << 24);
 }
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p)
-{
-   return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-constexpr long long kMbarSpin = 1LL << 26;
-
-// waits for the given phase of an mbarrier, at most kMbarSpin polls
-__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t phase)
-{
-   for (long long spins = 0; spins < kMbarSpin; ++spins) {
-      uint32_t done;
-      asm volatile(
-         "{\n\t.reg .pred P1;\n\t"
-         "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
-         "selp.b32 %0, 1, 0, P1;\n\t}\n"
-         : "=r"(done)
-         : "r"(addr), "r"(phase)
-         : "memory");
-      if (done) return true;
-   }
-   return false;
-}
-
 template <int K, int N, class Epi>
 __global__ void __launch_bounds__(128, 4) gemm_tc(int64_t rows, GemmA a,
                                                   const bf16* __restrict__ Bt, Epi epi, int* status,
@@ -490,12 +467,6 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
       "%3}], [%4];" ::"r"(dst),
       "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(mbar)
       : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes)
-{
-   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes)
-                : "memory");
 }
 
 template <class Epi>

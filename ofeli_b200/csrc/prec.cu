@@ -392,6 +392,7 @@ struct SolveArgs {
    int* status;
    const int* skip;
    int* worked;
+   const int32_t* seg_keep;
 };
 
 // Band hand-off.  A block takes a band of kBandWarps consecutive strands,
@@ -402,14 +403,26 @@ struct SolveArgs {
 // next warp of the band waits once per segment, with an acquire, until the
 // rows of the previous strand that the segment needs are published, and
 // reads them from the ring instead of waiting for them to travel through
-// L2.  The ring is only a faster path: when the producer may have
-// overwritten a slot (it ran more than kRing - 32 rows ahead, checked
-// before and after the reads), the segment takes those values from global
-// memory, where they were stored first.  The arithmetic is the same either
-// way, so the results are bit for bit those of the global path.
+// L2.  A segment reads the ring when the lowest previous-strand row its
+// register slots need is within kRing / 2 of the highest such row needed
+// by it or an earlier segment of its strand (a property of the plan);
+// otherwise it reads them from global memory.  Every warp also publishes
+// keep_from: the lowest previous-strand row that it, or a later segment of
+// its strand, still reads from the ring (the plan's seg_keep); before
+// writing a segment into its ring, a warp waits (bounded) until its
+// consumer's keep_from is past the rows those slots held.  That wait always
+// ends: while the consumer waits for a row r, every ring row it will still
+// read is above r - kRing / 2, below what the producer overwrites before
+// publishing r.  The arithmetic is the same on either path, so the results
+// are bit for bit equal.
 //
-// A segment step is a dependent chain (wait, gather, scan, publish) that
-// one warp executes; the step is kept short: the register slots are sized
+// The time of a sweep is about (strands) x (the part of a segment step
+// between the previous strand's publish and this strand's), so that part
+// is kept short: everything that does not depend on the previous strand
+// (the other slots' values, the coupling to the row before, the
+// multiplicative half of the affine scan, the consumer check) is done
+// before the wait, the ring is read without a branch, and the ring and
+// the release go out before the global copy.  The register slots are sized
 // to the plan's widest segment (NS = 4 or 8), indices are 32-bit, and the
 // previous strand is waited for once per segment.
 constexpr int kBandWarps = 16;
@@ -420,7 +433,7 @@ constexpr long long kSpinSmemSlow = 1 << 22;  // x ~0.5 us sleep: a few seconds 
 // segment ahead into registers); the slot data of the segment kPrefetch
 // ahead is pulled into L2 first (one bulk prefetch per array, issued by
 // lane 0: a strand's segments are contiguous in the slot layout), and its
-// right-hand side and pivots likewise, one row per lane.
+// right-hand side, pivots and dot_with entries likewise, one row per lane.
 constexpr int kPrefetch = 4;
 
 __device__ __forceinline__ void prefetch_l2_bulk(const void* p, uint32_t bytes)
@@ -468,10 +481,10 @@ __device__ __noinline__ int wait_published(const int* done_end, int need, int* s
 
 template <int NS>
 struct SegRegs {
-   int32_t off, w;
+   int32_t off, w, keep;
    int32_t c[NS];
    double a[NS];
-   double b, pv;
+   double b, pv, dw;  // dw: the row's entry of dot_with (0 without)
 };
 
 template <bool FWD, int NS>
@@ -480,6 +493,7 @@ __device__ __forceinline__ void load_segment(const SolveArgs& g, int64_t s, int3
 {
    R.off = g.seg_off[s];
    R.w = (g.seg_off[s + 1] - R.off) >> 5;
+   R.keep = g.seg_keep[s];
 #pragma unroll
    for (int k = 0; k < NS; ++k) {
       R.c[k] = -1;
@@ -492,10 +506,12 @@ __device__ __forceinline__ void load_segment(const SolveArgs& g, int64_t s, int3
    const int32_t rho = s0 + lane;
    R.b = 0.0;
    R.pv = 1.0;
+   R.dw = 0.0;
    if (rho < end) {
       const int32_t row = FWD ? rho : (int32_t)g.n - 1 - rho;
       R.b = g.in[row];
       R.pv = g.piv[row];
+      if (g.dot_with) R.dw = g.dot_with[row];
    }
 }
 
@@ -506,6 +522,7 @@ __global__ void __launch_bounds__(kBandWarps * 32, 1) solve_sweep(SolveArgs g)
    __shared__ double segv[kBandWarps][32];
    __shared__ double ring[kBandWarps][kRing];
    __shared__ int done_end[kBandWarps];
+   __shared__ int keep_from[kBandWarps];
    __shared__ int band_sh;
    const int lane = threadIdx.x & 31;
    const int w = threadIdx.x >> 5;
@@ -527,9 +544,15 @@ __global__ void __launch_bounds__(kBandWarps * 32, 1) solve_sweep(SolveArgs g)
       const int32_t beg = active ? g.sstart[t] : 0, end = active ? g.sstart[t + 1] : 0;
       // the previous strand is this block's warp w - 1 (rows pbeg .. beg-1)
       const int32_t pbeg = (active && w > 0) ? g.sstart[t - 1] : beg;
-      if (lane == 0) done_end[w] = beg;
+      if (lane == 0) {
+         done_end[w] = beg;
+         keep_from[w] = active ? g.seg_keep[g.tseg[t]] : INT32_MAX;
+      }
       __syncthreads();
       if (!active) continue;
+      // the next strand of the band, which reads this warp's ring
+      const bool has_consumer = w + 1 < kBandWarps && t + 1 < g.nstrands;
+      int run_need = -1;  // highest previous-strand row needed so far
       const int* prev_done = &done_end[w > 0 ? w - 1 : 0];
       const int64_t sfirst = g.tseg[t], slast = g.tseg[t + 1];
       double carry = 0.0;
@@ -552,103 +575,124 @@ __global__ void __launch_bounds__(kBandWarps * 32, 1) solve_sweep(SolveArgs g)
                const int32_t row = FWD ? rp : n - 1 - rp;
                prefetch_l2(g.in + row);
                prefetch_l2(g.piv + row);
+               if (g.dot_with) prefetch_l2(g.dot_with + row);
             }
          }
          if (s + 1 < slast) load_segment<FWD, NS>(g, s + 1, s0 + 32, end, lane, nxt);
          const int32_t rho = s0 + lane;
          const bool valid = rho < end;
-         // logical rows of the slots; other blocks' strands are loaded now
-         // (consumed in slot order below), the previous strand's rows are
-         // waited for once for the whole segment
+         // Before the wait: the values of the slots that do not come from
+         // the previous strand (the carry, this strand's earlier segments,
+         // other blocks' strands), the coupling to the row before (m1) and
+         // the multiplicative half of the segment scan.  Once the previous
+         // strand's rows are published, only their reads, the slot sum, the
+         // additive half of the scan and the publish remain on the chain
+         // that runs from strand to strand.
          int32_t lj[NS];
-         double z[NS];
+         double pre[NS];
+         bool from_prev[NS];
          int need = -1, low = INT32_MAX;
-#pragma unroll
-         for (int k = 0; k < NS; ++k) {
-            const int32_t c = cur.c[k];
-            lj[k] = c < 0 ? -1 : (FWD ? c : n - 1 - c);
-            z[k] = 0.0;
-            if (c >= 0 && lj[k] < pbeg) z[k] = ld_relaxed(g.out + c);
-            if (lj[k] >= pbeg && lj[k] < beg) {
-               need = max(need, lj[k]);
-               low = min(low, lj[k]);
-            }
-         }
-         bool from_ring = false;
-         need = __reduce_max_sync(FULL, need);
-         if (need >= 0) {
-            low = __reduce_min_sync(FULL, low);
-            const int de = wait_published(prev_done, need, g.status);
-            from_ring = de > need && de - low < kRing - 32;
-         }
-         double sext = 0.0, m1 = 0.0;
+         double m1 = 0.0;
          bool other_intra = false;
 #pragma unroll
          for (int k = 0; k < NS; ++k) {
             const int32_t c = cur.c[k];
+            lj[k] = c < 0 ? -1 : (FWD ? c : n - 1 - c);
+            pre[k] = 0.0;
+            from_prev[k] = false;
             if (c < 0) continue;
             if (lj[k] >= s0) {
                if (lj[k] == rho - 1) m1 = cur.a[k];
                else other_intra = true;
-               continue;
             }
-            double v;
-            if (lj[k] == s0 - 1 && have_carry) v = carry;
-            else if (lj[k] >= beg) v = wait_value(g.out + c, g.status);  // own strand, earlier segment
-            else if (lj[k] >= pbeg)
-               v = from_ring ? ring[w - 1][lj[k] & (kRing - 1)] : wait_value(g.out + c, g.status);
-            else v = is_sentinel(z[k]) ? wait_value_slow(g.out + c, g.status) : z[k];
-            sext += cur.a[k] * v;
-         }
-         if (from_ring) {
-            // the ring slots read must still hold those rows
-            __threadfence_block();
-            const int de2 = *(volatile const int*)prev_done;
-            if (de2 - low >= kRing - 32) {
-               sext = 0.0;
-#pragma unroll
-               for (int k = 0; k < NS; ++k) {
-                  const int32_t c = cur.c[k];
-                  if (c < 0 || lj[k] >= s0) continue;
-                  double v;
-                  if (lj[k] == s0 - 1 && have_carry) v = carry;
-                  else if (lj[k] >= pbeg) v = wait_value(g.out + c, g.status);
-                  else v = is_sentinel(z[k]) ? wait_value_slow(g.out + c, g.status) : z[k];
-                  sext += cur.a[k] * v;
-               }
+            else if (lj[k] == s0 - 1 && have_carry) pre[k] = carry;
+            else if (lj[k] >= beg) pre[k] = wait_value(g.out + c, g.status);  // own strand
+            else if (lj[k] >= pbeg) {
+               from_prev[k] = true;
+               need = max(need, lj[k]);
+               low = min(low, lj[k]);
             }
+            else pre[k] = wait_value(g.out + c, g.status);  // another block's strand
          }
          for (int k = NS; k < cur.w; ++k) {  // rows wider than the register slots
             const int32_t c = g.sl_col[cur.off + k * 32 + lane];
             if (c < 0) continue;
-            const double a = g.sl_val[cur.off + k * 32 + lane];
             const int32_t l = FWD ? c : n - 1 - c;
             if (l >= s0) {
-               if (l == rho - 1) m1 = a;
+               if (l == rho - 1) m1 = g.sl_val[cur.off + k * 32 + lane];
                else other_intra = true;
-               continue;
             }
+         }
+         const bool affine = !__any_sync(FULL, other_intra);
+         const double bi = cur.b, pv = cur.pv;
+         double Mr[5];  // M of the scan at the start of each round
+         if (affine) {
+            double M;
+            if (MODE == FWD_DILU || MODE == BWD_DILU) M = -pv * m1;
+            else M = -m1 / pv;
+            if (!valid || lane == 0) M = 0.0;
+#pragma unroll
+            for (int r = 0; r < 5; ++r) {
+               Mr[r] = M;
+               const double Mp = __shfl_up_sync(FULL, M, 1 << r);
+               if (lane >= (1 << r)) M = M * Mp;
+            }
+         }
+         // the consumer no longer reads the ring slots this segment overwrites
+         if (has_consumer && ld_acquire_cta(&keep_from[w + 1]) <= s0 + 31 - kRing)
+            wait_published(&keep_from[w + 1], s0 + 31 - kRing, g.status);
+         bool from_ring = false;
+         need = __reduce_max_sync(FULL, need);
+         run_need = max(run_need, need);
+         if (need >= 0) {
+            low = __reduce_min_sync(FULL, low);
+            int de = ld_acquire_cta(prev_done);
+            for (int q = 0; q < 32 && de <= need; ++q) de = ld_acquire_cta(prev_done);
+            if (de <= need) de = wait_published(prev_done, need, g.status);
+            from_ring = de > need && run_need - low < kRing / 2;
+         }
+         double sext = 0.0;
+         if (from_ring) {
+            // every slot reads the ring (the empty ones a harmless slot) and
+            // selects: no branch between the wait and the sum
+            double rv[NS];
+#pragma unroll
+            for (int k = 0; k < NS; ++k) rv[k] = ring[w - 1][lj[k] & (kRing - 1)];
+#pragma unroll
+            for (int k = 0; k < NS; ++k) {
+               if (cur.c[k] < 0 || lj[k] >= s0) continue;
+               sext += cur.a[k] * (from_prev[k] ? rv[k] : pre[k]);
+            }
+         }
+         else {
+#pragma unroll
+            for (int k = 0; k < NS; ++k) {
+               if (cur.c[k] < 0 || lj[k] >= s0) continue;
+               const double v = from_prev[k] ? wait_value(g.out + cur.c[k], g.status) : pre[k];
+               sext += cur.a[k] * v;
+            }
+         }
+         for (int k = NS; k < cur.w; ++k) {
+            const int32_t c = g.sl_col[cur.off + k * 32 + lane];
+            if (c < 0) continue;
+            const int32_t l = FWD ? c : n - 1 - c;
+            if (l >= s0) continue;
+            const double a = g.sl_val[cur.off + k * 32 + lane];
             const double v = (l == s0 - 1 && have_carry) ? carry : wait_value(g.out + c, g.status);
             sext += a * v;
          }
-         const double bi = cur.b, pv = cur.pv;
          double zr;
-         if (!__any_sync(FULL, other_intra)) {
-            double C, M;
-            if (MODE == FWD_DILU) { C = pv * (bi - sext); M = -pv * m1; }
-            else if (MODE == FWD_SSOR) { C = (bi - sext) / pv; M = -m1 / pv; }
-            else if (MODE == BWD_DILU) { C = bi - pv * sext; M = -pv * m1; }
-            else { C = bi - sext / pv; M = -m1 / pv; }
-            if (!valid) { C = 0.0; M = 0.0; }
-            if (lane == 0) M = 0.0;
+         if (affine) {
+            double C;
+            if (MODE == FWD_DILU) C = pv * (bi - sext);
+            else if (MODE == FWD_SSOR) C = (bi - sext) / pv;
+            else if (MODE == BWD_DILU) C = bi - pv * sext;
+            else C = bi - sext / pv;
+            if (!valid) C = 0.0;
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-               const double Cp = __shfl_up_sync(FULL, C, o);
-               const double Mp = __shfl_up_sync(FULL, M, o);
-               if (lane >= o) {
-                  C = C + M * Cp;
-                  M = M * Mp;
-               }
+            for (int r = 0; r < 5; ++r) {
+               const double Cp = __shfl_up_sync(FULL, C, 1 << r);
+               if (lane >= (1 << r)) C = C + Mr[r] * Cp;
             }
             zr = C;
          }
@@ -685,18 +729,22 @@ __global__ void __launch_bounds__(kBandWarps * 32, 1) solve_sweep(SolveArgs g)
             }
             if (!__all_sync(FULL, done) && lane == 0) atomicOr(g.status, 2);
          }
-         if (valid) {
-            const int32_t row = FWD ? rho : n - 1 - rho;
-            st_relaxed(g.out + row, zr);
-            ring[w][rho & (kRing - 1)] = zr;
-            if (g.reset) g.reset[row] = sentinel_value();
-            if (g.dot_with) dotp += g.dot_with[row] * zr;
-         }
-         // publish the segment to the next warp of the band
+         // publish the segment: the ring and the release for the next warp
+         // of the band first, the global copy (for other blocks' strands,
+         // whose readers spin on its sentinel) after
+         if (valid) ring[w][rho & (kRing - 1)] = zr;
          __syncwarp();
          if (lane == 0) {
             __threadfence_block();
+            st_release_cta(&keep_from[w], s + 1 < slast ? nxt.keep : INT32_MAX);
             st_release_cta(&done_end[w], min(end, s0 + 32));
+         }
+         if (valid) {
+            const int32_t row = FWD ? rho : n - 1 - rho;
+            st_relaxed(g.out + row, zr);
+            if (g.reset) g.reset[row] = sentinel_value();
+            // dot_with's entry came with the segment's slot data
+            dotp += cur.dw * zr;
          }
          const int last = min(31, end - 1 - s0);
          carry = __shfl_sync(FULL, zr, last);
@@ -842,6 +890,41 @@ void build_plan(ofg_matrix* A, bool fwd, SweepPlan& plan)
       }
    }
    plan.nseg = (int64_t)seg_off.size() - 1;
+   // ring reads of the solve sweeps: a segment of strand t (not the first
+   // of its band) reads the previous strand's rows from the ring when the
+   // lowest of the rows its register slots need is within half the ring of
+   // the highest row needed by it or an earlier segment of the strand; keep
+   // is the suffix minimum of the lowest such row over the strand's segments
+   {
+      const int ns = plan.wmax <= 4 ? 4 : 8;  // register slots of the launch
+      std::vector<int32_t> keep(plan.nseg > 0 ? plan.nseg : 1, INT32_MAX);
+      for (int64_t t = 0, s = 0; t < plan.nstrands; ++t) {
+         const int64_t b = starts[t], e = starts[t + 1];
+         const int64_t s_first = s;
+         int64_t run_need = -1;
+         for (int64_t s0 = b; s0 < e; s0 += 32, ++s) {
+            if (t % kBandWarps == 0) continue;
+            const int64_t pb = starts[t - 1];
+            int64_t need = -1, low = INT64_MAX;
+            for (int64_t rho = s0; rho < std::min(e, s0 + 32); ++rho) {
+               int32_t kb, ke;
+               dep_range(rho, kb, ke);
+               for (int32_t k = kb; k < ke && k - kb < ns; ++k) {
+                  const int64_t l = fwd ? col[k] : n - 1 - col[k];
+                  if (l >= pb && l < b) {
+                     need = std::max(need, l);
+                     low = std::min(low, l);
+                  }
+               }
+            }
+            run_need = std::max(run_need, need);
+            if (need >= 0 && run_need - low < kRing / 2) keep[s] = (int32_t)low;
+         }
+         for (int64_t q = s - 2; q >= s_first; --q) keep[q] = std::min(keep[q], keep[q + 1]);
+      }
+      plan.seg_keep.alloc(keep.size());
+      plan.seg_keep.upload(keep.data(), keep.size());
+   }
    plan.tseg.alloc(tseg.size());
    plan.tseg.upload(tseg.data(), tseg.size());
    plan.seg_off.alloc(seg_off.size());
@@ -869,6 +952,7 @@ SolveArgs solve_args(ofg_prec* P, const SweepPlan& plan)
    g.n = P->A->n;
    g.tseg = plan.tseg.p;
    g.seg_off = plan.seg_off.p;
+   g.seg_keep = plan.seg_keep.p;
    g.sl_col = plan.sl_col.p;
    g.sl_val = plan.sl_val.p;
    g.piv = P->pivot.p;
