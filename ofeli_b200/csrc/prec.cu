@@ -456,9 +456,19 @@ __device__ __forceinline__ int ld_acquire_cta(const int* p)
    return v;
 }
 
-__device__ __forceinline__ void st_release_cta(int* p, int v)
+__device__ __forceinline__ int ld_relaxed_cta(const int* p)
 {
-   asm volatile("st.release.cta.shared.s32 [%0], %1;" ::"r"((unsigned)__cvta_generic_to_shared(p)),
+   int v;
+   asm volatile("ld.relaxed.cta.shared.s32 %0, [%1];"
+                : "=r"(v)
+                : "r"((unsigned)__cvta_generic_to_shared(p))
+                : "memory");
+   return v;
+}
+
+__device__ __forceinline__ void st_relaxed_cta(int* p, int v)
+{
+   asm volatile("st.relaxed.cta.shared.s32 [%0], %1;" ::"r"((unsigned)__cvta_generic_to_shared(p)),
                 "r"(v)
                 : "memory");
 }
@@ -646,9 +656,11 @@ __global__ void __launch_bounds__(kBandWarps * 32, 1) solve_sweep(SolveArgs g)
          run_need = max(run_need, need);
          if (need >= 0) {
             low = __reduce_min_sync(FULL, low);
-            int de = ld_acquire_cta(prev_done);
-            for (int q = 0; q < 32 && de <= need; ++q) de = ld_acquire_cta(prev_done);
+            // relaxed polls, then one fence: an acquire of what was seen
+            int de = ld_relaxed_cta(prev_done);
+            for (int q = 0; q < 32 && de <= need; ++q) de = ld_relaxed_cta(prev_done);
             if (de <= need) de = wait_published(prev_done, need, g.status);
+            asm volatile("fence.acq_rel.cta;" ::: "memory");
             from_ring = de > need && run_need - low < kRing / 2;
          }
          double sext = 0.0;
@@ -735,9 +747,10 @@ __global__ void __launch_bounds__(kBandWarps * 32, 1) solve_sweep(SolveArgs g)
          if (valid) ring[w][rho & (kRing - 1)] = zr;
          __syncwarp();
          if (lane == 0) {
+            // one fence, then relaxed stores: a release of both
             __threadfence_block();
-            st_release_cta(&keep_from[w], s + 1 < slast ? nxt.keep : INT32_MAX);
-            st_release_cta(&done_end[w], min(end, s0 + 32));
+            st_relaxed_cta(&keep_from[w], s + 1 < slast ? nxt.keep : INT32_MAX);
+            st_relaxed_cta(&done_end[w], min(end, s0 + 32));
          }
          if (valid) {
             const int32_t row = FWD ? rho : n - 1 - rho;
