@@ -41,12 +41,14 @@ __global__ void __launch_bounds__(256) assemble_rows(int64_t nn, const int32_t* 
                                                      double* __restrict__ a, double* __restrict__ b,
                                                      int* bad)
 {
+   // each thread sums its row in shared memory (a column per thread)
+   __shared__ double racc[kRowAcc * 256];
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += stride) {
       const int32_t r = dof[i];   // 1-based equation, 0 for an imposed node
       const double bi =
          gather_node_rows(i, r, n2e_ptr[i], n2e_ptr[i + 1], n2e, elem, emap, row_ptr, el, a,
-                          [&](int64_t e) { atomicMin(bad, (int)e); });
+                          [&](int64_t e) { atomicMin(bad, (int)e); }, racc + threadIdx.x, 256);
       if (r) b[r - 1] = bi;
    }
 }

@@ -219,6 +219,9 @@ struct ConvDiffT3 {
 // report(e).  Used by the single-problem kernel (assembly.cu) and the
 // batched solver (batch.cu).  The connectivity of the next element is loaded
 // while the current one is computed.
+// longest row summed in shared memory by gather_node_rows
+constexpr int kRowAcc = 16;
+
 template <class Elem, class Report>
 __device__ __forceinline__ double gather_node_rows(int64_t i, int32_t r, int32_t q0, int32_t q1,
                                                    const int32_t* __restrict__ n2e,
@@ -226,11 +229,24 @@ __device__ __forceinline__ double gather_node_rows(int64_t i, int32_t r, int32_t
                                                    const int32_t* __restrict__ emap,
                                                    const int32_t* __restrict__ row_ptr,
                                                    const Elem& el, double* __restrict__ a,
-                                                   Report&& report)
+                                                   Report&& report, double* racc = nullptr,
+                                                   int rstride = 0)
 {
    constexpr int NEN = Elem::NEN;
-   if (r)
-      for (int32_t k = row_ptr[r - 1]; k < row_ptr[r]; ++k) a[k] = 0.0;
+   // the row is summed in racc (entry j at racc[j * rstride], shared
+   // memory) when given and the row fits, then stored once; the additions
+   // are the same, in the same order, as in place
+   int32_t rs = 0, rl = 0;
+   bool local = false;
+   if (r) {
+      rs = row_ptr[r - 1];
+      rl = row_ptr[r] - rs;
+      local = racc != nullptr && rl <= kRowAcc;
+      if (local)
+         for (int32_t j = 0; j < rl; ++j) racc[j * rstride] = 0.0;
+      else
+         for (int32_t k = rs; k < rs + rl; ++k) a[k] = 0.0;
+   }
    double bi = 0.0;
    int64_t e_next = q0 < q1 ? n2e[q0] : 0;
    int32_t en_next[NEN];
@@ -263,11 +279,20 @@ __device__ __forceinline__ double gather_node_rows(int64_t i, int32_t r, int32_t
          if (li == 0) report(e);
          continue;
       }
+      if (local) {
 #pragma unroll
-      for (int j = 0; j < NEN; ++j)
-         if (pos[j] >= 0) a[pos[j]] += krow[j];
+         for (int j = 0; j < NEN; ++j)
+            if (pos[j] >= 0) racc[(pos[j] - rs) * rstride] += krow[j];
+      }
+      else {
+#pragma unroll
+         for (int j = 0; j < NEN; ++j)
+            if (pos[j] >= 0) a[pos[j]] += krow[j];
+      }
       bi += frow;
    }
+   if (local)
+      for (int32_t j = 0; j < rl; ++j) a[rs + j] = racc[j * rstride];
    return bi;
 }
 
