@@ -555,7 +555,9 @@ void fgmres_mixed(ofg_prec* P, int inner_bits, const double* b, double* x, int m
                "inner_bits must be 32, 16 or 0 (automatic)");
    OFG_REQUIRE(inner_tol > 0 && inner_tol < 1, OFG_ERR_ARG, "inner_tol must be in (0, 1)");
    const int64_t n = A->n;
-   ensure_sell(A);
+   // FP32 values asked for: both SELL copies of new values in one pass
+   if (inner_bits == 32) ensure_sell32(A);
+   else ensure_sell(A);
    ensure_dpos(A);
    OFG_REQUIRE(A->dpos_complete, OFG_ERR_PIVOT, "a row has no diagonal entry");
    bool learned = P->type == OFG_LEARNED;

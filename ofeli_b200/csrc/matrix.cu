@@ -154,6 +154,19 @@ __global__ void sell_values(int64_t total, const int32_t* ssrc, const double* va
    }
 }
 
+// both SELL copies (FP64 and FP32) from one gather of the CSR values
+__global__ void sell_values_both(int64_t total, const int32_t* ssrc, const double* val,
+                                 double* sval, float* sval32)
+{
+   int64_t stride = (int64_t)gridDim.x * blockDim.x;
+   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+      const int32_t s = ssrc[i];
+      const double v = s >= 0 ? val[s] : 0.0;
+      sval[i] = v;
+      sval32[i] = (float)v;
+   }
+}
+
 __global__ void sell_values_bf16(int64_t total, const int32_t* ssrc, const double* val,
                                  uint16_t* sval)
 {
@@ -487,6 +500,18 @@ void ensure_sell(ofg_matrix* A)
 
 void ensure_sell32(ofg_matrix* A)
 {
+   if (A->sell_ready && A->sell_version != A->version && A->sell_val32.n == A->sell_val.n) {
+      // both copies stale (new values): one pass writes both
+      const int64_t total = A->sell_val.n;
+      sell_values_both<<<grid_for(total, 256), 256, 0, stream()>>>(total, A->sell_src.p, A->val.p,
+                                                                   A->sell_val.p,
+                                                                   A->sell_val32.p);
+      count_launch();
+      OFG_LAUNCH_CHECK();
+      A->sell_version = A->version;
+      A->sell32_version = A->version;
+      return;
+   }
    ensure_sell(A);
    if (A->sell32_version != A->version || A->sell_val32.n != A->sell_val.n) {
       int64_t total = A->sell_val.n;

@@ -469,7 +469,9 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
    OFG_REQUIRE(mode == 0 || mode == 1, OFG_ERR_ARG, "mode must be 0 or 1");
    OFG_REQUIRE(inner_tol > 0 && inner_tol < 1, OFG_ERR_ARG, "inner_tol must be in (0, 1)");
    const int64_t n = A->n;
-   ensure_sell(A);
+   // FP32 values asked for: both SELL copies of new values in one pass
+   if (inner_bits == 32) ensure_sell32(A);
+   else ensure_sell(A);
    ensure_dpos(A);
    OFG_REQUIRE(A->dpos_complete, OFG_ERR_PIVOT, "a row has no diagonal entry");
    bool g16 = false;
