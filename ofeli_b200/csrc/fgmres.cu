@@ -58,15 +58,17 @@ struct FGState {
    int steps;          // Arnoldi steps completed in the cycle
    int stop;           // the cycle is over
    int done;           // FP64 true residual <= toler
-   int pad;
+   int skip_end;       // the cycle-end kernels of this batch do nothing
 };
 
 // r = b - q (FP64); ||r||, ||b|| (first call); the FP64 convergence test
 __global__ void __launch_bounds__(kRedBlock, 8) fg_residual(int64_t n, const double* __restrict__ b,
                                                          const double* __restrict__ q, double* r,
                                                          FGState* S, double* partials,
-                                                         unsigned* counter, double tol, int first)
+                                                         unsigned* counter, double tol, int first,
+                                                         int end)
 {
+   if (end && S->skip_end) return;
    double v[2] = {0.0, 0.0};
    int64_t stride = (int64_t)gridDim.x * blockDim.x;
    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
@@ -399,12 +401,19 @@ __global__ void __launch_bounds__(kRedBlock, 8) fg_next(int64_t nquads, const do
    }
 }
 
-// y = R^{-1} s over the cycle's S->steps columns (R = the rotated H)
-__global__ void fg_backsolve(const double* H, const double* s, double* y, int m, const FGState* S)
+// The end of a batch of Arnoldi steps: when the cycle is over (stopped,
+// or `last`: all m steps done), y = R^{-1} s over its S->steps columns (R
+// = the rotated H); otherwise it marks the batch's cycle-end kernels (the
+// solution update, the FP64 residual) to do nothing.
+__global__ void fg_backsolve(const double* H, const double* s, double* y, int m, FGState* S,
+                             int last)
 {
    pdl_wait();
    pdl_release();
    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+   const int end = last || S->stop;
+   S->skip_end = end ? 0 : 1;
+   if (!end) return;
    const int ld = m + 1, k = S->steps;
    for (int i = 0; i < k; ++i) y[i] = s[i];
    for (int i = k - 1; i >= 0; --i) {
@@ -422,6 +431,7 @@ __global__ void __launch_bounds__(kRedBlock, 8) fg_update_x(int64_t n, double* x
    __shared__ double ys[kMaxRestart];
    pdl_wait();
    pdl_release();
+   if (S->skip_end) return;
    const int k = S->steps;
    for (int l = threadIdx.x; l < k; l += blockDim.x) ys[l] = y[l];
    __syncthreads();
@@ -622,10 +632,11 @@ void fgmres_mixed(ofg_prec* P, int inner_bits, const double* b, double* x, int m
    DBuf<unsigned> counter(1);
    counter.zero();
 
-   auto true_residual = [&](int first) {
-      spmv_sell(A, x, q64.p);
+   // end = 1: the cycle-end form, a no-op while S->skip_end is set
+   auto true_residual = [&](int first, int end = 0) {
+      spmv_sell(A, x, q64.p, end ? &S.p->skip_end : nullptr);
       fg_residual<<<gn, kRedBlock, 0, stream()>>>(n, b, q64.p, r.p, S.p, partials.p, counter.p, tol,
-                                                  first);
+                                                  first, end);
       count_launch();
       OFG_LAUNCH_CHECK();
    };
@@ -652,7 +663,8 @@ void fgmres_mixed(ofg_prec* P, int inner_bits, const double* b, double* x, int m
       if (learned) learned_z(0);
       const CycleRule rule{inner_tol, 0.5 * tol * h.bnorm, m, max_inner - n_inner};
       int j = 0;
-      for (int batch = 4; j < m; batch *= 2) {
+      bool cycle_over = false;
+      for (int batch = 4; !cycle_over; batch *= 2) {
          const int end = std::min(m, j + batch);
          for (; j < end; ++j) {
             float* zj = Z.p + (size_t)j * ldz;
@@ -682,19 +694,17 @@ void fgmres_mixed(ofg_prec* P, int inner_bits, const double* b, double* x, int m
                if (learned) learned_z(j + 1);
             }
          }
+         // the cycle's end (back-substitution, x += Z y, the FP64 residual)
+         // is enqueued after every batch and runs only when the cycle is
+         // over, so one read of the state per batch decides
+         launch_pdl(fg_backsolve, 1, 32, H.p, s.p, y.p, m, S.p, end == m ? 1 : 0);
+         launch_pdl(fg_update_x, gn, kRedBlock, n, x, Z.p, ldz, y.p, S.p);
          OFG_LAUNCH_CHECK();
-         if (j < m) {
-            S.download(&h, 1);
-            if (h.stop) break;
-         }
+         true_residual(0, 1);
+         S.download(&h, 1);
+         cycle_over = !h.skip_end;
       }
-      launch_pdl(fg_backsolve, 1, 32, H.p, s.p, y.p, m, S.p);
-      launch_pdl(fg_update_x, gn, kRedBlock, n, x, Z.p, ldz, y.p, S.p);
-      OFG_LAUNCH_CHECK();
-      S.download(&h, 1);
       n_inner += h.steps;
-      true_residual(0);
-      S.download(&h, 1);
       n_outer++;
       // the learned preconditioner must keep the FP64 residual falling;
       // otherwise the remaining cycles use the diagonal one
