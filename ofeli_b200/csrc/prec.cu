@@ -148,6 +148,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) sweep_kernel(SweepArgs g)
          // column order; intra-segment couplings are recorded
          double sext = 0.0, m1 = 0.0;
          bool other_intra = false;
+         // FACTOR: the coupling to the row before, when it is the row's
+         // last lower entry (then the sum subtracts it last)
+         bool has_prev = false;
+         double a_prev = 0.0, t_prev = 0.0;
          if (MODE == FACTOR) sext = valid ? g.val[dk] : 0.0;
          // the first kPre entries: all loads (matrix and earlier results)
          // are issued before any is consumed, so their latencies overlap
@@ -184,7 +188,15 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) sweep_kernel(SweepArgs g)
             if (MODE == FACTOR) {
                const int32_t tp = g.tpos[kb + q];
                if (tp < 0) continue;
-               if (lj >= s0) { other_intra = true; continue; }
+               if (lj >= s0) {
+                  if (lj == rho - 1 && kb + q == ke - 1) {
+                     has_prev = true;
+                     a_prev = a;
+                     t_prev = g.val[tp];
+                  }
+                  else other_intra = true;
+                  continue;
+               }
                sext = __dsub_rn(sext, __dmul_rn(__dmul_rn(a, v), g.val[tp]));
             }
             else {
@@ -203,7 +215,15 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) sweep_kernel(SweepArgs g)
             if (MODE == FACTOR) {
                const int32_t tp = g.tpos[k];
                if (tp < 0) continue;
-               if (lj >= s0) { other_intra = true; continue; }
+               if (lj >= s0) {
+                  if (lj == rho - 1 && k == ke - 1) {
+                     has_prev = true;
+                     a_prev = a;
+                     t_prev = g.val[tp];
+                  }
+                  else other_intra = true;
+                  continue;
+               }
                const double v = (lj == s0 - 1 && have_carry) ? carry : wait_value(g.out + j, g.status);
                sext = __dsub_rn(sext, __dmul_rn(__dmul_rn(a, v), g.val[tp]));
             }
@@ -223,8 +243,22 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) sweep_kernel(SweepArgs g)
             pv = g.piv[row];
          }
          double z;
-         const bool exact = (MODE == FACTOR) || __any_sync(FULL, other_intra);
-         if (!exact) {
+         const bool chain = (MODE == FACTOR) && !__any_sync(FULL, other_intra);
+         const bool exact = !chain && ((MODE == FACTOR) || __any_sync(FULL, other_intra));
+         if (chain) {
+            // pivots in lane order: a lane coupled only to the row before
+            // takes that row's pivot by a shuffle and subtracts its term
+            // last, in OFELI's order; the others need nothing from the
+            // segment
+            z = 0.0;
+            if (valid && !has_prev) z = __ddiv_rn(1.0, sext);
+            for (int i = 1; i < 32; ++i) {
+               const double v = __shfl_sync(FULL, z, i - 1);
+               if (lane == i && valid && has_prev)
+                  z = __ddiv_rn(1.0, __dsub_rn(sext, __dmul_rn(__dmul_rn(a_prev, v), t_prev)));
+            }
+         }
+         else if (!exact) {
             // z = C + M * z_prev with z_prev the previous lane's result
             double C, M;
             if (MODE == FWD_DILU) { C = pv * (bi - sext); M = -pv * m1; }
