@@ -59,6 +59,8 @@ struct FGState {
    int stop;           // the cycle is over
    int done;           // FP64 true residual <= toler
    int skip_end;       // the cycle-end kernels of this batch do nothing
+   int zero_diag;      // a diagonal entry is zero (FP32 values: checked with the first state read)
+   int pad;
 };
 
 // r = b - q (FP64); ||r||, ||b|| (first call); the FP64 convergence test
@@ -596,14 +598,21 @@ void fgmres_mixed(ofg_prec* P, int inner_bits, const double* b, double* x, int m
                                                                        bad.p + 1);
       count_launch();
    }
+   DBuf<FGState> S(1);
+   S.zero();
    DBuf<float> dinv(nv);
+   // with FP32 values nothing waits for the zero-diagonal flag: it travels
+   // in the solver state and is checked at its first read
    fg_inv_diag<<<grid_for(nv, 256), 256, 0, stream()>>>(n, npad, A->dpos.p, A->val.p, dinv.p,
-                                                         P->type == OFG_IDENT ? 1 : 0, bad.p);
+                                                         P->type == OFG_IDENT ? 1 : 0,
+                                                         inner_bits == 32 ? &S.p->zero_diag : bad.p);
    count_launch();
    OFG_LAUNCH_CHECK();
    int hb[2] = {0, 0};
-   bad.download(hb, 2);
-   OFG_REQUIRE(!hb[0], OFG_ERR_PIVOT, "zero diagonal entry");
+   if (inner_bits != 32) {
+      bad.download(hb, 2);
+      OFG_REQUIRE(!hb[0], OFG_ERR_PIVOT, "zero diagonal entry");
+   }
    // automatic format: BF16 values only when every value is exact in BF16
    const bool use16 = inner_bits == 16 || (inner_bits == 0 && !hb[1]);
    if (use16) {
@@ -624,7 +633,6 @@ void fgmres_mixed(ofg_prec* P, int inner_bits, const double* b, double* x, int m
    v32.zero();
    t32.zero();
    DBuf<double> H((size_t)(m + 1) * (m + 1)), s(m + 1), cs(m + 1), sn(m + 1), y(m + 1), h2(m + 1);
-   DBuf<FGState> S(1);
    const unsigned gq = grid_for(nquads, kRedBlock, kQuadBlocks);
    const unsigned gr = grid_for(nquads, kRedBlock, 4);
    const unsigned gn = grid_for(n, kRedBlock, 8);
@@ -654,6 +662,7 @@ void fgmres_mixed(ofg_prec* P, int inner_bits, const double* b, double* x, int m
    FGState h{};
    true_residual(1);
    S.download(&h, 1);
+   OFG_REQUIRE(!h.zero_diag, OFG_ERR_PIVOT, "zero diagonal entry");
    int n_outer = 0, n_inner = 0, no_gain = 0;
    double last_rel = h.rel;
    while (!h.done && n_outer < max_outer && n_inner < max_inner && n > 0) {
