@@ -615,7 +615,7 @@ void solve_mixed(ofg_matrix* A, int prec_type, int inner_bits, int mode, const d
    // stagnation watch of the learned iteration: the recursive residual must
    // halve within kStallIters iterations and stay finite, and the true
    // residual must fall at every refinement
-   constexpr int kStallIters = 500;
+   constexpr int kStallIters = 2000;
    bool stalled = false;
    int no_gain = 0;
    double last_rel = h.rel;
