@@ -523,6 +523,66 @@ __device__ __noinline__ int wait_published(const int* done_end, int need, int* s
    return de;
 }
 
+// waits until the previous warp of the band has published past row `need`:
+// relaxed polls, then one fence (an acquire of what was seen); returns the
+// value seen, or -1 when the wait ran out (status set)
+__device__ __forceinline__ int wait_previous(const int* prev_done, int need, int* status)
+{
+   int de = ld_relaxed_cta(prev_done);
+   for (int q = 0; q < 32 && de <= need; ++q) de = ld_relaxed_cta(prev_done);
+   if (de <= need) de = wait_published(prev_done, need, status);
+   asm volatile("fence.acq_rel.cta;" ::: "memory");
+   return de;
+}
+
+// Polls (bounded) the earlier rows of the slots in `pend` until none holds
+// the sentinel: every round issues the loads of all pending slots before it
+// tests any, so that slots published together cost one round trip.  On
+// time-out the status is set and the missing values read as 0.
+template <int NS>
+__device__ __forceinline__ void poll_slots(const double* out, const int32_t (&c)[NS], unsigned pend,
+                                        double (&v)[NS], int* status)
+{
+   for (long long it = 0; pend; ++it) {
+      if (it >= kSpinFast + kSpinSlow) {
+         atomicOr(status, 1);
+#pragma unroll
+         for (int k = 0; k < NS; ++k)
+            if ((pend >> k) & 1) v[k] = 0.0;
+         return;
+      }
+      if (it >= kSpinFast) __nanosleep(500);
+#pragma unroll
+      for (int k = 0; k < NS; ++k)
+         if ((pend >> k) & 1) v[k] = ld_relaxed(out + c[k]);
+#pragma unroll
+      for (int k = 0; k < NS; ++k)
+         if (((pend >> k) & 1) && !is_sentinel(v[k])) pend &= ~(1u << k);
+   }
+}
+
+// The additive half of a segment's affine scan: row rho's result is
+// C(rho) + M(rho) z(rho - 1), C from the slot sum; Mr[r] is the product of M
+// over the 2^r rows ending at this lane (the multiplicative half)
+template <int MODE>
+__device__ __forceinline__ double affine_scan(double sext, double bi, double pv, bool valid,
+                                              const double (&Mr)[5], int lane)
+{
+   const unsigned FULL = 0xffffffffu;
+   double C;
+   if (MODE == FWD_DILU) C = pv * (bi - sext);
+   else if (MODE == FWD_SSOR) C = (bi - sext) / pv;
+   else if (MODE == BWD_DILU) C = bi - pv * sext;
+   else C = bi - sext / pv;
+   if (!valid) C = 0.0;
+#pragma unroll
+   for (int r = 0; r < 5; ++r) {
+      const double Cp = __shfl_up_sync(FULL, C, 1 << r);
+      if (lane >= (1 << r)) C = C + Mr[r] * Cp;
+   }
+   return C;
+}
+
 template <int NS>
 struct SegRegs {
    int32_t off, w, keep;
@@ -598,6 +658,7 @@ __global__ void __launch_bounds__(kBandWarps * 32, 1) solve_sweep(SolveArgs g)
       const bool has_consumer = w + 1 < kBandWarps && t + 1 < g.nstrands;
       int run_need = -1;  // highest previous-strand row needed so far
       const int* prev_done = &done_end[w > 0 ? w - 1 : 0];
+      const double* prev_ring = ring[w > 0 ? w - 1 : 0];
       const int64_t sfirst = g.tseg[t], slast = g.tseg[t + 1];
       double carry = 0.0;
       bool have_carry = false;
@@ -638,6 +699,7 @@ __global__ void __launch_bounds__(kBandWarps * 32, 1) solve_sweep(SolveArgs g)
          int need = -1, low = INT32_MAX;
          double m1 = 0.0;
          bool other_intra = false;
+         unsigned gpend = 0;  // slots loaded from global memory
 #pragma unroll
          for (int k = 0; k < NS; ++k) {
             const int32_t c = cur.c[k];
@@ -650,13 +712,17 @@ __global__ void __launch_bounds__(kBandWarps * 32, 1) solve_sweep(SolveArgs g)
                else other_intra = true;
             }
             else if (lj[k] == s0 - 1 && have_carry) pre[k] = carry;
-            else if (lj[k] >= beg) pre[k] = wait_value(g.out + c, g.status);  // own strand
-            else if (lj[k] >= pbeg) {
+            else if (lj[k] >= beg || lj[k] < pbeg) {
+               // this strand's earlier segments or another block's strand:
+               // loaded from global memory, all such slots together
+               pre[k] = ld_relaxed(g.out + c);
+               gpend |= 1u << k;
+            }
+            else {
                from_prev[k] = true;
                need = max(need, lj[k]);
                low = min(low, lj[k]);
             }
-            else pre[k] = wait_value(g.out + c, g.status);  // another block's strand
          }
          for (int k = NS; k < cur.w; ++k) {  // rows wider than the register slots
             const int32_t c = g.sl_col[cur.off + k * 32 + lane];
@@ -682,110 +748,114 @@ __global__ void __launch_bounds__(kBandWarps * 32, 1) solve_sweep(SolveArgs g)
                if (lane >= (1 << r)) M = M * Mp;
             }
          }
+         // global slots whose value was not there yet (the first strand of a
+         // band waiting for the previous block's last strand): polled together
+#pragma unroll
+         for (int k = 0; k < NS; ++k)
+            if (!is_sentinel(pre[k])) gpend &= ~(1u << k);
+         if (gpend) poll_slots<NS>(g.out, cur.c, gpend, pre, g.status);
          // the consumer no longer reads the ring slots this segment overwrites
          if (has_consumer && ld_acquire_cta(&keep_from[w + 1]) <= s0 + 31 - kRing)
             wait_published(&keep_from[w + 1], s0 + 31 - kRing, g.status);
-         bool from_ring = false;
          need = __reduce_max_sync(FULL, need);
+         low = __reduce_min_sync(FULL, low);
          run_need = max(run_need, need);
-         if (need >= 0) {
-            low = __reduce_min_sync(FULL, low);
-            // relaxed polls, then one fence: an acquire of what was seen
-            int de = ld_relaxed_cta(prev_done);
-            for (int q = 0; q < 32 && de <= need; ++q) de = ld_relaxed_cta(prev_done);
-            if (de <= need) de = wait_published(prev_done, need, g.status);
-            asm volatile("fence.acq_rel.cta;" ::: "memory");
-            from_ring = de > need && run_need - low < kRing / 2;
-         }
-         double sext = 0.0;
-         if (from_ring) {
-            // every slot reads the ring (the empty ones a harmless slot) and
-            // selects: no branch between the wait and the sum
+         // ring reads are safe when the rows lie within half the ring of the
+         // highest row needed so far (the plan's back-pressure covers them)
+         const bool ring_ok = need >= 0 && run_need - low < kRing / 2;
+         double zr;
+         if (affine && cur.w <= NS && (need < 0 || ring_ok)) {
+            // the common step: chosen before the wait, so that nothing after
+            // it branches.  Every slot reads the ring (the empty ones a
+            // harmless slot) and selects.
+            if (need >= 0) wait_previous(prev_done, need, g.status);
             double rv[NS];
 #pragma unroll
-            for (int k = 0; k < NS; ++k) rv[k] = ring[w - 1][lj[k] & (kRing - 1)];
+            for (int k = 0; k < NS; ++k) rv[k] = prev_ring[lj[k] & (kRing - 1)];
+            double sext = 0.0;
 #pragma unroll
             for (int k = 0; k < NS; ++k) {
                if (cur.c[k] < 0 || lj[k] >= s0) continue;
                sext += cur.a[k] * (from_prev[k] ? rv[k] : pre[k]);
             }
+            zr = affine_scan<MODE>(sext, bi, pv, valid, Mr, lane);
          }
          else {
+            bool from_ring = false;
+            if (need >= 0) from_ring = wait_previous(prev_done, need, g.status) > need && ring_ok;
+            double sext = 0.0;
+            if (from_ring) {
+               double rv[NS];
 #pragma unroll
-            for (int k = 0; k < NS; ++k) {
-               if (cur.c[k] < 0 || lj[k] >= s0) continue;
-               const double v = from_prev[k] ? wait_value(g.out + cur.c[k], g.status) : pre[k];
-               sext += cur.a[k] * v;
-            }
-         }
-         for (int k = NS; k < cur.w; ++k) {
-            const int32_t c = g.sl_col[cur.off + k * 32 + lane];
-            if (c < 0) continue;
-            const int32_t l = FWD ? c : n - 1 - c;
-            if (l >= s0) continue;
-            const double a = g.sl_val[cur.off + k * 32 + lane];
-            const double v = (l == s0 - 1 && have_carry) ? carry : wait_value(g.out + c, g.status);
-            sext += a * v;
-         }
-         double zr;
-         if (affine) {
-            double C;
-            if (MODE == FWD_DILU) C = pv * (bi - sext);
-            else if (MODE == FWD_SSOR) C = (bi - sext) / pv;
-            else if (MODE == BWD_DILU) C = bi - pv * sext;
-            else C = bi - sext / pv;
-            if (!valid) C = 0.0;
+               for (int k = 0; k < NS; ++k) rv[k] = prev_ring[lj[k] & (kRing - 1)];
 #pragma unroll
-            for (int r = 0; r < 5; ++r) {
-               const double Cp = __shfl_up_sync(FULL, C, 1 << r);
-               if (lane >= (1 << r)) C = C + Mr[r] * Cp;
-            }
-            zr = C;
-         }
-         else {
-            // exact wave over the intra-segment couplings
-            segv[w][lane] = sentinel_value();
-            __syncwarp();
-            bool done = !valid;
-            zr = 0.0;
-            for (int round = 0; round < 32; ++round) {
-               if (!done) {
-                  bool ready = true;
-                  double acc = sext;
-                  // (re-read from the slot arrays: indexing the register
-                  // copies with a run-time k would move them to local memory)
-                  for (int k = 0; k < cur.w && ready; ++k) {
-                     const int32_t c = g.sl_col[cur.off + k * 32 + lane];
-                     if (c < 0) continue;
-                     const int32_t l = FWD ? c : n - 1 - c;
-                     if (l < s0) continue;
-                     const double v = segv[w][l - s0];
-                     if (is_sentinel(v)) { ready = false; break; }
-                     acc += g.sl_val[cur.off + k * 32 + lane] * v;
-                  }
-                  if (ready) {
-                     zr = finish_row<MODE>(acc, bi, pv);
-                     done = true;
-                  }
+               for (int k = 0; k < NS; ++k) {
+                  if (cur.c[k] < 0 || lj[k] >= s0) continue;
+                  sext += cur.a[k] * (from_prev[k] ? rv[k] : pre[k]);
                }
-               __syncwarp();
-               if (done && valid) segv[w][lane] = zr;
-               __syncwarp();
-               if (__all_sync(FULL, done)) break;
             }
-            if (!__all_sync(FULL, done) && lane == 0) atomicOr(g.status, 2);
+            else {
+#pragma unroll
+               for (int k = 0; k < NS; ++k) {
+                  if (cur.c[k] < 0 || lj[k] >= s0) continue;
+                  const double v = from_prev[k] ? wait_value(g.out + cur.c[k], g.status) : pre[k];
+                  sext += cur.a[k] * v;
+               }
+            }
+            for (int k = NS; k < cur.w; ++k) {
+               const int32_t c = g.sl_col[cur.off + k * 32 + lane];
+               if (c < 0) continue;
+               const int32_t l = FWD ? c : n - 1 - c;
+               if (l >= s0) continue;
+               const double a = g.sl_val[cur.off + k * 32 + lane];
+               const double v = (l == s0 - 1 && have_carry) ? carry : wait_value(g.out + c, g.status);
+               sext += a * v;
+            }
+            if (affine) zr = affine_scan<MODE>(sext, bi, pv, valid, Mr, lane);
+            else {
+               // exact wave over the intra-segment couplings
+               segv[w][lane] = sentinel_value();
+               __syncwarp();
+               bool done = !valid;
+               zr = 0.0;
+               for (int round = 0; round < 32; ++round) {
+                  if (!done) {
+                     bool ready = true;
+                     double acc = sext;
+                     // (re-read from the slot arrays: indexing the register
+                     // copies with a run-time k would move them to local memory)
+                     for (int k = 0; k < cur.w && ready; ++k) {
+                        const int32_t c = g.sl_col[cur.off + k * 32 + lane];
+                        if (c < 0) continue;
+                        const int32_t l = FWD ? c : n - 1 - c;
+                        if (l < s0) continue;
+                        const double v = segv[w][l - s0];
+                        if (is_sentinel(v)) { ready = false; break; }
+                        acc += g.sl_val[cur.off + k * 32 + lane] * v;
+                     }
+                     if (ready) {
+                        zr = finish_row<MODE>(acc, bi, pv);
+                        done = true;
+                     }
+                  }
+                  __syncwarp();
+                  if (done && valid) segv[w][lane] = zr;
+                  __syncwarp();
+                  if (__all_sync(FULL, done)) break;
+               }
+               if (!__all_sync(FULL, done) && lane == 0) atomicOr(g.status, 2);
+            }
          }
          // publish the segment: the ring and the release for the next warp
          // of the band first, the global copy (for other blocks' strands,
-         // whose readers spin on its sentinel) after
+         // whose readers spin on its sentinel) after.  One fence, then
+         // relaxed stores (every lane the same value): a release of both,
+         // with no branch on the lane.
          if (valid) ring[w][rho & (kRing - 1)] = zr;
          __syncwarp();
-         if (lane == 0) {
-            // one fence, then relaxed stores: a release of both
-            __threadfence_block();
-            st_relaxed_cta(&keep_from[w], s + 1 < slast ? nxt.keep : INT32_MAX);
-            st_relaxed_cta(&done_end[w], min(end, s0 + 32));
-         }
+         __threadfence_block();
+         st_relaxed_cta(&keep_from[w], s + 1 < slast ? nxt.keep : INT32_MAX);
+         st_relaxed_cta(&done_end[w], min(end, s0 + 32));
          if (valid) {
             const int32_t row = FWD ? rho : n - 1 - rho;
             st_relaxed(g.out + row, zr);

@@ -107,6 +107,29 @@ def test_fgmres_mixed_edges(cuda):
     assert not res <= TOL
 
 
+@pytest.mark.parametrize("inner_bits", [32, 16, 0])
+def test_fgmres_mixed_zero_diagonal_raises(cuda, inner_bits):
+    """A zero diagonal entry that appears after the preconditioner was made
+    is an error for every value format (with FP32 values the flag travels in
+    the solver state and is read with the first state read), and the matrix
+    solves again once the entry is restored."""
+    g, info = load_golden("cd2d_17")
+    rp, ci = g["row_ptr"], g["col_ind"]
+    A = F.SpMatrix(rp, ci, g["a0"])
+    P = F.Prec(A, F.DIAG_PREC)
+    a = np.array(g["a0"], dtype=np.float64)
+    row = 40
+    d = next(k for k in range(rp[row], rp[row + 1]) if ci[k] == row)
+    a[d] = 0.0
+    A.set_values(a)
+    with pytest.raises(F.OFELIException, match="zero diagonal"):
+        F.fgmres_mixed(P, g["b0"], np.zeros(A.n), inner_bits=inner_bits, toler=TOL)
+    A.set_values(g["a0"])
+    x = np.zeros(A.n)
+    res = F.fgmres_mixed(P, g["b0"], x, inner_bits=inner_bits, toler=TOL)[2]
+    assert res <= TOL
+
+
 @pytest.fixture(scope="module")
 def transient_net(cuda):
     net, info = LN.train_transient(nproblems=4, sizes=(64, 128), rounds=6)
