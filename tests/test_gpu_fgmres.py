@@ -119,7 +119,8 @@ def test_fgmres_mixed_zero_diagonal_raises(cuda, inner_bits):
     P = F.Prec(A, F.DIAG_PREC)
     a = np.array(g["a0"], dtype=np.float64)
     row = 40
-    d = next(k for k in range(rp[row], rp[row + 1]) if ci[k] == row)
+    # (OFELI's 1-based column indices)
+    d = next(k for k in range(rp[row], rp[row + 1]) if ci[k] == row + 1)
     a[d] = 0.0
     A.set_values(a)
     with pytest.raises(F.OFELIException, match="zero diagonal"):
