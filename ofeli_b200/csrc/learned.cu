@@ -403,7 +403,7 @@ __global__ void __launch_bounds__(128, 4) gemm_tc(int64_t rows, GemmA a,
                smem_u32(mbar))
             : "memory");
       }
-      // bounded wait for the MMAs of this tile; the verdict is made uniform
+      // bounded wait for the MMAs of this tile; the outcome is made uniform
       // over the block so that every thread leaves the loop together
       if (__syncthreads_or(mbar_wait(smem_u32(mbar), phase) ? 0 : 1)) {
          failed = true;
@@ -722,7 +722,7 @@ __global__ void __launch_bounds__(128, 4) wgrad_tc(int64_t rows, GemmA a,
       }
       any = true;
       // the tile's MMAs must finish before the next tile overwrites the
-      // operands (bounded wait, verdict uniform over the block)
+      // operands (bounded wait, outcome uniform over the block)
       if (__syncthreads_or(mbar_wait(smem_u32(mbar), phase) ? 0 : 1)) {
          failed = true;
          if (tid == 0) atomicOr(status, 1);
